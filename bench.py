@@ -1,0 +1,310 @@
+"""Benchmark: transient path tracing throughput (paths/s) on one B200 per rank.
+
+Workload (the configuration the headline metric is quoted on): the Cornell room with two boxes
+plus a displaced icosphere at subdivision 7 (327,714 triangles), 512x512 pixels, 2048 time bins
+of 0.0025, 256 samples per pixel, max depth 8 -- 67,108,864 camera paths per frame.  One step
+renders one full frame (all 256 samples of every pixel) into the device FP64 streak film.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Multi-GPU (torchrun): every rank renders its own seeded replica
+of the frame (weak scaling, no exchange); value = all paths / max-over-ranks device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Canonical-BVH traffic per query for the icosphere workload, measured by the oracle on its own
+# one-sample-per-pixel render rays (python oracle/measure_traffic.py icosphere):
+# B = 48 B ray in/out + 64 B per two-child node visit + 48 B per triangle test.
+B_CLOSEST = 48 + 64 * 19.397909840536915 + 48 * 8.579641797558255     # 1701.3 B
+B_SHADOW = 48 + 64 * 16.98375084460311 + 48 * 6.767252594318216       # 1459.8 B
+# DRAM bytes per extend launch from one ncu capture (scaled to a full launch), or None.
+TRAFFIC_PER_EXTEND_LAUNCH = None
+
+WORKLOAD = "icosphere"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spp-per-step", type=int, default=None, help="default: the workload's 256")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(scene, rows_per_proc, procs):
+    """Times the reference renderer (oracle/_ref/ref_render, the reference's own integrator and
+    film built from its sources) on host cores: `procs` processes over disjoint scanlines."""
+    from oracle import refscene, pyoracle
+    if not refscene.ref_available():
+        # the oracle port, all threads, on the same rows
+        o = pyoracle.Oracle(scene)
+        nthreads = os.cpu_count() or 1
+        y0 = scene.height // 2
+        t0 = time.perf_counter()
+        r = o.render(sample_count=scene.spp, window=(0, y0, scene.width, y0 + rows_per_proc), nthreads=nthreads,
+                     streak=False)
+        dt = time.perf_counter() - t0
+        return {"value": r["stats"]["paths"] / dt, "unit": "paths/s", "cores": nthreads, "kind": "port",
+                "sample": f"{rows_per_proc} scanlines x {scene.width} px x {scene.spp} spp, oracle port"}
+    wd = tempfile.mkdtemp(prefix="bk_bench_")
+    sp = os.path.join(wd, "scene.txt")
+    refscene.write_scene(scene, sp)
+    ps = []
+    for i in range(procs):
+        y0 = (scene.height // 2 - procs * rows_per_proc // 2 + i * rows_per_proc) % scene.height
+        y1 = min(scene.height, y0 + rows_per_proc)
+        ps.append(subprocess.Popen([refscene.REF_BIN, sp, os.path.join(wd, f"out{i}.bin"), str(y0), str(y1),
+                                    "--no-streak"], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True))
+    paths, secs = 0, 0.0
+    for p in ps:
+        _, err = p.communicate()
+        info = json.loads(err.strip().splitlines()[-1])
+        paths += info["paths"]
+        secs = max(secs, info["seconds"])
+    for f in os.listdir(wd):
+        os.remove(os.path.join(wd, f))
+    os.rmdir(wd)
+    return {"value": paths / secs, "unit": "paths/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x {rows_per_proc} scanline(s) x {scene.width} px x {scene.spp} spp "
+                      f"({paths} paths), reference integrator with its own triangle/BVH backend, "
+                      f"render loop time of the slowest process"}
+
+
+def run_reference(args, rank, world):
+    from jarabotransientrendering_b200 import scenes as S
+    if rank != 0:
+        return
+    sc = S.WORKLOADS[WORKLOAD]()
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    rows = max(1, args.steps)
+    cb = cpu_reference(sc, rows, procs)
+    paths_per_step = sc.paths_per_frame()
+    line = {"impl": "reference", "metric": "paths/s", "value": cb["value"], "unit": "paths/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": paths_per_step / cb["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8",
+                       "triangles": sc.num_triangles, "paths_per_step": paths_per_step},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import jarabotransientrendering_b200 as T
+    from jarabotransientrendering_b200 import scenes as S
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    sc = S.WORKLOADS[WORKLOAD](seed=1 + rank)
+    spp = args.spp_per_step or sc.spp
+    paths_per_step = sc.width * sc.height * spp * sc.incoming_samples
+
+    ctx = T.Context(sc, device=local)
+    stream = torch.cuda.Stream()
+    T._abi.check(T._abi.lib().tr_set_stream(ctx.h, stream.cuda_stream))
+    T._abi.check(T._abi.lib().tr_set_profiling(ctx.h, 1))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ctx.render(0, spp)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kern = {"extend_ms": 0.0, "shade_ms": 0.0, "shadow_ms": 0.0, "splat_ms": 0.0, "raygen_ms": 0.0}
+    launches = 0
+    ext_launches = 0
+    st0 = ctx.stats()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ctx.render(0, spp)
+        st = ctx.stats()
+        for k in kern:
+            kern[k] += st[k]
+        launches += st["kernel_launches"]
+        ext_launches += st["extend_launches"]
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    st1 = ctx.stats()
+    closest = st1["closest_rays"] - st0["closest_rays"]
+    shadow = st1["shadow_rays"] - st0["shadow_rays"]
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_paths = paths_per_step * args.steps * world
+    value = total_paths / (ms / 1e3)
+
+    # roofline of the dominant kernel (largest device time)
+    peak, peak_kind = peaks()
+    dom = max(("extend_ms", "shadow_ms", "shade_ms", "splat_ms"), key=lambda k: kern[k])
+    if dom == "shadow_ms":
+        achieved = shadow * B_SHADOW / (kern["shadow_ms"] / 1e3) / 1e9
+        algo_bytes = B_SHADOW
+    else:
+        achieved = closest * B_CLOSEST / (kern["extend_ms"] / 1e3) / 1e9
+        algo_bytes = B_CLOSEST
+    roofline = {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)" if dom != "shadow_ms" else
+                "k_shadow (any-hit traversal)", "dominant_by_time": dom,
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": TRAFFIC_PER_EXTEND_LAUNCH,
+                "algorithmic_bytes_per_query": algo_bytes,
+                "kernel_ms_per_step": {k: v / args.steps for k, v in kern.items()},
+                "queries_per_step": {"closest": closest / args.steps, "shadow": shadow / args.steps}}
+
+    out = {"metric": "paths/s", "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8",
+                      "triangles": sc.num_triangles, "paths_per_step": paths_per_step,
+                      "film": "FP64 [512][512][2048][3] in HBM (12.9 GB)",
+                      "l2": "film and path state larger than L2; 256 MiB write between steps",
+                      "parallelism": f"replicas x{world}"},
+           "rays_per_s": (closest + shadow) * world / (ms / 1e3),
+           "gpu_launches": launches, "clocks": clk, "roofline": roofline}
+
+    if not args.no_e2e:
+        # end to end through the C ABI with host buffers: scene upload + BVH build (tr_create),
+        # render, film read-back into pinned host memory (tr_get_film), tr_destroy
+        ctx.close()
+        del flush
+        torch.cuda.empty_cache()
+        v, t_, m = sc.flatten()
+        pv = torch.from_numpy(v).pin_memory().numpy()
+        pt = torch.from_numpy(t_).pin_memory().numpy()
+        pm = torch.from_numpy(m).pin_memory().numpy()
+        H, W, Tb = sc.height, sc.width, sc.time_bins
+        streak = torch.empty((H, W, Tb, 3), dtype=torch.float64, pin_memory=True).numpy()
+        steady = torch.empty((H, W, 3), dtype=torch.float64, pin_memory=True).numpy()
+        weight = torch.empty((H, W), dtype=torch.float64, pin_memory=True).numpy()
+        e2e_steps = max(1, min(args.steps, 3))
+        times = []
+        for i in range(e2e_steps + 1):
+            t0 = time.perf_counter()
+            c = T.Context(sc, device=local, arrays=(pv, pt, pm))
+            c.render(0, spp)
+            c.film_into(streak, steady, weight)
+            c.close()
+            times.append(time.perf_counter() - t0)
+        et = sum(times[1:]) / e2e_steps          # first iteration warms the allocator
+        out["e2e"] = {"value": paths_per_step * world / et, "unit": "paths/s",
+                      "h2d_bytes_per_step": int(pv.nbytes + pt.nbytes + pm.nbytes),
+                      "d2h_bytes_per_step": int(streak.nbytes + steady.nbytes + weight.nbytes),
+                      "ms_per_step": et * 1e3,
+                      "includes": "tr_create (scene H2D from pinned memory + host BVH build + film alloc), "
+                                  "tr_render, tr_get_film (D2H into pinned memory), tr_destroy"}
+    else:
+        ctx.close()
+
+    if rank == 0 and not args.no_cpu_baseline:
+        procs = max(1, min(os.cpu_count() or 1, 32))
+        out["cpu_baseline"] = cpu_reference(sc, 1, procs)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

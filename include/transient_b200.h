@@ -1,0 +1,219 @@
+/*
+ * transient_b200.h - C ABI of the B200 transient path tracer.
+ *
+ * The GPU path replaces the reference renderer's CPU render call
+ *   RenderEngine<D,Radiance,RadAtt>::render(name, World&, Integrator*, const Camera&,
+ *                                           Film*, Sampler*)              (src/Renderer/RenderEngine.h:67-68)
+ * as overridden by TransientRenderer::render                             (src/Renderer/TransientRenderer.h:76-201),
+ * together with the scene set-up it depends on (World::add_triangle_mesh / add_light /
+ * set_medium / freeze, src/RayTracing/World.h:209-550,695-707) and the film read-out
+ * (StreakCameraFilm::write, src/Film/StreakCameraFilm.h:233-242).
+ *
+ * Everything is plain C: flat arrays, explicit sizes, integer status codes.  No C++
+ * exception crosses this boundary; the reference's exceptions (bad mesh, missing
+ * integrator) come back as TR_ERR_INVALID_ARGUMENT with a message in tr_last_error().
+ * Calls on one context must be serialised by the caller (the reference renderer is
+ * single-threaded and not re-entrant either: src/Utils/RandomNumbers.h:227).
+ */
+#ifndef TRANSIENT_B200_H
+#define TRANSIENT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TR_ABI_VERSION 1
+
+typedef enum tr_status {
+    TR_OK = 0,
+    TR_ERR_INVALID_ARGUMENT = 1, /* bad sizes / indices / NaN geometry / unknown kinds        */
+    TR_ERR_CUDA = 2,             /* a CUDA runtime call failed (message in tr_last_error)      */
+    TR_ERR_OUT_OF_MEMORY = 3,    /* film or path state does not fit in device memory           */
+    TR_ERR_NOT_SUPPORTED = 4,    /* feature not available in this build                        */
+    TR_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up                         */
+    TR_ERR_NO_DEVICE = 6,        /* no CUDA device / wrong architecture                        */
+    TR_ERR_IO = 7                /* file could not be read or written                          */
+} tr_status;
+
+/* ---- scene description (mirrors what World owns after parse_args) ---------------------- */
+
+enum { TR_MAT_LAMBERTIAN = 0, TR_MAT_GGX = 1 };
+
+/* Lambertian: UberMaterial holding one Lambertian(Kd)      (bunnykiller.cpp:328-337,
+ *             src/Material/Reflectance/Lambertian.h:68-122)
+ * GGX:        microfacet reflector, Kd = Schlick F0, alpha = GGX roughness (no reference
+ *             counterpart; Walter et al. 2007 evaluation, Heitz 2018 visible-normal sampling). */
+typedef struct tr_material {
+    uint32_t kind;
+    float kd[3];
+    float alpha;
+    float reserved[3];
+} tr_material;
+
+enum { TR_LIGHT_POINT = 0, TR_LIGHT_RECT = 1 };
+
+/* Point light:  position, intensity                       (src/LightSource/PointLightSource.h:141-171)
+ * Rect light:   position = corner, left/up = edge vectors already scaled by the size,
+ *               normal, area; as RectangularAreaLightSource::setup builds them
+ *               (src/LightSource/RectangularAreaLightSource.h:66-80,221-248). */
+typedef struct tr_light {
+    uint32_t kind;
+    float position[3];
+    float intensity[3];
+    float left[3];
+    float up[3];
+    float normal[3];
+    float area;
+} tr_light;
+
+/* Homogeneous world medium with a Henyey-Greenstein phase function
+ * (src/Media/HomogeneousMedium.h:32-199, HenyeyGreensteinPhaseFunction.h:218-276). */
+typedef struct tr_medium {
+    uint32_t enabled;
+    float sigma_a[3];
+    float sigma_s[3];
+    float g;
+} tr_medium;
+
+typedef struct tr_scene {
+    const float* vertices;            /* [num_vertices][3]                                     */
+    uint32_t num_vertices;
+    const uint32_t* triangles;        /* [num_triangles][3], 0-based                           */
+    uint32_t num_triangles;           /* triangle id = index here (OBJ face order per mesh)    */
+    const uint32_t* triangle_material;/* [num_triangles]                                       */
+    const tr_material* materials;
+    uint32_t num_materials;
+    const tr_light* lights;
+    uint32_t num_lights;
+    tr_medium medium;
+} tr_scene;
+
+/* Pinhole camera basis as PinholeCamera builds it (src/Camera/PinholeCamera.h:56-91):
+ * direction(px,py) = normalize(nv*focal_distance + 2*uv*px - 2*vv*py). */
+typedef struct tr_camera {
+    float position[3];
+    float nv[3];
+    float uv[3];
+    float vv[3];
+    float focal_distance;
+} tr_camera;
+
+/* Streak film (src/Film/StreakCameraFilm.h:91-121): width x height pixels, time_bins bins of
+ * `exposure` path-length units starting at `offset`. */
+typedef struct tr_film {
+    uint32_t width;
+    uint32_t height;
+    uint32_t time_bins;
+    float exposure;
+    float offset;
+} tr_film;
+
+/* Unidirectional path tracing with next-event estimation, the only mode the reference CLI runs
+ * (src/Integrator/BidirectionalPathTracing.h:122-137,1099-1140; ProgramParams.h:162-164).
+ * sqrt_spp strata per axis (StratifiedSampler.h:47-89), incoming_samples paths per camera
+ * sample ("-bidirectional-path-tracing N"), max_bounces = "-max-nb-bounces". */
+typedef struct tr_integrator {
+    uint32_t max_bounces;
+    uint32_t sqrt_spp;
+    uint32_t incoming_samples;
+    uint32_t reserved;
+    uint64_t seed;
+} tr_integrator;
+
+/* ---- ray-batch interface (correctness batch of World::first_intersection / intersects) --- */
+
+/* One ray = 8 floats: origin xyz, tnear, direction xyz, tfar.                               */
+typedef struct tr_hit {
+    float t;            /* hit distance (tfar of the closest hit)                            */
+    uint32_t prim_id;   /* triangle id, 0xffffffff = miss                                    */
+    float u, v;         /* barycentrics: p = (1-u-v) p0 + u p1 + v p2                        */
+} tr_hit;
+
+#define TR_INVALID_ID 0xffffffffu
+
+typedef struct tr_stats {
+    uint64_t paths;            /* paths traced (camera samples x incoming samples)          */
+    uint64_t camera_samples;   /* camera samples accumulated into the film                  */
+    uint64_t closest_rays;     /* closest-hit queries                                        */
+    uint64_t shadow_rays;      /* any-hit (shadow) queries                                   */
+    uint64_t splats;           /* radiance samples landing inside the film window            */
+    double   render_ms;        /* device time of the last tr_render call                     */
+    double   bvh_build_ms;     /* host time of the BVH build                                 */
+    uint32_t bvh_nodes;
+    uint32_t bvh_depth;
+    uint64_t device_bytes;     /* device memory held by the context                          */
+    uint64_t kernel_launches;  /* kernels launched by the last tr_render call                */
+    /* per-kernel device time of the last tr_render call (only with tr_set_profiling(ctx,1)),
+     * measured with CUDA events around each launch on the render stream                      */
+    double   raygen_ms, extend_ms, shade_ms, shadow_ms, splat_ms;
+    uint64_t extend_launches, shadow_launches;
+} tr_stats;
+
+/* ---- lifetime ----------------------------------------------------------------------------- */
+
+typedef struct tr_ctx tr_ctx;
+
+/* Uploads the scene, builds the BVH and allocates the streak film on `device`.
+ * Replaces World::add_triangle_mesh + World::freeze and the film allocation.               */
+tr_status tr_create(const tr_scene* scene, const tr_camera* camera, const tr_film* film,
+                    const tr_integrator* integrator, int device, tr_ctx** out);
+
+/* Renders camera samples [sample_begin, sample_begin + sample_count) of every pixel and adds
+ * them to the film (the while-loop of TransientRenderer::render).  Additive: calling it for
+ * [0,a) then [a,b) equals one call for [0,b).  Camera sample s uses stratum s mod sqrt_spp^2. */
+tr_status tr_render(tr_ctx* ctx, uint64_t sample_begin, uint32_t sample_count);
+
+/* As tr_render but only for the pixel window [x0,x1) x [y0,y1) (the reference's
+ * -film-scanline / -film-single-pixel partial renders, bunnykiller.cpp:1770-1791).          */
+tr_status tr_render_region(tr_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                           uint64_t sample_begin, uint32_t sample_count);
+
+/* Zeroes film, steady image and weights. */
+tr_status tr_clear_film(tr_ctx* ctx);
+
+/* Copies the accumulated (not yet averaged) film to host memory; any pointer may be NULL.
+ *   streak: [height][width][time_bins][3] sums of radiance per time bin
+ *   steady: [height][width][3]            sums of in-window radiance (Film::m_image)
+ *   weight: [height][width]               number of camera samples (Film::m_weight)
+ * Dividing streak/steady by weight gives what StreakCameraFilm::average_and_save_slice writes. */
+tr_status tr_get_film(tr_ctx* ctx, double* streak, double* steady, double* weight);
+
+/* Same as tr_get_film but into device memory owned by the caller (no host copy). */
+tr_status tr_get_film_device(tr_ctx* ctx, double* d_streak, double* d_steady, double* d_weight);
+
+/* Writes the averaged film the way the reference does: one RGBE .hdr streak image per
+ * scanline "<name>_%04d.hdr" (time_bins x width) and the steady image "<name>.hdr"
+ * (StreakCameraFilm.h:356-437, Film.h:357-471, ImageIO.h:146-193).                           */
+tr_status tr_write_film(tr_ctx* ctx, const char* name);
+
+/* Closest-hit (any_hit = 0) or occlusion (any_hit = 1) queries for n host rays.
+ * Closest hit: smallest t in (tnear, tfar], ties broken by the lower triangle id.
+ * Occlusion: prim_id is any triangle with t in (tnear, tfar], or TR_INVALID_ID.             */
+tr_status tr_trace_rays(tr_ctx* ctx, const float* rays, uint32_t n, int any_hit, tr_hit* out);
+
+/* Same with device pointers on the caller's CUDA stream (cudaStream_t passed as void*). */
+tr_status tr_trace_rays_device(tr_ctx* ctx, const float* d_rays, uint32_t n, int any_hit,
+                               tr_hit* d_out, void* stream);
+
+tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
+
+/* Runs all later work of the context on the caller's CUDA stream (cudaStream_t as void*;
+ * NULL restores the context's own stream).  The stream must belong to the context's device. */
+tr_status tr_set_stream(tr_ctx* ctx, void* stream);
+
+/* Enables (1) or disables (0) per-kernel CUDA-event timing inside tr_render. */
+tr_status tr_set_profiling(tr_ctx* ctx, int on);
+tr_status tr_destroy(tr_ctx* ctx);
+
+const char* tr_status_string(tr_status s);
+/* Thread-local message of the last failing call on this thread. */
+const char* tr_last_error(void);
+int tr_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRANSIENT_B200_H */

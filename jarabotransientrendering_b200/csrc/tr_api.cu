@@ -1,0 +1,630 @@
+// tr_api.cu - the C ABI (include/transient_b200.h): context, scene upload, wavefront batch
+// scheduling and film read-out.  Host code; kernels live in tr_kernels.cu.
+#include "transient_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "tr_device.cuh"
+#include "tr_kernels.cuh"
+#include "tr_film_io.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+tr_status fail(tr_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* what) : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+#define TR_CUDA(call)                                           \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) throw CudaError(e_, #call);      \
+    } while (0)
+
+template <class T>
+T* dalloc(size_t count, size_t& total) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) throw CudaError(e, "cudaMalloc");
+    total += count * sizeof(T);
+    return static_cast<T*>(p);
+}
+
+constexpr uint32_t kMaxBounces = 63;            // counters hold 64 depths
+constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batch
+constexpr size_t kSplatSmemBudget = 100 * 1024;  // two splat CTAs per SM
+
+}  // namespace
+
+struct tr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    // scene
+    float4* d_nodes = nullptr;
+    float4* d_tris = nullptr;
+    float4* d_tri_ng = nullptr;
+    float4* d_mats = nullptr;
+    float4* d_mats2 = nullptr;
+    float4* d_lights = nullptr;
+    trk::SceneDev scene{};
+    uint32_t nt = 0, bvh_nodes = 0, bvh_depth = 0;
+    double bvh_ms = 0.0;
+
+    tr_camera cam{};
+    tr_film film{};
+    tr_integrator integ{};
+
+    // film
+    double* d_streak = nullptr;
+    double* d_steady = nullptr;
+    double* d_weight = nullptr;
+
+    // wavefront state
+    trk::Wave wave{};
+    int trace_grid = 0;
+    int splat_g = 1;
+
+    // ray-batch scratch
+    float* d_rays = nullptr;
+    void* d_hits = nullptr;
+    uint32_t ray_cap = 0;
+    uint32_t* d_cursor = nullptr;
+
+    tr_stats stats{};
+    cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events; // pool of timing events
+    cudaStream_t s() const { return user_stream ? user_stream : stream; }
+
+    template <class T>
+    T* alloc(size_t n) {
+        T* p = dalloc<T>(n, bytes);
+        allocs.push_back(p);
+        return p;
+    }
+    void release() {
+        for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
+        prof_events.clear();
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+        ev0 = ev1 = nullptr;
+        stream = nullptr;
+    }
+};
+
+namespace {
+
+tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, const tr_integrator* it) {
+    if (!s || !c || !f || !it) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    if (!s->vertices || !s->triangles || !s->triangle_material || s->num_triangles == 0)
+        return fail(TR_ERR_INVALID_ARGUMENT, "scene has no triangles");
+    if (s->num_materials == 0 || !s->materials) return fail(TR_ERR_INVALID_ARGUMENT, "scene has no materials");
+    if (s->num_materials > (uint32_t)trk::kMaxMaterials) return fail(TR_ERR_INVALID_ARGUMENT, "too many materials");
+    if (s->num_lights == 0 || !s->lights)
+        return fail(TR_ERR_INVALID_ARGUMENT, "scene has no light source (next-event estimation needs one)");
+    if (s->num_lights > (uint32_t)trk::kMaxLights) return fail(TR_ERR_INVALID_ARGUMENT, "too many lights");
+    for (uint32_t i = 0; i < s->num_triangles; ++i)
+        if (s->triangle_material[i] >= s->num_materials)
+            return fail(TR_ERR_INVALID_ARGUMENT, "triangle " + std::to_string(i) + " has material index out of range");
+    for (uint32_t i = 0; i < s->num_materials; ++i) {
+        const tr_material& m = s->materials[i];
+        if (m.kind != TR_MAT_LAMBERTIAN && m.kind != TR_MAT_GGX)
+            return fail(TR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has unknown kind");
+        if (m.kind == TR_MAT_GGX) return fail(TR_ERR_NOT_SUPPORTED, "GGX material is not available in this build");
+        for (float v : m.kd)
+            if (!std::isfinite(v)) return fail(TR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " albedo is not finite");
+    }
+    for (uint32_t i = 0; i < s->num_lights; ++i) {
+        const tr_light& L = s->lights[i];
+        if (L.kind != TR_LIGHT_POINT && L.kind != TR_LIGHT_RECT)
+            return fail(TR_ERR_INVALID_ARGUMENT, "light " + std::to_string(i) + " has unknown kind");
+        if (L.kind == TR_LIGHT_RECT && !(L.area > 0.0f))
+            return fail(TR_ERR_INVALID_ARGUMENT, "rectangular light " + std::to_string(i) + " has zero area");
+    }
+    if (s->medium.enabled) {
+        for (int k = 0; k < 3; ++k) {
+            if (!(s->medium.sigma_a[k] >= 0.0f) || !(s->medium.sigma_s[k] >= 0.0f))
+                return fail(TR_ERR_INVALID_ARGUMENT, "medium coefficients must be >= 0");
+        }
+        float st = (s->medium.sigma_a[0] + s->medium.sigma_s[0]) + (s->medium.sigma_a[1] + s->medium.sigma_s[1]) +
+                   (s->medium.sigma_a[2] + s->medium.sigma_s[2]);
+        if (!(st > 0.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "medium extinction must be > 0");
+        if (!(std::fabs(s->medium.g) < 1.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "HG g must be in (-1, 1)");
+    }
+    if (f->width == 0 || f->height == 0 || f->time_bins == 0)
+        return fail(TR_ERR_INVALID_ARGUMENT, "film has zero size");
+    if (!(f->exposure > 0.0f) || !std::isfinite(f->offset))
+        return fail(TR_ERR_INVALID_ARGUMENT, "film exposure must be > 0");
+    if ((uint64_t)f->width * f->height >= (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "film too large");
+    if (trk::splat_smem_bytes(f->time_bins, 1) > 220 * 1024)
+        return fail(TR_ERR_NOT_SUPPORTED, "time_bins too large for one shared-memory pixel tile");
+    if (it->sqrt_spp == 0 || it->incoming_samples == 0)
+        return fail(TR_ERR_INVALID_ARGUMENT, "sqrt_spp and incoming_samples must be >= 1");
+    if (it->max_bounces > kMaxBounces) return fail(TR_ERR_INVALID_ARGUMENT, "max_bounces must be <= 63");
+    if (!std::isfinite(c->focal_distance)) return fail(TR_ERR_INVALID_ARGUMENT, "camera focal distance not finite");
+    return TR_OK;
+}
+
+void upload(void* dst, const void* src, size_t bytes) {
+    TR_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+}
+
+void ensure_wave(tr_ctx* x, uint32_t capacity) {
+    if (x->wave.capacity >= capacity) return;
+    // grow: drop the old buffers (they are only scratch between calls)
+    auto drop = [&](void* p) {
+        if (!p) return;
+        cudaFree(p);
+        x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), p), x->allocs.end());
+    };
+    trk::Wave& w = x->wave;
+    drop(w.ray_o); drop(w.ray_d); drop(w.thr); drop(w.rng); drop(w.hit); drop(w.q[0]); drop(w.q[1]);
+    drop(w.sh_o); drop(w.sh_d); drop(w.sh_L); drop(w.rec); drop(w.rec_n);
+    const size_t R = std::max<uint32_t>(1u, x->integ.max_bounces);
+    w.ray_o = x->alloc<float4>(capacity);
+    w.ray_d = x->alloc<float4>(capacity);
+    w.thr = x->alloc<float4>(capacity);
+    w.rng = x->alloc<unsigned long long>(capacity);
+    w.hit = x->alloc<float4>(capacity);
+    w.q[0] = x->alloc<uint32_t>(capacity);
+    w.q[1] = x->alloc<uint32_t>(capacity);
+    w.sh_o = x->alloc<float4>(capacity);
+    w.sh_d = x->alloc<float4>(capacity);
+    w.sh_L = x->alloc<float4>(capacity);
+    w.rec = x->alloc<float4>((size_t)capacity * R);
+    w.rec_n = x->alloc<uint8_t>(capacity);
+    if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
+    if (!w.stats) {
+        w.stats = x->alloc<unsigned long long>(8);
+        TR_CUDA(cudaMemset(w.stats, 0, 8 * sizeof(unsigned long long)));
+    }
+    w.capacity = capacity;
+}
+
+trk::Params make_params(tr_ctx* x) {
+    trk::Params p{};
+    p.scene = x->scene;
+    for (int k = 0; k < 3; ++k) {
+        p.cam.pos[k] = x->cam.position[k]; p.cam.nv[k] = x->cam.nv[k];
+        p.cam.uv[k] = x->cam.uv[k]; p.cam.vv[k] = x->cam.vv[k];
+    }
+    p.cam.fd = x->cam.focal_distance;
+    p.film.streak = x->d_streak; p.film.steady = x->d_steady; p.film.weight = x->d_weight;
+    p.film.W = x->film.width; p.film.H = x->film.height; p.film.T = x->film.time_bins;
+    p.film.exposure = x->film.exposure; p.film.offset = x->film.offset;
+    p.wave = x->wave;
+    p.seed = x->integ.seed;
+    p.max_bounces = x->integ.max_bounces;
+    p.sqrt_spp = x->integ.sqrt_spp;
+    return p;
+}
+
+tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                        uint64_t s0, uint32_t ns_total) {
+    if (x1 > x->film.width || y1 > x->film.height || x0 >= x1 || y0 >= y1)
+        return fail(TR_ERR_INVALID_ARGUMENT, "pixel window out of range or empty");
+    if (ns_total == 0) return TR_OK;
+    if (s0 + ns_total > (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "camera sample index must stay below 2^32");
+    const uint32_t ninc = x->integ.incoming_samples;
+    const uint32_t win_w = x1 - x0, win_h = y1 - y0;
+    const uint64_t win_pix = (uint64_t)win_w * win_h;
+    const uint64_t total_slots = win_pix * (uint64_t)ns_total * ninc;
+    uint32_t cap = (uint32_t)std::min<uint64_t>(total_slots, kDefaultCapacity);
+    cap = std::max<uint32_t>(cap, ninc);
+    ensure_wave(x, cap);
+    // samples per pixel per batch, and pixels per batch
+    uint32_t ns_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(ns_total, cap / ninc));
+    cudaStream_t strm = x->s();
+    // per-kernel timing: an event before and after each launch, kind-tagged
+    struct Mark { int kind; size_t ev; };
+    std::vector<Mark> marks;
+    size_t next_ev = 0;
+    auto ev_get = [&]() -> cudaEvent_t {
+        if (next_ev == x->prof_events.size()) {
+            cudaEvent_t e;
+            TR_CUDA(cudaEventCreate(&e));
+            x->prof_events.push_back(e);
+        }
+        return x->prof_events[next_ev++];
+    };
+    auto timed = [&](int kind, auto&& launch) {
+        if (!x->profiling) { TR_CUDA(launch()); return; }
+        size_t a = next_ev;
+        TR_CUDA(cudaEventRecord(ev_get(), strm));
+        TR_CUDA(launch());
+        TR_CUDA(cudaEventRecord(ev_get(), strm));
+        marks.push_back({kind, a});
+    };
+    uint64_t launches = 0, ext_l = 0, sh_l = 0;
+    TR_CUDA(cudaEventRecord(x->ev0, strm));
+    for (uint64_t sb = 0; sb < ns_total; sb += ns_chunk) {
+        const uint32_t ns = (uint32_t)std::min<uint64_t>(ns_chunk, ns_total - sb);
+        const uint32_t per_pix = ns * ninc;
+        const uint32_t ppb = std::max<uint32_t>(1u, cap / per_pix);
+        for (uint64_t pb = 0; pb < win_pix; pb += ppb) {
+            const uint32_t npix = (uint32_t)std::min<uint64_t>(ppb, win_pix - pb);
+            trk::Params p = make_params(x);
+            p.batch.win_x0 = x0; p.batch.win_y0 = y0; p.batch.win_w = win_w;
+            p.batch.pix_begin = (uint32_t)pb; p.batch.npix = npix;
+            p.batch.s0 = s0 + sb; p.batch.ns = ns; p.batch.ninc = ninc;
+            p.batch.n_slots = npix * per_pix;
+            TR_CUDA(cudaMemsetAsync(x->wave.counters, 0, trk::kCounters * sizeof(uint32_t), strm));
+            timed(0, [&] { return trk::launch_raygen(p, strm); });
+            for (uint32_t d = 0; d < x->integ.max_bounces; ++d) {
+                timed(1, [&] { return trk::launch_extend(p, (int)d, x->trace_grid, strm); });
+                timed(2, [&] { return trk::launch_shade(p, (int)d, strm); });
+                timed(3, [&] { return trk::launch_shadow(p, (int)d, x->trace_grid, strm); });
+            }
+            timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm); });
+            launches += 2 + 3ull * x->integ.max_bounces;
+            ext_l += x->integ.max_bounces;
+            sh_l += x->integ.max_bounces;
+        }
+    }
+    TR_CUDA(cudaEventRecord(x->ev1, strm));
+    TR_CUDA(cudaEventSynchronize(x->ev1));
+    float ms = 0.f;
+    TR_CUDA(cudaEventElapsedTime(&ms, x->ev0, x->ev1));
+    double kms[5] = {0, 0, 0, 0, 0};
+    for (const Mark& m : marks) {
+        float e = 0.f;
+        TR_CUDA(cudaEventElapsedTime(&e, x->prof_events[m.ev], x->prof_events[m.ev + 1]));
+        kms[m.kind] += e;
+    }
+    x->stats.raygen_ms = kms[0]; x->stats.extend_ms = kms[1]; x->stats.shade_ms = kms[2];
+    x->stats.shadow_ms = kms[3]; x->stats.splat_ms = kms[4];
+    x->stats.kernel_launches = launches;
+    x->stats.extend_launches = ext_l;
+    x->stats.shadow_launches = sh_l;
+    unsigned long long st[8];
+    TR_CUDA(cudaMemcpy(st, x->wave.stats, sizeof(st), cudaMemcpyDeviceToHost));
+    x->stats.closest_rays = st[0];
+    x->stats.shadow_rays = st[1];
+    x->stats.splats = st[2];
+    x->stats.paths += total_slots;
+    x->stats.camera_samples += win_pix * ns_total;
+    x->stats.render_ms = ms;
+    return TR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tr_abi_version(void) { return TR_ABI_VERSION; }
+
+const char* tr_status_string(tr_status s) {
+    switch (s) {
+        case TR_OK: return "ok";
+        case TR_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case TR_ERR_CUDA: return "CUDA error";
+        case TR_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case TR_ERR_NOT_SUPPORTED: return "not supported";
+        case TR_ERR_TIMEOUT: return "device wait timed out";
+        case TR_ERR_NO_DEVICE: return "no usable CUDA device";
+        case TR_ERR_IO: return "I/O error";
+    }
+    return "unknown status";
+}
+
+const char* tr_last_error(void) { return g_last_error.c_str(); }
+
+tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, const tr_integrator* it,
+                    int device, tr_ctx** out) {
+    if (!out) return fail(TR_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    tr_status v = validate(s, c, f, it);
+    if (v != TR_OK) return v;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(TR_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(TR_ERR_NO_DEVICE, "device index out of range");
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, device);
+    if (prop.major != 10) return fail(TR_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+    tr_ctx* x = new (std::nothrow) tr_ctx();
+    if (!x) return fail(TR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    try {
+        x->device = device;
+        TR_CUDA(cudaSetDevice(device));
+        TR_CUDA(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+        TR_CUDA(cudaEventCreate(&x->ev0));
+        TR_CUDA(cudaEventCreate(&x->ev1));
+        x->cam = *c; x->film = *f; x->integ = *it;
+        x->nt = s->num_triangles;
+
+        // BVH (replaces World::freeze -> rtcCommit)
+        trh::BvhBuildResult bvh;
+        std::string msg;
+        if (!trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg)) {
+            delete x;
+            return fail(TR_ERR_INVALID_ARGUMENT, msg);
+        }
+        if (bvh.depth + 1 >= (uint32_t)trk::kStack) {
+            delete x;
+            return fail(TR_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
+        }
+        x->bvh_nodes = (uint32_t)bvh.nodes.size();
+        x->bvh_depth = bvh.depth;
+        x->bvh_ms = bvh.build_ms;
+        x->d_nodes = x->alloc<float4>(bvh.nodes.size() * 4);
+        upload(x->d_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode));
+        x->d_tris = x->alloc<float4>(bvh.tris.size() * 3);
+        upload(x->d_tris, bvh.tris.data(), bvh.tris.size() * sizeof(trh::GpuTri));
+
+        // per-triangle reference geometric normal normalize(cross(p2-p0, p1-p0)) (World.h:449)
+        std::vector<float4> ng(s->num_triangles);
+        for (uint32_t t = 0; t < s->num_triangles; ++t) {
+            const uint32_t* tri = &s->triangles[3 * (size_t)t];
+            const float* a = &s->vertices[3 * (size_t)tri[0]];
+            const float* b = &s->vertices[3 * (size_t)tri[1]];
+            const float* cc = &s->vertices[3 * (size_t)tri[2]];
+            trd::f3 p0 = trd::mk(a[0], a[1], a[2]), p1 = trd::mk(b[0], b[1], b[2]), p2 = trd::mk(cc[0], cc[1], cc[2]);
+            trd::f3 n = trd::normalize(trd::cross(p2 - p0, p1 - p0));
+            uint32_t mi = s->triangle_material[t];
+            float mf;
+            std::memcpy(&mf, &mi, 4);
+            ng[t] = make_float4(n.x, n.y, n.z, mf);
+        }
+        x->d_tri_ng = x->alloc<float4>(ng.size());
+        upload(x->d_tri_ng, ng.data(), ng.size() * sizeof(float4));
+
+        std::vector<float4> mats(s->num_materials), mats2(s->num_materials);
+        for (uint32_t i = 0; i < s->num_materials; ++i) {
+            const tr_material& m = s->materials[i];
+            float kf;
+            std::memcpy(&kf, &m.kind, 4);
+            mats[i] = make_float4(m.kd[0], m.kd[1], m.kd[2], kf);
+            mats2[i] = make_float4(m.alpha, 0.f, 0.f, 0.f);
+        }
+        x->d_mats = x->alloc<float4>(mats.size());
+        upload(x->d_mats, mats.data(), mats.size() * sizeof(float4));
+        x->d_mats2 = x->alloc<float4>(mats2.size());
+        upload(x->d_mats2, mats2.data(), mats2.size() * sizeof(float4));
+
+        std::vector<float4> lights(5 * (size_t)s->num_lights);
+        for (uint32_t i = 0; i < s->num_lights; ++i) {
+            const tr_light& L = s->lights[i];
+            float kf;
+            std::memcpy(&kf, &L.kind, 4);
+            lights[5 * i + 0] = make_float4(L.position[0], L.position[1], L.position[2], kf);
+            lights[5 * i + 1] = make_float4(L.intensity[0], L.intensity[1], L.intensity[2], L.area);
+            lights[5 * i + 2] = make_float4(L.left[0], L.left[1], L.left[2], 0.f);
+            lights[5 * i + 3] = make_float4(L.up[0], L.up[1], L.up[2], 0.f);
+            lights[5 * i + 4] = make_float4(L.normal[0], L.normal[1], L.normal[2], 0.f);
+        }
+        x->d_lights = x->alloc<float4>(lights.size());
+        upload(x->d_lights, lights.data(), lights.size() * sizeof(float4));
+
+        trk::SceneDev& sc = x->scene;
+        sc.nodes = x->d_nodes; sc.tris = x->d_tris; sc.tri_ng = x->d_tri_ng;
+        sc.mats = x->d_mats; sc.mats2 = x->d_mats2; sc.lights = x->d_lights;
+        sc.num_lights = s->num_lights;
+        sc.medium = s->medium.enabled ? 1u : 0u;
+        if (sc.medium) {
+            trd::f3 st = trd::mk(s->medium.sigma_a[0] + s->medium.sigma_s[0], s->medium.sigma_a[1] + s->medium.sigma_s[1],
+                                 s->medium.sigma_a[2] + s->medium.sigma_s[2]);
+            for (int k = 0; k < 3; ++k) { sc.sig_s[k] = s->medium.sigma_s[k]; sc.sig_t[k] = trd::comp(st, k); }
+            sc.lambda = trd::avg3(st);
+            sc.g = s->medium.g;
+        }
+
+        // film: [H][W][T][3] + steady + weights, double precision, zeroed
+        const size_t nstreak = (size_t)f->width * f->height * f->time_bins * 3u;
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        if (nstreak * sizeof(double) + ((size_t)2 << 30) > free_b) {
+            x->release();
+            delete x;
+            return fail(TR_ERR_OUT_OF_MEMORY, "streak film of " + std::to_string(nstreak * 8 >> 20) +
+                                                  " MiB does not fit in free device memory");
+        }
+        x->d_streak = x->alloc<double>(nstreak);
+        x->d_steady = x->alloc<double>((size_t)f->width * f->height * 3u);
+        x->d_weight = x->alloc<double>((size_t)f->width * f->height);
+        TR_CUDA(cudaMemsetAsync(x->d_streak, 0, nstreak * sizeof(double), x->stream));
+        TR_CUDA(cudaMemsetAsync(x->d_steady, 0, (size_t)f->width * f->height * 3u * sizeof(double), x->stream));
+        TR_CUDA(cudaMemsetAsync(x->d_weight, 0, (size_t)f->width * f->height * sizeof(double), x->stream));
+
+        x->trace_grid = trk::trace_grid_size(device);
+        int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
+        x->splat_g = std::max(1, std::min(g, 16));
+        x->d_cursor = x->alloc<uint32_t>(1);
+        TR_CUDA(cudaStreamSynchronize(x->stream));
+
+        x->stats.bvh_build_ms = x->bvh_ms;
+        x->stats.bvh_nodes = x->bvh_nodes;
+        x->stats.bvh_depth = x->bvh_depth;
+    } catch (const CudaError& e) {
+        x->release();
+        delete x;
+        return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        x->release();
+        delete x;
+        return fail(TR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    *out = x;
+    return TR_OK;
+}
+
+tr_status tr_render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                           uint64_t sample_begin, uint32_t sample_count) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        return render_region(x, x0, y0, x1, y1, sample_begin, sample_count);
+    } catch (const CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
+    }
+}
+
+tr_status tr_render(tr_ctx* x, uint64_t sample_begin, uint32_t sample_count) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    return tr_render_region(x, 0, 0, x->film.width, x->film.height, sample_begin, sample_count);
+}
+
+tr_status tr_clear_film(tr_ctx* x) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        const size_t npix = (size_t)x->film.width * x->film.height;
+        TR_CUDA(cudaMemsetAsync(x->d_streak, 0, npix * x->film.time_bins * 3u * sizeof(double), x->s()));
+        TR_CUDA(cudaMemsetAsync(x->d_steady, 0, npix * 3u * sizeof(double), x->s()));
+        TR_CUDA(cudaMemsetAsync(x->d_weight, 0, npix * sizeof(double), x->s()));
+        TR_CUDA(cudaStreamSynchronize(x->s()));
+        x->stats.camera_samples = 0;
+        x->stats.paths = 0;
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+static tr_status copy_film(tr_ctx* x, double* streak, double* steady, double* weight, cudaMemcpyKind kind) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        TR_CUDA(cudaStreamSynchronize(x->s()));
+        const size_t npix = (size_t)x->film.width * x->film.height;
+        if (streak) TR_CUDA(cudaMemcpy(streak, x->d_streak, npix * x->film.time_bins * 3u * sizeof(double), kind));
+        if (steady) TR_CUDA(cudaMemcpy(steady, x->d_steady, npix * 3u * sizeof(double), kind));
+        if (weight) TR_CUDA(cudaMemcpy(weight, x->d_weight, npix * sizeof(double), kind));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+tr_status tr_get_film(tr_ctx* x, double* streak, double* steady, double* weight) {
+    return copy_film(x, streak, steady, weight, cudaMemcpyDeviceToHost);
+}
+
+tr_status tr_get_film_device(tr_ctx* x, double* streak, double* steady, double* weight) {
+    return copy_film(x, streak, steady, weight, cudaMemcpyDeviceToDevice);
+}
+
+tr_status tr_write_film(tr_ctx* x, const char* name) {
+    if (!x || !name) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    const size_t npix = (size_t)x->film.width * x->film.height;
+    std::vector<double> streak, steady(npix * 3), weight(npix);
+    try {
+        streak.resize(npix * x->film.time_bins * 3u);
+    } catch (const std::bad_alloc&) {
+        return fail(TR_ERR_OUT_OF_MEMORY, "host film buffer");
+    }
+    tr_status st = tr_get_film(x, streak.data(), steady.data(), weight.data());
+    if (st != TR_OK) return st;
+    std::string err;
+    if (!trio::write_streak_film(name, x->film.width, x->film.height, x->film.time_bins, streak.data(),
+                                 steady.data(), weight.data(), &err))
+        return fail(TR_ERR_IO, err);
+    return TR_OK;
+}
+
+tr_status tr_trace_rays_device(tr_ctx* x, const float* d_rays, uint32_t n, int any_hit, tr_hit* d_out, void* stream) {
+    if (!x || (!d_rays && n) || (!d_out && n)) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return TR_OK;
+    if ((reinterpret_cast<uintptr_t>(d_rays) & 15u) != 0) return fail(TR_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : x->s();
+        TR_CUDA(cudaMemsetAsync(x->d_cursor, 0, sizeof(uint32_t), s));
+        TR_CUDA(trk::launch_trace_user(x->scene, d_rays, n, any_hit, d_out, x->d_cursor, x->trace_grid, s));
+        x->stats.closest_rays += any_hit ? 0 : n;
+        x->stats.shadow_rays += any_hit ? n : 0;
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+tr_status tr_trace_rays(tr_ctx* x, const float* rays, uint32_t n, int any_hit, tr_hit* out) {
+    if (!x || (!rays && n) || (!out && n)) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return TR_OK;
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        if (x->ray_cap < n) {
+            auto drop = [&](void* p) {
+                if (!p) return;
+                cudaFree(p);
+                x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), p), x->allocs.end());
+            };
+            drop(x->d_rays); drop(x->d_hits);
+            x->d_rays = x->alloc<float>((size_t)n * 8);
+            x->d_hits = x->alloc<tr_hit>(n);
+            x->ray_cap = n;
+        }
+        cudaStream_t strm = x->s();
+        TR_CUDA(cudaMemcpyAsync(x->d_rays, rays, (size_t)n * 8 * sizeof(float), cudaMemcpyHostToDevice, strm));
+        tr_status st = tr_trace_rays_device(x, x->d_rays, n, any_hit, static_cast<tr_hit*>(x->d_hits), strm);
+        if (st != TR_OK) return st;
+        TR_CUDA(cudaMemcpyAsync(out, x->d_hits, (size_t)n * sizeof(tr_hit), cudaMemcpyDeviceToHost, strm));
+        TR_CUDA(cudaStreamSynchronize(strm));
+    } catch (const CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+tr_status tr_stats_get(tr_ctx* x, tr_stats* out) {
+    if (!x || !out) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    *out = x->stats;
+    out->device_bytes = x->bytes;
+    return TR_OK;
+}
+
+tr_status tr_set_stream(tr_ctx* x, void* stream) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        TR_CUDA(cudaStreamSynchronize(x->s()));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    x->user_stream = static_cast<cudaStream_t>(stream);
+    return TR_OK;
+}
+
+tr_status tr_set_profiling(tr_ctx* x, int on) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    x->profiling = on != 0;
+    return TR_OK;
+}
+
+tr_status tr_destroy(tr_ctx* x) {
+    if (!x) return TR_OK;
+    cudaSetDevice(x->device);
+    cudaStreamSynchronize(x->s());
+    if (x->stream) cudaStreamSynchronize(x->stream);
+    x->release();
+    delete x;
+    return TR_OK;
+}
+
+}  // extern "C"

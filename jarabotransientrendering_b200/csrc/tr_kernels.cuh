@@ -1,0 +1,99 @@
+// tr_kernels.cuh - parameters shared by the host scheduler and the wavefront kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace trk {
+
+constexpr int kStack = 64;          // per-thread traversal stack entries (shared memory)
+constexpr int kTraceBlock = 128;    // threads per traversal block
+constexpr int kMaxLights = 64;
+constexpr int kMaxMaterials = 256;
+
+// Scene as the kernels see it (device pointers).
+struct SceneDev {
+    const float4* nodes;      // 4 float4 per two-child node
+    const float4* tris;       // 3 float4 per triangle, leaf order (v0.w = triangle id)
+    const float4* tri_ng;     // per triangle id: geometric normal xyz, material index (bits)
+    const float4* mats;       // per material: kd.rgb, kind (bits)
+    const float4* mats2;      // per material: alpha, 0, 0, 0
+    const float4* lights;     // 5 float4 per light: (pos, kind) (I, area) (left,0) (up,0) (normal,0)
+    uint32_t num_lights;
+    uint32_t medium;          // 0/1
+    float sig_s[3], sig_t[3];
+    float lambda;             // mean extinction avg(sigma_t)
+    float g;
+};
+
+struct CameraDev {
+    float pos[3], nv[3], uv[3], vv[3], fd;
+};
+
+// One wavefront batch: pixels [0, npix) of a pixel list (window rows, row-major) times
+// camera samples [s0, s0+ns) times incoming samples [0, ninc).
+// slot = ((pixel_local * ns) + s_local) * ninc + j
+struct Batch {
+    uint32_t win_x0, win_y0, win_w;     // pixel list = window rows, row-major
+    uint32_t pix_begin;                 // first window-local pixel index of this batch
+    uint32_t npix;
+    unsigned long long s0;
+    uint32_t ns, ninc;
+    uint32_t n_slots;
+};
+
+struct Wave {
+    float4* ray_o;            // o.xyz, tfar (sampled free-flight distance or +inf)
+    float4* ray_d;            // d.xyz, accumulated time
+    float4* thr;              // throughput rgb, pending pdf factor (RR prob * direction pdf)
+    unsigned long long* rng;  // PCG32 state (increment derived from the camera sample)
+    float4* hit;              // t, triangle id (bits), u, v
+    uint32_t* q[2];           // extend queues (ping-pong)
+    float4* sh_o;             // shadow: origin, tfar
+    float4* sh_d;             // shadow: direction, time bin (bits)
+    float4* sh_L;             // shadow: contribution rgb, slot (bits)
+    float4* rec;              // splat records [slot][max_bounces]: rgb, bin (bits)
+    uint8_t* rec_n;           // records per slot
+    uint32_t* counters;       // see counter_* helpers below
+    unsigned long long* stats;// closest, shadow, splats, paths (accumulated)
+    uint32_t capacity;
+};
+
+struct FilmDev {
+    double* streak;           // [H][W][T][3]
+    double* steady;           // [H][W][3]
+    double* weight;           // [H][W]
+    uint32_t W, H, T;
+    float exposure, offset;
+};
+
+struct Params {
+    SceneDev scene;
+    CameraDev cam;
+    FilmDev film;
+    Wave wave;
+    Batch batch;
+    unsigned long long seed;
+    uint32_t max_bounces;
+    uint32_t sqrt_spp;
+};
+
+// counters layout (uint32): [0, 64) extend counts per depth, [64, 128) shadow counts per
+// depth, [128, 192) extend fetch cursors, [192, 256) shadow fetch cursors.
+constexpr int kCounters = 256;
+__host__ __device__ constexpr int cnt_ext(int d) { return d; }
+__host__ __device__ constexpr int cnt_sh(int d) { return 64 + d; }
+__host__ __device__ constexpr int cur_ext(int d) { return 128 + d; }
+__host__ __device__ constexpr int cur_sh(int d) { return 192 + d; }
+
+// host launchers (tr_kernels.cu)
+cudaError_t launch_raygen(const Params& p, cudaStream_t s);
+cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s);
+cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s);
+cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
+cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s);
+cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
+                              void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);
+int trace_grid_size(int device);
+size_t splat_smem_bytes(uint32_t T, int pixels_per_cta);
+
+}  // namespace trk

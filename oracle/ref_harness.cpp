@@ -1,0 +1,215 @@
+/*
+ * ref_harness.cpp - runs the reference renderer's own transient path tracer on a scene file.
+ *
+ * TEST INFRASTRUCTURE ONLY (oracle/): built by `make -C oracle ref` into oracle/_ref/ from the
+ * reference's header sources where they lie; it is the statistical pin of the CPU oracle and
+ * the CPU baseline of bench.py.  Nothing in the product links it.
+ *
+ * Everything on the sampling path is the reference's code: World (non-Embree backend),
+ * PinholeCamera, StratifiedSampler, BidirectionalPathTracing in path-tracing-only steady-state
+ * mode, UberMaterial+Lambertian, PointLightSource, RectangularAreaLightSource,
+ * HomogeneousMedium with Henyey-Greenstein / isotropic phase, TransientRenderer::render.
+ * Set-up follows main() (src/bunnykiller.cpp:1504-1827).  Two pieces are the harness's own:
+ *   - triangles are the reference's smooth Triangle (src/Geometry/Primitives/3D/Triangle.h)
+ *     with all three shading normals = the Embree geometric normal
+ *     normalize(cross(p2-p0, p1-p0)) (src/RayTracing/World.h:449,514-540), placed in the
+ *     reference's BVH (src/Geometry/Aggregate/BVH.h), because the Embree backend needs
+ *     CMake-generated headers;
+ *   - the film is a StreakCameraFilm whose add_samples (StreakCameraFilm.h:139-192) is
+ *     overridden to accumulate the same (pixel, bin) sums in double precision into one
+ *     buffer instead of averaging and writing RGBE scanlines.
+ *
+ * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
+ *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
+ *   streak [H][W][T][3] (unless --no-streak), steady [H][W][3], weight [H][W].
+ *   Prints one JSON line with paths, seconds and paths/s on stdout.
+ */
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "Utils/RandomNumbers.h"
+#include "Camera/PinholeCamera.h"
+#include "RayTracing/World.h"
+#include "Renderer/TransientRenderer.h"
+#include "Film/StreakCameraFilm.h"
+#include "Geometry/Primitives/3D/Triangle.h"
+#include "Geometry/Aggregate/BVH.h"
+#include "Geometry/ObjectPointer.h"
+#include "Material/UberMaterial.h"
+#include "Material/Reflectance/Lambertian.h"
+#include "LightSource/PointLightSource.h"
+#include "LightSource/RectangularAreaLightSource.h"
+#include "Sampling/StratifiedSampler.h"
+#include "Integrator/BidirectionalPathTracing.h"
+#include "Media/HomogeneousMedium.h"
+#include "Media/PhaseFunction/IsotropicPhaseFunction.h"
+#include "Media/PhaseFunction/HenyeyGreensteinPhaseFunction.h"
+
+typedef Spectrum Radiance;
+typedef Spectrum RadianceAttenuation;
+
+class AccumStreakFilm : public StreakCameraFilm<3, Radiance> {
+    using Base = StreakCameraFilm<3, Radiance>;
+public:
+    unsigned W, H, T;
+    Real exposure, offset;
+    std::vector<double> streak, steady, weight;
+    bool keep_streak;
+    AccumStreakFilm(unsigned w, unsigned h, unsigned t, Real exp_, Real off, bool ks)
+        : Base(w, h, t, exp_, false, nullptr), W(w), H(h), T(t), exposure(exp_), offset(off),
+          keep_streak(ks) {
+        if (off > 0) this->set_offset(off);
+        if (ks) streak.assign((size_t)h * w * t * 3, 0.0);
+        steady.assign((size_t)h * w * 3, 0.0);
+        weight.assign((size_t)h * w, 0.0);
+    }
+    /* StreakCameraFilm::add_samples with the box filter of size 1 (weight 1, one pixel): */
+    void add_samples(const Sample& sample, const RadianceSampleRecordVector<3, Radiance>& rec) override {
+        unsigned x = (unsigned)std::floor(sample.position[0]);
+        unsigned y = (unsigned)std::floor(sample.position[1]);
+        size_t pix = (size_t)y * W + x;
+        weight[pix] += sample.weight;
+        for (const RadianceSample<3, Radiance>& r : rec.samples) {
+            Real pos_sensor = (r.time - offset) / exposure;
+            if (!(pos_sensor < T && pos_sensor >= 0.0)) continue;
+            size_t t = (size_t)std::floor(pos_sensor);
+            for (int c = 0; c < 3; ++c) {
+                if (keep_streak) streak[(pix * T + t) * 3 + c] += (double)r.radiance[c];
+                steady[pix * 3 + c] += (double)r.radiance[c];
+            }
+        }
+    }
+    void write(const char*) override {}
+};
+
+static void fail(const char* m) { fprintf(stderr, "ref_render: %s\n", m); exit(2); }
+
+int main(int argc, char** argv) {
+    if (argc < 3) fail("usage: ref_render SCENE OUT [y0 y1] [--no-streak]");
+    bool keep_streak = true;
+    int y0 = -1, y1 = -1;
+    std::vector<std::string> pos;
+    for (int i = 3; i < argc; ++i) {
+        if (!strcmp(argv[i], "--no-streak")) keep_streak = false;
+        else pos.push_back(argv[i]);
+    }
+    if (pos.size() >= 2) { y0 = atoi(pos[0].c_str()); y1 = atoi(pos[1].c_str()); }
+
+    std::ifstream in(argv[1]);
+    if (!in) fail("cannot open scene");
+    std::string tag;
+    unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1;
+    Real exposure = 0, offset = 0, fov = 40;
+    unsigned long long seed = 1;
+    Vector3 cpos, cfoc, cup;
+    int med_on = 0; float sa[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, g = 0;
+    std::vector<UberMaterial3D*> mats;
+    World<3, Radiance> w;
+    BVH<Object3DPointer, 3>* bvh = new BVH<Object3DPointer, 3>();
+    std::vector<std::string> light_lines;
+    while (in >> tag) {
+        if (tag == "film") { in >> W >> H >> T >> exposure >> offset; }
+        else if (tag == "camera") {
+            float a[9]; for (float& v : a) in >> v; in >> fov;
+            cpos = Vector3(a[0], a[1], a[2]); cfoc = Vector3(a[3], a[4], a[5]); cup = Vector3(a[6], a[7], a[8]);
+        } else if (tag == "integrator") { in >> maxb >> sqrt_spp >> ninc >> seed; }
+        else if (tag == "medium") { in >> med_on >> sa[0] >> sa[1] >> sa[2] >> ss[0] >> ss[1] >> ss[2] >> g; }
+        else if (tag == "material") {
+            unsigned kind; float kd[3], alpha; in >> kind >> kd[0] >> kd[1] >> kd[2] >> alpha;
+            if (kind != 0) fail("the reference has no GGX material");
+            UberMaterial3D* um = new UberMaterial3D();     /* bunnykiller.cpp:328-337 */
+            um->add_bsdf(new Lambertian3D(Spectrum(kd[0], kd[1], kd[2])));
+            mats.push_back(um);
+        } else if (tag == "light") { std::string l; std::getline(in, l); light_lines.push_back(l); }
+        else if (tag == "mesh") {
+            size_t nv, nt; unsigned m; in >> nv >> nt >> m;
+            if (m >= mats.size()) fail("bad material index");
+            std::vector<Vector3f> v(nv);
+            for (size_t i = 0; i < nv; ++i) { float a, b, c; in >> a >> b >> c; v[i] = Vector3f(a, b, c); }
+            for (size_t i = 0; i < nt; ++i) {
+                size_t a, b, c; in >> a >> b >> c;
+                Vector3f p0 = v[a], p1 = v[b], p2 = v[c];
+                Vector3f ngf = cross(p2 - p0, p1 - p0).normalized();      /* World.h:449 */
+                Vector3 ng(ngf[0], ngf[1], ngf[2]);
+                Vector2 uv0(0., 0.);
+                Triangle* tri = new Triangle(Vector3(p0[0], p0[1], p0[2]), ng, uv0,
+                                             Vector3(p1[0], p1[1], p1[2]), ng, uv0,
+                                             Vector3(p2[0], p2[1], p2[2]), ng, uv0, mats[m]);
+                bvh->add_primitive(Object3DPointer(tri));
+            }
+        } else if (tag == "end") break;
+        else fail("unknown tag");
+    }
+    for (const std::string& l : light_lines) {
+        std::istringstream ls(l);
+        std::string kind; ls >> kind;
+        if (kind == "point") {
+            float p[3], I[3]; ls >> p[0] >> p[1] >> p[2] >> I[0] >> I[1] >> I[2];
+            w.add_light(new PointLightSource<3, Radiance>(&w, Vector3(p[0], p[1], p[2]), Radiance(I[0], I[1], I[2])));
+        } else if (kind == "rect") {
+            float p[3], t[3], sz[2], I; ls >> p[0] >> p[1] >> p[2] >> t[0] >> t[1] >> t[2] >> sz[0] >> sz[1] >> I;
+            Vector3 pp(p[0], p[1], p[2]), tt(t[0], t[1], t[2]);          /* bunnykiller.cpp:1242-1262 */
+            w.add_light(new RectangularAreaLightSource<Radiance>(&w, pp, (tt - pp).normalized(),
+                                                                 Vector2(sz[0], sz[1]), Radiance(I), nullptr));
+        } else fail("unknown light");
+    }
+    if (med_on) {                                                       /* bunnykiller.cpp:184-227 */
+        Spectrum a(sa[0], sa[1], sa[2]), s(ss[0], ss[1], ss[2]);
+        if (g == 0.f)
+            w.set_medium(new HomogeneousMedium<3, PhaseFunction::Isotropic<3>>(a, s, PhaseFunction::Isotropic<3>(0.)));
+        else
+            w.set_medium(new HomogeneousMedium<3, PhaseFunction::HenyeyGreenstein<3>>(a, s,
+                         PhaseFunction::HenyeyGreenstein<3>(g, 0.)));
+    }
+    bvh->freeze();
+    w.add_object(Object3DPointer(bvh));
+    w.set_background(Spectrum(0.));
+    w.freeze();
+
+    Real fovr = M_PI / 180. * fov / 2;                                   /* bunnykiller.cpp:1156-1161 */
+    Real fd = 1. / tan(fovr);
+    PinholeCamera camera(cpos, cfoc, cup, fd);
+    AccumStreakFilm film(W, H, T, exposure, offset, keep_streak);
+    StratifiedSampler sampler(W, H, sqrt_spp, true);
+    TransientRenderer<3, Radiance, RadianceAttenuation> engine(nullptr, false);
+    Random::StdRNG.seed(seed);                                           /* bunnykiller.cpp:1794 */
+    BidirectionalPathTracing<3, Radiance, RadianceAttenuation> bpt(w, ninc, nullptr, &film);
+    bpt.set_max_path_size(maxb);
+    bpt.set_path_tracing_only(true);
+    bpt.set_scattering_components(Scattering::ALL);
+    bpt.set_mode(BidirectionalPathTracing<3, Radiance, RadianceAttenuation>::SamplingMode::SteadyState);
+
+    FILE* devnull = freopen("/dev/null", "w", stdout);   /* the renderer prints progress */
+    (void)devnull;
+    auto t0 = std::chrono::steady_clock::now();
+    unsigned long long paths = 0;
+    if (y0 >= 0) {
+        for (int y = y0; y < y1; ++y) {
+            sampler.set_scanline(y);                                     /* -film-scanline, :1782-1791 */
+            engine.render("ref", w, &bpt, camera, &film, &sampler);
+            paths += (unsigned long long)W * sqrt_spp * sqrt_spp * ninc;
+        }
+    } else {
+        engine.render("ref", w, &bpt, camera, &film, &sampler);
+        paths = (unsigned long long)W * H * sqrt_spp * sqrt_spp * ninc;
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    double secs = std::chrono::duration<double>(t1 - t0).count();
+    FILE* out = fopen(argv[2], "wb");
+    if (!out) fail("cannot write output");
+    if (keep_streak) fwrite(film.streak.data(), sizeof(double), film.streak.size(), out);
+    fwrite(film.steady.data(), sizeof(double), film.steady.size(), out);
+    fwrite(film.weight.data(), sizeof(double), film.weight.size(), out);
+    fclose(out);
+    FILE* tty = fopen("/dev/stderr", "w");
+    fprintf(tty, "{\"paths\": %llu, \"seconds\": %.6f, \"paths_per_s\": %.3f}\n", paths, secs, paths / secs);
+    fclose(tty);
+    return 0;
+}

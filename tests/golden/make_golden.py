@@ -1,0 +1,53 @@
+"""Generate the golden fixtures of tests/golden/ from the reference renderer itself.
+
+Runs oracle/_ref/ref_render (the reference's own integrator, sampler, camera, lights, media
+and streak film, compiled from the reference sources by oracle/Makefile) on small seeded
+scenes with K independent seeds and stores per-bin mean and standard error of the streak
+film, plus per-seed total energy.  Needs the reference sources (only in the build
+container); the committed .npz files are what the tests read.
+
+    python tests/golden/make_golden.py            # writes tests/golden/ref_*.npz
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from jarabotransientrendering_b200 import scenes as S  # noqa: E402
+from oracle import refscene  # noqa: E402
+
+K = 96
+
+
+def golden_scenes():
+    """Small variants of the benchmark workloads (light 0.2 below the ceiling so that the
+    per-bin variance has no near-singular ceiling hot spot)."""
+    c = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
+    c.lights[0].position = (0.5, 0.8, 0.5)
+    m = S.medium(width=12, height=12, time_bins=48, exposure=0.15, sqrt_spp=8, incoming_samples=1,
+                 max_bounces=12)
+    m.lights[0].position = (0.5, 0.8, 0.5)
+    a = S.guided(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6,
+                 lambertian_floor=True)
+    a.lights = [S.rect_light((0.6, 0.8, 0.6), (0.6, 0.0, 0.6), (0.2, 0.2), 4.0)]
+    return {"cornell": c, "medium": m, "arealight": a}
+
+
+def main():
+    if not refscene.build_ref():
+        raise SystemExit("reference sources not available: cannot build oracle/_ref/ref_render")
+    for name, sc in golden_scenes().items():
+        films = np.array([refscene.render(sc, seed=s)["streak"] for s in range(1, K + 1)])
+        mean = films.mean(0)
+        se = films.std(0, ddof=1) / np.sqrt(K)
+        energy = films.sum(axis=(1, 2, 3, 4))
+        out = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}.npz")
+        np.savez_compressed(out, mean=mean.astype(np.float32), se=se.astype(np.float32), energy=energy, k=K)
+        print(name, out, "energy %.4f +- %.4f" % (energy.mean(), energy.std(ddof=1) / np.sqrt(K)))
+
+
+if __name__ == "__main__":
+    main()

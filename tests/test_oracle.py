@@ -1,0 +1,172 @@
+"""CPU oracle checks (no GPU): math kernels, the reference's PCG32, statistical agreement with
+the reference renderer's own films (tests/golden/ref_*.npz, made by tests/golden/make_golden.py
+from oracle/_ref/ref_render), ray-cast agreement with the Embree Moeller-Trumbore restatement."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from jarabotransientrendering_b200 import scenes as S
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_log_exp_sincos_accuracy(oracle_lib):
+    L = oracle_lib.lib()
+    xs = np.concatenate([np.geomspace(2.0 ** -23, 1.0, 3000), np.linspace(1e-3, 1.0, 2000)]).astype(np.float32)
+    for x in xs[::7]:
+        got = L.orc_log(float(x))
+        ref = np.log(np.float64(x))
+        assert abs(got - ref) <= 2e-7 * max(1.0, abs(ref)), (x, got, ref)
+    for x in np.linspace(-60.0, 5.0, 1500).astype(np.float32)[::3]:
+        got = L.orc_exp(float(x))
+        ref = np.exp(np.float64(x))
+        assert abs(got - ref) <= 3e-7 * ref, (x, got, ref)
+    s, c = C.c_float(), C.c_float()
+    for xi in np.linspace(0.0, 1.0, 4097, endpoint=False).astype(np.float32):
+        L.orc_sincos2pi(float(xi), C.byref(s), C.byref(c))
+        a = 2.0 * np.pi * np.float64(xi)
+        assert abs(s.value - np.sin(a)) < 3e-7 and abs(c.value - np.cos(a)) < 3e-7
+    assert L.orc_log(0.0) == -np.inf
+    assert L.orc_exp(-200.0) == 0.0
+
+
+def _pcg_reference(state, seq, k):
+    """PCG32 exactly as src/Utils/RandomNumbers.h:119-128,167-174 (Python big ints)."""
+    M = (1 << 64) - 1
+    st = 0
+    inc = ((seq << 1) | 1) & M
+
+    def nxt():
+        nonlocal st
+        old = st
+        st = (old * 6364136223846793005 + inc) & M
+        xs = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xs >> rot) | (xs << ((-rot) & 31))) & 0xFFFFFFFF
+
+    nxt()
+    st = (st + state) & M
+    nxt()
+    return [nxt() for _ in range(k + 1)][k]
+
+
+@pytest.mark.parametrize("state,seq", [(0x853c49e6748fea9b, 0xda3e39cb94b95bdb), (1, 1), (42, 54), (7, 1 << 40)])
+def test_pcg32_matches_reference_generator(oracle_lib, state, seq):
+    L = oracle_lib.lib()
+    for k in (0, 1, 2, 17, 100):
+        assert L.orc_pcg32_first(state, seq, k) == _pcg_reference(state, seq, k)
+
+
+def test_pcg32_known_answer(oracle_lib):
+    # PCG32 demo stream (initstate 42, initseq 54) first outputs, as published with pcg32
+    L = oracle_lib.lib()
+    expect = [0xa15c02b7, 0x7b47f409, 0xba1d3330, 0x83d2f293, 0xbfa4784b, 0xcbed606e]
+    assert [L.orc_pcg32_first(42, 54, k) for k in range(6)] == expect
+
+
+def _golden(name):
+    return np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+
+
+def _golden_scene(name):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.golden_scenes()[name]
+
+
+def compare_to_golden(films, g, energy_tol=0.005):
+    """Per-bin z-scores against the reference mean/SE and the total-energy agreement."""
+    K = len(films)
+    mean = films.mean(0)
+    se = films.std(0, ddof=1) / np.sqrt(K)
+    tot = np.sqrt(se.astype(np.float64) ** 2 + g["se"].astype(np.float64) ** 2)
+    m = tot > 0
+    z = (mean - g["mean"])[m] / tot[m]
+    e = films.sum(axis=(1, 2, 3, 4))
+    e_ref, e_se = g["energy"].mean(), g["energy"].std(ddof=1) / np.sqrt(len(g["energy"]))
+    e_z = (e.mean() - e_ref) / np.sqrt(e_se ** 2 + (e.std(ddof=1) / np.sqrt(K)) ** 2)
+    both_empty = (~m) & ((mean != 0) | (g["mean"] != 0))
+    return {"frac_z3": float((np.abs(z) > 3).mean()), "max_z": float(np.abs(z).max()), "mean_z": float(z.mean()),
+            "energy_z": float(e_z),
+            "energy_rel": float(e.mean() / e_ref - 1.0), "one_sided_bins": int(both_empty.sum()),
+            "bins": int(m.sum())}
+
+
+@pytest.mark.parametrize("name", ["cornell", "medium", "arealight"])
+def test_oracle_matches_reference_statistics(oracle_lib, name):
+    """The CPU restatement agrees with the reference renderer within 3 standard errors per
+    time bin (up to the Gaussian tail rate) and in total energy."""
+    sc = _golden_scene(name)
+    g = _golden(name)
+    o = oracle_lib.Oracle(sc)
+    K = len(g["energy"])     # same number of independent runs as the reference fixture
+    films = np.array([o.render(sample_begin=64 * k, sample_count=64, nthreads=4)["streak"] for k in range(K)])
+    r = compare_to_golden(films, g)
+    # SE estimated from K seeds of a skewed estimator: the |z|>3 rate sits near the Student-t
+    # value (~0.5%), well under 2%; a biased restatement shows up as a shifted mean z.
+    assert r["frac_z3"] < 0.02, r
+    assert abs(r["mean_z"]) < 0.1, r
+    assert r["max_z"] < 7.0, r
+    assert abs(r["energy_z"]) < 4.0, r
+    assert abs(r["energy_rel"]) < max(0.005, 4.0 * abs(r["energy_rel"] / r["energy_z"]) if r["energy_z"] else 0.005), r
+    assert r["one_sided_bins"] == 0, r
+
+
+def test_oracle_reference_harness_live(oracle_lib):
+    """When the reference sources are present, rebuild and rerun the reference harness and
+    check it still reproduces the committed golden statistics."""
+    from oracle import refscene
+    if not os.path.isdir("/root/reference/src"):
+        pytest.skip("reference sources not present on this machine")
+    assert refscene.build_ref()
+    sc = _golden_scene("cornell")
+    g = _golden("cornell")
+    films = np.array([refscene.render(sc, seed=1000 + s)["streak"] for s in range(48)])
+    r = compare_to_golden(films, g)
+    assert r["frac_z3"] < 0.02 and abs(r["mean_z"]) < 0.1 and abs(r["energy_z"]) < 4.0, r
+
+
+def test_watertight_vs_embree_moeller(oracle_lib):
+    """Closest hits of the watertight test against the restated Embree Moeller-Trumbore
+    intersector on the seeded correctness batch (origins in the room, uniform directions):
+    same triangle id and hit distance within 2 ulp; the only id disagreements are ties
+    between coplanar triangles (box bottoms lying on the floor) at distances within 2 ulp."""
+    for sc in (S.cornell(), S.icosphere(subdiv=5)):
+        o = oracle_lib.Oracle(sc)
+        rays = S.random_rays(50000, seed=3)
+        hw = o.trace(rays)
+        hm = o.trace_moller(rays)
+        same = hw["prim_id"] == hm["prim_id"]
+        assert same.mean() > 0.99
+        both = same & (hw["prim_id"] != 0xFFFFFFFF)
+        ulp = np.abs(hw["t"][both].view(np.int32).astype(np.int64) - hm["t"][both].view(np.int32))
+        # the restated reference divides with a Newton-refined hardware reciprocal (~1-2 ulp);
+        # the watertight path divides exactly, so a rare 3-ulp gap is the reference's rounding
+        assert (ulp <= 2).mean() > 0.9999 and ulp.max() <= 4
+        diff = ~same
+        assert ((hw["prim_id"][diff] != 0xFFFFFFFF) & (hm["prim_id"][diff] != 0xFFFFFFFF)).all()
+        dulp = np.abs(hw["t"][diff].view(np.int32).astype(np.int64) - hm["t"][diff].view(np.int32))
+        assert (dulp <= 4).all()
+        v, t, _ = sc.flatten()
+        for a, b in zip(hw["prim_id"][diff][:50], hm["prim_id"][diff][:50]):
+            na = np.cross(v[t[a, 2]] - v[t[a, 0]], v[t[a, 1]] - v[t[a, 0]])
+            nb = np.cross(v[t[b, 2]] - v[t[b, 0]], v[t[b, 1]] - v[t[b, 0]])
+            cosang = abs(np.dot(na, nb)) / (np.linalg.norm(na) * np.linalg.norm(nb))
+            assert cosang > 0.9999      # coplanar pair
+
+
+def test_oracle_bvh_stats_and_counts(oracle_lib):
+    sc = S.icosphere(subdiv=4)
+    o = oracle_lib.Oracle(sc)
+    info = o.bvh_info()
+    assert info["leaves"] >= sc.num_triangles / 4
+    rays = S.random_rays(2000, seed=5)
+    h, nv, nt = o.trace(rays, counts=True)
+    assert nv.mean() > 1 and nt.mean() > 1
+    # any-hit agrees with closest-hit on whether something is hit
+    ha = o.trace(rays, any_hit=True)
+    assert ((ha["prim_id"] != 0xFFFFFFFF) == (h["prim_id"] != 0xFFFFFFFF)).all()
