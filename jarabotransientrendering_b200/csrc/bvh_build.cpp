@@ -155,7 +155,16 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
         out.leaves++;
         return ~(int32_t)((first << 3) | n.count);
     };
-    auto write_box = [](GpuNode& g, int slot, const Box& b) {
+    auto write_box = [](GpuNode& g, int slot, const Box& bin) {
+        // one ulp outward: a ray lying exactly in a face plane of a box (zero direction
+        // component, origin on the face) still sees a non-empty slab interval
+        Box b = bin;
+        for (int k = 0; k < 3; ++k) {
+            if (b.lo[k] <= b.hi[k]) {
+                b.lo[k] = std::nextafter(b.lo[k], -INFINITY);
+                b.hi[k] = std::nextafter(b.hi[k], INFINITY);
+            }
+        }
         if (slot == 0) {
             g.a[0] = b.lo[0]; g.a[1] = b.hi[0]; g.a[2] = b.lo[1]; g.a[3] = b.hi[1];
             g.c[0] = b.lo[2]; g.c[1] = b.hi[2];

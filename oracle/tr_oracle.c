@@ -287,6 +287,13 @@ int orc_create(const orc_scene* s, const orc_camera* c, const orc_film* f, const
     B.nodes = (bnode*)malloc(sizeof(bnode) * (2 * nt + 1)); B.n = 0;
     uint32_t maxd = 0;
     build_rec(&B, 0, nt, 0, &maxd);
+    /* one ulp outward so that a ray lying in a face plane (zero direction component, origin
+       on the face) still sees a non-empty slab interval */
+    for (uint32_t i = 0; i < B.n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            B.nodes[i].box.lo[k] = nextafterf(B.nodes[i].box.lo[k], -INFINITY);
+            B.nodes[i].box.hi[k] = nextafterf(B.nodes[i].box.hi[k], INFINITY);
+        }
     x->nodes = B.nodes; x->nnodes = B.n; x->order = B.idx; x->depth = maxd;
     x->nleaves = 0;
     for (uint32_t i = 0; i < B.n; ++i) if (B.nodes[i].left < 0) x->nleaves++;
