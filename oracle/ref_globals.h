@@ -14,6 +14,7 @@
 #include <memory>
 #include <limits>
 #include <algorithm>
+#include <stdexcept>
 #define DIM 3
 #define SPECTRUM_CHANNELS 3
 using Real = float;
