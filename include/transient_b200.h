@@ -198,6 +198,29 @@ tr_status tr_trace_rays(tr_ctx* ctx, const float* rays, uint32_t n, int any_hit,
 tr_status tr_trace_rays_device(tr_ctx* ctx, const float* d_rays, uint32_t n, int any_hit,
                                tr_hit* d_out, void* stream);
 
+/* Render without allocating.  No counterpart in the reference renderer: it exists for callers
+ * that cannot allocate GPU memory once their set-up is done -- for example engines whose own
+ * memory pool owns the whole device and forbids foreign cudaMalloc calls, or frame loops that
+ * cannot afford cudaMalloc's implicit device-wide synchronisation in the middle of a frame.
+ * tr_render may grow its path buffers with cudaMalloc; this entry
+ * point instead keeps the per-path state of the wavefront in one fixed array compiled into
+ * the library (24 MiB per GPU that loads the library, held until the process exits).
+ * It adds camera samples [sample_begin, sample_begin + sample_count) of the pixel window
+ * [x0,x1) x [y0,y1) to the context's film, exactly as tr_render_region does, asynchronously
+ * on `stream` (cudaStream_t as void*, NULL = the context's stream).
+ * Limits: (x1-x0)*(y1-y0)*sample_count*incoming_samples <= TR_NOALLOC_MAX_PATHS paths per
+ * call and max_bounces <= TR_NOALLOC_MAX_BOUNCES; larger requests return
+ * TR_ERR_INVALID_ARGUMENT -- split the window or the sample range over several calls.
+ * The array is shared by every call in the process on that GPU: calls that can overlap on
+ * the GPU (different streams, or different contexts on one device) race and corrupt each
+ * other's paths, so issue them on one stream.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture begins. */
+#define TR_NOALLOC_MAX_PATHS 65536u
+#define TR_NOALLOC_MAX_BOUNCES 16u
+tr_status tr_render_region_noalloc(tr_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                                   uint64_t sample_begin, uint32_t sample_count, void* stream);
+
 tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
 
 /* Runs all later work of the context on the caller's CUDA stream (cudaStream_t as void*;

@@ -81,6 +81,8 @@ PROTOTYPES = {
     "tr_write_film": (C.c_int, [C.c_void_p, C.c_char_p]),
     "tr_trace_rays": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]),
     "tr_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
+    "tr_render_region_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                           C.c_uint64, C.c_uint32, C.c_void_p]),
     "tr_stats_get": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "tr_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tr_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),

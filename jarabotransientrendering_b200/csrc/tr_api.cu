@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -596,6 +597,112 @@ tr_status tr_stats_get(tr_ctx* x, tr_stats* out) {
     if (!x || !out) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
     *out = x->stats;
     out->device_bytes = x->bytes;
+    return TR_OK;
+}
+
+// -----------------------------------------------------------------------------------------
+// tr_render_region_noalloc: the same wavefront kernels, with every per-path buffer carved out
+// of one file-scope device array instead of cudaMalloc'd memory.
+// -----------------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t na_align(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kNaSlots = TR_NOALLOC_MAX_PATHS;
+constexpr size_t kNaF4 = na_align(sizeof(float4) * kNaSlots);
+constexpr size_t kNaBytes = 7 * kNaF4                                            // ray_o ray_d thr hit sh_o sh_d sh_L
+                          + na_align(sizeof(unsigned long long) * kNaSlots)       // rng
+                          + 2 * na_align(sizeof(uint32_t) * kNaSlots)             // extend queues
+                          + na_align(sizeof(float4) * kNaSlots * TR_NOALLOC_MAX_BOUNCES)  // records
+                          + na_align(kNaSlots)                                    // records per slot
+                          + na_align(sizeof(uint32_t) * trk::kCounters)           // queue counters
+                          + na_align(sizeof(unsigned long long) * 8);             // ray / splat counts
+
+// The scratch itself.  Its name is only a host-side handle: host code must use the device
+// address from cudaGetSymbolAddress, never &g_noalloc_scratch.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};     // device address of the array, per device ordinal
+
+// Looks the array up once per device, with that device current.
+tr_status noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= 64) return fail(TR_ERR_NO_DEVICE, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(TR_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+    return TR_OK;
+}
+
+}  // namespace
+
+extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                                              uint64_t s0, uint32_t ns, void* stream) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    if (x1 > x->film.width || y1 > x->film.height || x0 >= x1 || y0 >= y1)
+        return fail(TR_ERR_INVALID_ARGUMENT, "pixel window out of range or empty");
+    if (ns == 0) return TR_OK;
+    if (s0 + ns > (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "camera sample index must stay below 2^32");
+    if (x->integ.max_bounces > TR_NOALLOC_MAX_BOUNCES)
+        return fail(TR_ERR_INVALID_ARGUMENT, "tr_render_region_noalloc supports max_bounces <= " +
+                                                 std::to_string(TR_NOALLOC_MAX_BOUNCES) + " (scene has " +
+                                                 std::to_string(x->integ.max_bounces) + ")");
+    const uint64_t npix = (uint64_t)(x1 - x0) * (y1 - y0);
+    const uint64_t paths = npix * ns * x->integ.incoming_samples;
+    if (paths > TR_NOALLOC_MAX_PATHS)
+        return fail(TR_ERR_INVALID_ARGUMENT, "tr_render_region_noalloc renders at most " +
+                                                 std::to_string(TR_NOALLOC_MAX_PATHS) + " paths per call (asked for " +
+                                                 std::to_string(paths) + "); split the window or the samples");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        unsigned char* base = nullptr;
+        tr_status st = noalloc_scratch(x->device, &base);
+        if (st != TR_OK) return st;
+        cudaStream_t strm = stream ? static_cast<cudaStream_t>(stream) : x->s();
+        trk::Params p = make_params(x);
+        trk::Wave& w = p.wave;
+        unsigned char* c = base;
+        auto take = [&](size_t bytes) { unsigned char* r = c; c += na_align(bytes); return r; };
+        w.ray_o = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.ray_d = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.thr = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.hit = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.sh_o = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.sh_d = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.sh_L = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
+        w.rng = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * kNaSlots));
+        w.q[0] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * kNaSlots));
+        w.q[1] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * kNaSlots));
+        w.rec = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots * TR_NOALLOC_MAX_BOUNCES));
+        w.rec_n = take(kNaSlots);
+        w.counters = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * trk::kCounters));
+        w.stats = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 8));
+        w.capacity = (uint32_t)kNaSlots;
+        // what the kernels expect to start at zero: queue counters / fetch cursors and the
+        // ray counters (records-per-slot are reset by the ray generation kernel)
+        TR_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * trk::kCounters, strm));
+        TR_CUDA(cudaMemsetAsync(w.stats, 0, sizeof(unsigned long long) * 8, strm));
+        p.batch.win_x0 = x0; p.batch.win_y0 = y0; p.batch.win_w = x1 - x0;
+        p.batch.pix_begin = 0; p.batch.npix = (uint32_t)npix;
+        p.batch.s0 = s0; p.batch.ns = ns; p.batch.ninc = x->integ.incoming_samples;
+        p.batch.n_slots = (uint32_t)paths;
+        TR_CUDA(trk::launch_raygen(p, strm));
+        for (uint32_t d = 0; d < x->integ.max_bounces; ++d) {
+            TR_CUDA(trk::launch_extend(p, (int)d, x->trace_grid, strm));
+            TR_CUDA(trk::launch_shade(p, (int)d, strm));
+            TR_CUDA(trk::launch_shadow(p, (int)d, x->trace_grid, strm));
+        }
+        TR_CUDA(trk::launch_splat(p, x->splat_g, strm));
+        x->stats.paths += paths;
+        x->stats.camera_samples += npix * ns;
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
     return TR_OK;
 }
 
