@@ -52,7 +52,7 @@ T* dalloc(size_t count, size_t& total) {
 
 constexpr uint32_t kMaxBounces = 63;            // counters hold 64 depths
 constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batch
-constexpr size_t kSplatSmemBudget = 100 * 1024;  // two splat CTAs per SM
+constexpr size_t kSplatSmemBudget = 56 * 1024;   // four 512-thread splat CTAs per SM
 
 }  // namespace
 
@@ -223,6 +223,7 @@ trk::Params make_params(tr_ctx* x) {
     p.seed = x->integ.seed;
     p.max_bounces = x->integ.max_bounces;
     p.sqrt_spp = x->integ.sqrt_spp;
+    p.bvh_depth = x->bvh_depth;
     return p;
 }
 
@@ -426,6 +427,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         sc.nodes = x->d_nodes; sc.tris = x->d_tris; sc.tri_ng = x->d_tri_ng;
         sc.mats = x->d_mats; sc.mats2 = x->d_mats2; sc.lights = x->d_lights;
         sc.num_lights = s->num_lights;
+        sc.bvh_depth = x->bvh_depth;
         sc.medium = s->medium.enabled ? 1u : 0u;
         if (sc.medium) {
             trd::f3 st = trd::mk(s->medium.sigma_a[0] + s->medium.sigma_s[0], s->medium.sigma_a[1] + s->medium.sigma_s[1],
@@ -452,7 +454,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         TR_CUDA(cudaMemsetAsync(x->d_steady, 0, (size_t)f->width * f->height * 3u * sizeof(double), x->stream));
         TR_CUDA(cudaMemsetAsync(x->d_weight, 0, (size_t)f->width * f->height * sizeof(double), x->stream));
 
-        x->trace_grid = trk::trace_grid_size(device);
+        x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);
         int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
         x->splat_g = std::max(1, std::min(g, 16));
         x->d_cursor = x->alloc<uint32_t>(1);

@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(256) k_raygen(Params p) {
 // -----------------------------------------------------------------------------------------
 // extend / shadow: persistent warps fetch 32 queue entries at a time.
 // -----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTraceBlock) k_extend(Params p, int depth) {
-    __shared__ int stack[kStack * kTraceBlock];
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(Params p, int depth) {
+    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
     const uint32_t n = depth == 0 ? p.batch.n_slots : p.wave.counters[cnt_ext(depth)];
     const uint32_t* q = p.wave.q[depth & 1];
     const unsigned lane = threadIdx.x & 31u;
@@ -183,12 +183,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_extend(Params p, int depth) {
     }
 }
 
-__global__ void __launch_bounds__(kTraceBlock) k_shadow(Params p, int depth) {
-    __shared__ int stack[kStack * kTraceBlock];
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(Params p, int depth) {
+    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
     const uint32_t n = p.wave.counters[cnt_sh(depth)];
     const unsigned lane = threadIdx.x & 31u;
     uint32_t* cursor = &p.wave.counters[cur_sh(depth)];
-    const uint32_t R = p.max_bounces;
+    const size_t rs = p.wave.capacity;          // record stride: records are [bounce][slot]
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.wave.stats[1], (unsigned long long)n);
     unsigned long long splats = 0;
     for (;;) {
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shadow(Params p, int depth) {
                 const float4 L = p.wave.sh_L[idx];
                 const uint32_t slot = __float_as_uint(L.w);
                 const uint32_t k = p.wave.rec_n[slot];
-                p.wave.rec[(size_t)slot * R + k] = make_float4(L.x, L.y, L.z, d.w);
+                p.wave.rec[(size_t)k * rs + slot] = make_float4(L.x, L.y, L.z, d.w);
                 p.wave.rec_n[slot] = (uint8_t)(k + 1);
                 ++splats;
             }
@@ -447,8 +447,8 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
 // A CTA owns `G` whole pixels of the batch, accumulates their records in an FP32 shared-memory
 // tile (warp-aggregated atomics on equal (pixel, bin) keys) and adds the tile to the FP64 film.
 // -----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_splat(Params p, int G) {
-    extern __shared__ float tile[];
+__global__ void __launch_bounds__(kSplatBlock) k_splat(Params p, int G) {
+    extern __shared__ __align__(16) float tile[];
     const uint32_t T = p.film.T;
     const uint32_t TT = T * 3u;
     const Batch& B = p.batch;
@@ -456,13 +456,18 @@ __global__ void __launch_bounds__(256) k_splat(Params p, int G) {
     if (pix0 >= B.npix) return;
     const uint32_t gp = min((uint32_t)G, B.npix - pix0);
     float* steady = tile + (size_t)G * TT;
-    for (uint32_t e = threadIdx.x; e < (uint32_t)G * TT + 3u * G; e += blockDim.x) tile[e] = 0.0f;
+    {
+        float4* t4 = reinterpret_cast<float4*>(tile);
+        const uint32_t n4 = ((uint32_t)G * TT + 3u * G + 3u) / 4u;
+        for (uint32_t e = threadIdx.x; e < n4; e += blockDim.x) t4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     __syncthreads();
     const uint32_t per_pix = B.ns * B.ninc;
     const uint32_t nslots = gp * per_pix;
     const uint32_t slot0 = pix0 * per_pix;
-    const uint32_t R = p.max_bounces;
+    const size_t rs = p.wave.capacity;           // records are [bounce][slot]
     const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt = lanemask_lt();
     // per-lane running steady-image sums, flushed when the lane moves to another pixel
     uint32_t acc_pl = 0xffffffffu;
     float ax = 0.f, ay = 0.f, az = 0.f;
@@ -483,14 +488,15 @@ __global__ void __launch_bounds__(256) k_splat(Params p, int G) {
         for (uint32_t k = 0; k < kmax; ++k) {
             const bool valid = k < cnt;
             float4 rc = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (valid) rc = p.wave.rec[(size_t)slot * R + k];
+            if (valid) rc = __ldcs(&p.wave.rec[(size_t)k * rs + slot]);     // streamed, read once
             const uint32_t key = valid ? pl * T + __float_as_uint(rc.w) : 0xffffffffu;
-            // group lanes with the same (pixel, bin); the group's lowest lane adds the sum
+            // lanes holding the same (pixel, bin) are summed with shuffles; the group's
+            // lowest lane issues one shared-memory atomic per channel
             const unsigned peers = __match_any_sync(kFull, key);
-            const int rank = __popc(peers & lanemask_lt());
+            const int rank = __popc(peers & lt);
             const int gsize = __popc(peers);
             float vx = rc.x, vy = rc.y, vz = rc.z;
-            const uint32_t maxg = __reduce_max_sync(kFull, (uint32_t)gsize);
+            const uint32_t maxg = __reduce_max_sync(kFull, valid ? (uint32_t)gsize : 1u);
             for (int step = 1; step < (int)maxg; step <<= 1) {
                 const int src_rank = rank + step;
                 const int src = src_rank < gsize ? (int)__fns(peers, 0, src_rank + 1) : (int)lane;
@@ -511,22 +517,32 @@ __global__ void __launch_bounds__(256) k_splat(Params p, int G) {
         atomicAdd(sd, ax); atomicAdd(sd + 1, ay); atomicAdd(sd + 2, az);
     }
     __syncthreads();
-    // flush: FP64 read-modify-write of the touched bins (the film starts zeroed)
-    for (uint32_t e = threadIdx.x; e < gp * TT; e += blockDim.x) {
-        const float v = tile[e];
-        if (v != 0.0f) {
-            const uint32_t pl = e / TT;
-            const uint32_t wpix = B.pix_begin + pix0 + pl;
-            const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * p.film.W + (B.win_x0 + wpix % B.win_w);
-            double* dst = p.film.streak + pixel * TT + (e - pl * TT);
-            *dst += (double)v;
-        }
-    }
-    for (uint32_t e = threadIdx.x; e < gp; e += blockDim.x) {
-        const uint32_t wpix = B.pix_begin + pix0 + e;
+    // flush: FP64 read-add-write of the touched bins (the film starts zeroed); four
+    // independent loads in flight per thread
+    for (uint32_t pl = 0; pl < gp; ++pl) {
+        const uint32_t wpix = B.pix_begin + pix0 + pl;
         const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * p.film.W + (B.win_x0 + wpix % B.win_w);
-        p.film.weight[pixel] += (double)B.ns;
-        for (int c = 0; c < 3; ++c) p.film.steady[pixel * 3 + c] += (double)steady[e * 3 + c];
+        double* dst = p.film.streak + pixel * TT;
+        const float* src = tile + (size_t)pl * TT;
+        for (uint32_t e0 = threadIdx.x; e0 < TT; e0 += 4u * blockDim.x) {
+            float v[4];
+            double o[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t e = e0 + (uint32_t)u * blockDim.x;
+                v[u] = e < TT ? src[e] : 0.0f;
+                o[u] = v[u] != 0.0f ? dst[e] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t e = e0 + (uint32_t)u * blockDim.x;
+                if (v[u] != 0.0f) dst[e] = o[u] + (double)v[u];
+            }
+        }
+        if (threadIdx.x == 0) {
+            p.film.weight[pixel] += (double)B.ns;
+            for (int c = 0; c < 3; ++c) p.film.steady[pixel * 3 + c] += (double)steady[pl * 3 + c];
+        }
     }
 }
 
@@ -535,10 +551,10 @@ __global__ void __launch_bounds__(256) k_splat(Params p, int G) {
 // -----------------------------------------------------------------------------------------
 struct HitOut { float t; uint32_t id; float u, v; };
 
-__global__ void __launch_bounds__(kTraceBlock) k_trace_user(SceneDev sc, const float* __restrict__ rays,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_user(SceneDev sc, const float* __restrict__ rays,
                                                             uint32_t n, int any_hit, HitOut* out,
                                                             uint32_t* cursor) {
-    __shared__ int stack[kStack * kTraceBlock];
+    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
     const unsigned lane = threadIdx.x & 31u;
     for (;;) {
         uint32_t base = 0;
@@ -562,15 +578,20 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_user(SceneDev sc, const f
 // -----------------------------------------------------------------------------------------
 // launchers
 // -----------------------------------------------------------------------------------------
-int trace_grid_size(int device) {
+size_t trace_smem_bytes(uint32_t bvh_depth) { return (size_t)(bvh_depth + 1u) * kTraceBlock * sizeof(int); }
+
+int trace_grid_size(int device, uint32_t bvh_depth) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend, kTraceBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend, kTraceBlock, trace_smem_bytes(bvh_depth));
     if (per_sm < 1) per_sm = 1;
     return sms * per_sm;
 }
 
-size_t splat_smem_bytes(uint32_t T, int G) { return ((size_t)G * T * 3u + 3u * (size_t)G) * sizeof(float); }
+size_t splat_smem_bytes(uint32_t T, int G) {
+    // tile [G][T][3] + steady [G][3] floats, rounded up to whole float4 (zeroed as float4)
+    return (((size_t)G * T * 3u + 3u * (size_t)G) * sizeof(float) + 15u) & ~size_t(15);
+}
 
 cudaError_t launch_raygen(const Params& p, cudaStream_t s) {
     const uint32_t n = p.batch.n_slots;
@@ -578,7 +599,7 @@ cudaError_t launch_raygen(const Params& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s) {
-    k_extend<<<grid, kTraceBlock, 0, s>>>(p, depth);
+    k_extend<<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
 }
 cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s) {
@@ -593,7 +614,7 @@ cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s) {
-    k_shadow<<<grid, kTraceBlock, 0, s>>>(p, depth);
+    k_shadow<<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
 }
 cudaError_t launch_splat(const Params& p, int G, cudaStream_t s) {
@@ -604,12 +625,13 @@ cudaError_t launch_splat(const Params& p, int G, cudaStream_t s) {
         attr_set = true;
     }
     const uint32_t blocks = (p.batch.npix + (uint32_t)G - 1) / (uint32_t)G;
-    k_splat<<<blocks, 256, smem, s>>>(p, G);
+    k_splat<<<blocks, kSplatBlock, smem, s>>>(p, G);
     return cudaGetLastError();
 }
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit, void* out,
                               uint32_t* cursor, int grid, cudaStream_t s) {
-    k_trace_user<<<grid, kTraceBlock, 0, s>>>(sc, rays, n, any_hit, reinterpret_cast<HitOut*>(out), cursor);
+    k_trace_user<<<grid, kTraceBlock, trace_smem_bytes(sc.bvh_depth), s>>>(sc, rays, n, any_hit,
+                                                                          reinterpret_cast<HitOut*>(out), cursor);
     return cudaGetLastError();
 }
 

@@ -5,8 +5,10 @@
 
 namespace trk {
 
-constexpr int kStack = 64;          // per-thread traversal stack entries (shared memory)
+constexpr int kStack = 64;          // max traversal stack entries per thread (BVH depth + 1)
 constexpr int kTraceBlock = 128;    // threads per traversal block
+constexpr int kTraceMinBlocks = 8;  // register budget: 8 traversal blocks per SM
+constexpr int kSplatBlock = 512;    // threads per splat block
 constexpr int kMaxLights = 64;
 constexpr int kMaxMaterials = 256;
 
@@ -23,6 +25,7 @@ struct SceneDev {
     float sig_s[3], sig_t[3];
     float lambda;             // mean extinction avg(sigma_t)
     float g;
+    uint32_t bvh_depth;       // deepest leaf; the traversal stack holds bvh_depth + 1 entries
 };
 
 struct CameraDev {
@@ -51,7 +54,7 @@ struct Wave {
     float4* sh_o;             // shadow: origin, tfar
     float4* sh_d;             // shadow: direction, time bin (bits)
     float4* sh_L;             // shadow: contribution rgb, slot (bits)
-    float4* rec;              // splat records [slot][max_bounces]: rgb, bin (bits)
+    float4* rec;              // splat records [bounce][capacity]: rgb, bin (bits)
     uint8_t* rec_n;           // records per slot
     uint32_t* counters;       // see counter_* helpers below
     unsigned long long* stats;// closest, shadow, splats, paths (accumulated)
@@ -75,6 +78,7 @@ struct Params {
     unsigned long long seed;
     uint32_t max_bounces;
     uint32_t sqrt_spp;
+    uint32_t bvh_depth;
 };
 
 // counters layout (uint32): [0, 64) extend counts per depth, [64, 128) shadow counts per
@@ -93,7 +97,8 @@ cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);
-int trace_grid_size(int device);
+int trace_grid_size(int device, uint32_t bvh_depth);
+size_t trace_smem_bytes(uint32_t bvh_depth);
 size_t splat_smem_bytes(uint32_t T, int pixels_per_cta);
 
 }  // namespace trk
