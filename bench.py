@@ -278,19 +278,27 @@ def main():
         steady = torch.empty((H, W, 3), dtype=torch.float64, pin_memory=True).numpy()
         weight = torch.empty((H, W), dtype=torch.float64, pin_memory=True).numpy()
         e2e_steps = max(1, min(args.steps, 3))
-        times = []
+        times, phases = [], []
         for i in range(e2e_steps + 1):
             t0 = time.perf_counter()
             c = T.Context(sc, device=local, arrays=(pv, pt, pm))
+            t1 = time.perf_counter()
             c.render(0, spp)
+            t2 = time.perf_counter()
             c.film_into(streak, steady, weight)
+            t3 = time.perf_counter()
+            bvh_ms = c.stats()["bvh_build_ms"]
             c.close()
-            times.append(time.perf_counter() - t0)
+            t4 = time.perf_counter()
+            times.append(t4 - t0)
+            phases.append({"create_ms": (t1 - t0) * 1e3, "bvh_build_ms": bvh_ms, "render_ms": (t2 - t1) * 1e3,
+                           "film_d2h_ms": (t3 - t2) * 1e3, "destroy_ms": (t4 - t3) * 1e3})
         et = sum(times[1:]) / e2e_steps          # first iteration warms the allocator
         out["e2e"] = {"value": paths_per_step * world / et, "unit": "paths/s",
                       "h2d_bytes_per_step": int(pv.nbytes + pt.nbytes + pm.nbytes),
                       "d2h_bytes_per_step": int(streak.nbytes + steady.nbytes + weight.nbytes),
                       "ms_per_step": et * 1e3,
+                      "phases_last_step": phases[-1],
                       "includes": "tr_create (scene H2D from pinned memory + host BVH build + film alloc), "
                                   "tr_render, tr_get_film (D2H into pinned memory), tr_destroy"}
     else:

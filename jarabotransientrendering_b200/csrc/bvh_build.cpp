@@ -4,6 +4,8 @@
 #include "bvh_build.h"
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -32,13 +34,19 @@ struct Node { Box box; int32_t left = -1, right = -1; uint32_t first = 0, count 
 
 constexpr int kBins = 32;
 
+// Subtrees larger than this are built on their own thread (up to the hardware's thread count).
+constexpr uint32_t kParallelCutoff = 16384;
+
 struct Builder {
     const Box* tb;
     const float* cen;
     std::vector<uint32_t> idx;
-    std::vector<Node> nodes;
+    std::vector<Node> nodes;          // preallocated 2*nt; slots handed out by `next`
+    std::atomic<uint32_t> next{0};
+    std::atomic<uint32_t> depth{0};
+    std::atomic<int> threads{1};
+    int max_threads = 1;
     uint32_t max_leaf;
-    uint32_t depth = 0;
 
     int bin_of(float c, float lo, float scale) const {
         int b = (int)((c - lo) * scale);
@@ -46,8 +54,7 @@ struct Builder {
     }
 
     uint32_t build(uint32_t first, uint32_t count, uint32_t d) {
-        uint32_t me = (uint32_t)nodes.size();
-        nodes.emplace_back();
+        uint32_t me = next.fetch_add(1, std::memory_order_relaxed);
         Box nb, cb; nb.empty(); cb.empty();
         for (uint32_t i = first; i < first + count; ++i) {
             uint32_t t = idx[i];
@@ -55,7 +62,8 @@ struct Builder {
             cb.growp(&cen[3 * t]);
         }
         nodes[me].box = nb;
-        depth = std::max(depth, d);
+        uint32_t dd = depth.load(std::memory_order_relaxed);
+        while (d > dd && !depth.compare_exchange_weak(dd, d)) {}
         if (count <= max_leaf) {
             // SAH leaf test: keep as a leaf when small enough
             nodes[me].first = first; nodes[me].count = count;
@@ -99,8 +107,19 @@ struct Builder {
             mid = (uint32_t)(it - idx.begin());
             if (mid == first || mid == first + count) mid = first + count / 2;
         }
-        int32_t l = (int32_t)build(first, mid - first, d + 1);
-        int32_t r = (int32_t)build(mid, first + count - mid, d + 1);
+        int32_t l, r;
+        if (count > kParallelCutoff && threads.fetch_add(1) < max_threads) {
+            uint32_t rr = 0;
+            std::thread t([&] { rr = build(mid, first + count - mid, d + 1); });
+            l = (int32_t)build(first, mid - first, d + 1);
+            t.join();
+            threads.fetch_sub(1);
+            r = (int32_t)rr;
+        } else {
+            if (count > kParallelCutoff) threads.fetch_sub(1);
+            l = (int32_t)build(first, mid - first, d + 1);
+            r = (int32_t)build(mid, first + count - mid, d + 1);
+        }
         nodes[me].left = l; nodes[me].right = r; nodes[me].count = 0;
         return me;
     }
@@ -133,8 +152,10 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
     B.tb = tb.data(); B.cen = cen.data(); B.max_leaf = max_leaf;
     B.idx.resize(nt);
     for (uint32_t t = 0; t < nt; ++t) B.idx[t] = t;
-    B.nodes.reserve(2 * (size_t)nt);
+    B.nodes.resize(2 * (size_t)nt);
+    B.max_threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     B.build(0, nt, 0);
+    B.nodes.resize(B.next.load());
 
     // Flatten: one GpuNode per interior node, depth-first, left child adjacent to its parent.
     out.nodes.clear(); out.tris.clear(); out.leaves = 0;
@@ -213,7 +234,7 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
                 if (B.nodes[child[s]].left >= 0) stack.push_back((uint32_t)child[s]);
         }
     }
-    out.depth = B.depth;
+    out.depth = B.depth.load();
     out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return true;
 }

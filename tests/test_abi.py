@@ -179,3 +179,27 @@ def test_reference_adaptor_compiles():
     subprocess.check_call(["g++", "-fsyntax-only", "-std=c++14", "-w", "-include",
                            os.path.join(ROOT, "oracle", "ref_globals.h"), f"-I{ref}", f"-I{ROOT}/include",
                            os.path.join(ROOT, "tests", "adaptor_check.cpp")])
+
+
+@pytest.mark.parametrize("workload", ["cornell", "icosphere"])
+def test_product_bvh_builder_invariants(tmp_path, workload):
+    """The host BVH builder of the CUDA path (csrc/bvh_build.cpp, multithreaded binned SAH): every
+    triangle exactly once in leaf order with its vertices, boxes enclose their leaves, all nodes
+    reachable, reported depth bounds the traversal stack."""
+    import json
+    import subprocess
+    exe = tmp_path / "bvh_check"
+    csrc = os.path.join(ROOT, "jarabotransientrendering_b200", "csrc")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-pthread", "-ffp-contract=off", f"-I{csrc}",
+                           os.path.join(ROOT, "tests", "bvh_check.cpp"), os.path.join(csrc, "bvh_build.cpp"),
+                           "-o", str(exe)])
+    v, t, _ = S.WORKLOADS[workload]().flatten()
+    raw = tmp_path / "mesh.bin"
+    with open(raw, "wb") as fh:
+        fh.write(np.array([len(v), len(t)], np.uint32).tobytes())
+        fh.write(v.tobytes())
+        fh.write(t.tobytes())
+    out = subprocess.run([str(exe), str(raw)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout
+    info = json.loads(out.stdout)
+    assert info["depth"] + 1 < 64
