@@ -137,7 +137,8 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
         const tr_material& m = s->materials[i];
         if (m.kind != TR_MAT_LAMBERTIAN && m.kind != TR_MAT_GGX)
             return fail(TR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has unknown kind");
-        if (m.kind == TR_MAT_GGX) return fail(TR_ERR_NOT_SUPPORTED, "GGX material is not available in this build");
+        if (m.kind == TR_MAT_GGX && !(m.alpha >= 1e-3f && m.alpha <= 1.0f))
+            return fail(TR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + ": GGX alpha must be in [0.001, 1]");
         for (float v : m.kd)
             if (!std::isfinite(v)) return fail(TR_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " albedo is not finite");
     }

@@ -97,6 +97,10 @@ def lib():
         L.orc_exp.restype = C.c_float
         L.orc_exp.argtypes = [C.c_float]
         L.orc_sincos2pi.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.orc_ggx_sample.restype = C.c_int
+        L.orc_ggx_sample.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_ggx_eval_cos.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_pcg32_first.restype = C.c_uint32
         L.orc_pcg32_first.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32]
         _lib = L

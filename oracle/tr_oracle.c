@@ -524,6 +524,107 @@ static inline int is_finite3(const float* L) {
     return isfinite(L[0]) && isfinite(L[1]) && isfinite(L[2]);
 }
 
+/* ------------------------------------------------------------------------------------------
+ * GGX microfacet reflection (no counterpart in the reference; restated from the published
+ * methods): D, Smith height-correlated G2 and Schlick F of Walter et al. 2007 ("Microfacet
+ * models for refraction through rough surfaces", EGSR), visible-normal sampling of Heitz 2018
+ * ("Sampling the GGX distribution of visible normals", JCGT 7(4)).  Local frame around the
+ * geometric normal: Duff et al. 2017.  Reflection only; the back side absorbs.
+ * ---------------------------------------------------------------------------------------- */
+#define PI_F 3.14159274f
+typedef struct { v3 t1, t2, n; } frame3;
+static inline frame3 make_frame(v3 n) {
+    float sg = copysignf(1.0f, n.z);
+    float a = -1.0f / (sg + n.z);
+    float b = n.x * n.y * a;
+    frame3 F;
+    F.t1 = mk(1.0f + sg * n.x * n.x * a, sg * b, -sg * n.x);
+    F.t2 = mk(b, sg + n.y * n.y * a, -n.y);
+    F.n = n;
+    return F;
+}
+static inline v3 to_local(const frame3* F, v3 w) { return mk(dot(w, F->t1), dot(w, F->t2), dot(w, F->n)); }
+static inline v3 to_world(const frame3* F, v3 l) {
+    return add(add(muls(F->t1, l.x), muls(F->t2, l.y)), muls(F->n, l.z));
+}
+static inline float ggx_D(float a2, float hz) {
+    float c = hz * hz;
+    float d = c * (a2 - 1.0f) + 1.0f;
+    return a2 / ((PI_F * d) * d);
+}
+static inline float ggx_lambda(float a2, v3 w) {
+    float t2 = (w.x * w.x + w.y * w.y) / (w.z * w.z);
+    return (-1.0f + sqrtf(1.0f + a2 * t2)) * 0.5f;
+}
+static inline float schlick(float f0, float c) {
+    float m = 1.0f - c;
+    float m2 = m * m;
+    return f0 + (1.0f - f0) * ((m2 * m2) * m);
+}
+/* f(wo, wi) * max(0, n.wi); wo = towards the previous vertex, wi = towards the light */
+static v3 ggx_eval_cos(v3 kd, float alpha, v3 n, v3 wo_w, v3 wi_w) {
+    frame3 F = make_frame(n);
+    v3 wo = to_local(&F, wo_w), wi = to_local(&F, wi_w);
+    if (!(wo.z > 0.0f) || !(wi.z > 0.0f)) return mk(0.0f, 0.0f, 0.0f);
+    v3 h = normalize(add(wo, wi));
+    float a2 = alpha * alpha;
+    float D = ggx_D(a2, h.z);
+    float G2 = 1.0f / ((1.0f + ggx_lambda(a2, wo)) + ggx_lambda(a2, wi));
+    float c = dot(wo, h);
+    if (c < 0.0f) c = 0.0f;
+    float common = (D * G2) / (4.0f * wo.z);
+    return mk(schlick(kd.x, c) * common, schlick(kd.y, c) * common, schlick(kd.z, c) * common);
+}
+/* visible-normal sample; returns 0 when the reflected direction leaves below the surface */
+static int ggx_sample(v3 kd, float alpha, v3 n, v3 wo_w, float sp, float cp, float x2, v3* wi_w, v3* fa, float* pa) {
+    frame3 F = make_frame(n);
+    v3 wo = to_local(&F, wo_w);
+    if (!(wo.z > 0.0f)) return 0;
+    v3 Vh = normalize(mk(alpha * wo.x, alpha * wo.y, wo.z));
+    float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
+    v3 T1 = lensq > 0.0f ? divs(mk(-Vh.y, Vh.x, 0.0f), sqrtf(lensq)) : mk(1.0f, 0.0f, 0.0f);
+    v3 T2 = cross(Vh, T1);
+    float r = sqrtf(x2);
+    float t1 = r * cp, t2 = r * sp;
+    float s = 0.5f * (1.0f + Vh.z);
+    t2 = (1.0f - s) * sqrtf(1.0f - t1 * t1) + s * t2;
+    float tz2 = (1.0f - t1 * t1) - t2 * t2;
+    float tz = sqrtf(tz2 > 0.0f ? tz2 : 0.0f);
+    v3 Nh = add(add(muls(T1, t1), muls(T2, t2)), muls(Vh, tz));
+    v3 h = normalize(mk(alpha * Nh.x, alpha * Nh.y, Nh.z > 0.0f ? Nh.z : 0.0f));
+    float c = dot(wo, h);
+    v3 wi = sub(muls(h, 2.0f * c), wo);
+    if (!(wi.z > 0.0f)) return 0;
+    float a2 = alpha * alpha;
+    float Lo = ggx_lambda(a2, wo), Li = ggx_lambda(a2, wi);
+    float G1 = 1.0f / (1.0f + Lo);
+    float G2 = 1.0f / ((1.0f + Lo) + Li);
+    float pdf = (G1 * ggx_D(a2, h.z)) / (4.0f * wo.z);
+    float w = G2 / G1;
+    if (c < 0.0f) c = 0.0f;
+    *fa = mk((schlick(kd.x, c) * w) * pdf, (schlick(kd.y, c) * w) * pdf, (schlick(kd.z, c) * w) * pdf);
+    *pa = pdf;
+    *wi_w = normalize(to_world(&F, wi));
+    return 1;
+}
+
+/* exposed for unit tests: weight (f cos / pdf) and pdf of one sample, and eval */
+int orc_ggx_sample(const float* kd, float alpha, const float* n, const float* wo, float x1, float x2,
+                   float* wi, float* weight, float* pdf) {
+    float sp, cp;
+    orc_sincos2pi(x1, &sp, &cp);
+    v3 w, fa; float pa;
+    if (!ggx_sample(ld3(kd), alpha, ld3(n), ld3(wo), sp, cp, x2, &w, &fa, &pa)) return 0;
+    wi[0] = w.x; wi[1] = w.y; wi[2] = w.z;
+    weight[0] = fa.x / pa; weight[1] = fa.y / pa; weight[2] = fa.z / pa;
+    *pdf = pa;
+    return 1;
+}
+void orc_ggx_eval_cos(const float* kd, float alpha, const float* n, const float* wo, const float* wi, float* out) {
+    v3 r = ggx_eval_cos(ld3(kd), alpha, ld3(n), ld3(wo), ld3(wi));
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
 /* One random walk; appends its splat records (at most max_bounces) to rec. */
 static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc, srec* rec, pstats* st) {
     const orc_film* F = &x->film;
@@ -565,11 +666,16 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
         if (time > total_time) break;
 
         v3 n = mk(0, 0, 0), kd = mk(0, 0, 0);
+        int ggx = 0;
+        float alpha = 0.0f;
         if (surface) {
             n = x->ng[h.prim_id];
             const orc_material* m = &x->mats[x->mat[h.prim_id]];
             kd = ld3(m->kd);
+            ggx = m->kind == 1;
+            alpha = m->alpha;
         }
+        v3 wo = mk(-dir.x, -dir.y, -dir.z);
 
         /* ---- next-event estimation (connect_vertex_with_light + transient connect_paths) ---- */
         {
@@ -601,7 +707,9 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
             if (ok) {
                 v3 wl = mk(-ld.x, -ld.y, -ld.z);
                 v3 fe;
-                if (surface) {
+                if (surface && ggx) {
+                    fe = ggx_eval_cos(kd, alpha, n, wo, wl);
+                } else if (surface) {
                     float cs = dot(wl, n);
                     float cl = cs > 0.0f ? cs : 0.0f;
                     fe = mk((kd.x * INV_PI_F) * cl, (kd.y * INV_PI_F) * cl, (kd.z * INV_PI_F) * cl);
@@ -647,7 +755,9 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
         float sp, cp;
         orc_sincos2pi(x1, &sp, &cp);
         v3 fa; float pa; v3 nd;
-        if (surface) {
+        if (surface && ggx) {
+            if (!ggx_sample(kd, alpha, n, wo, sp, cp, x2, &nd, &fa, &pa)) break;
+        } else if (surface) {
             /* Lambertian cosine sampling in the frame of Intersection::set_coordinate_system */
             float ct = sqrtf(x2);
             float stt = sqrtf(1.0f - ct * ct);

@@ -94,6 +94,12 @@ int orc_render(const orc_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32
 int orc_path_records(const orc_ctx* ctx, uint32_t x, uint32_t y, uint64_t s, uint32_t j,
                      uint32_t* bins, float* rgb, int cap);
 
+/* GGX material kernels (unit tests): one visible-normal sample (weight = f cos / pdf per
+ * channel) and the evaluation f(wo, wi) * max(0, n.wi).  Return 0 when no direction results. */
+int  orc_ggx_sample(const float* kd, float alpha, const float* n, const float* wo, float x1, float x2,
+                    float* wi, float* weight, float* pdf);
+void orc_ggx_eval_cos(const float* kd, float alpha, const float* n, const float* wo, const float* wi, float* out);
+
 /* The math kernels shared by the oracle and the CUDA path, exposed for unit tests. */
 float orc_log(float x);
 float orc_exp(float x);

@@ -31,6 +31,8 @@ def small(name):
                         max_bounces=12)
     if name == "icosphere":
         return S.icosphere(subdiv=5, width=32, height=32, time_bins=512, exposure=0.01, sqrt_spp=4, max_bounces=8)
+    if name == "ggx":
+        return S.guided(width=24, height=24, time_bins=256, exposure=0.02, sqrt_spp=4, max_bounces=6)
     if name == "arealight":
         s = S.guided(width=24, height=24, time_bins=256, exposure=0.02, sqrt_spp=4, max_bounces=6,
                      lambertian_floor=True)
@@ -84,7 +86,7 @@ def test_trace_rays_edge_cases(gpu, oracle_lib):
     assert ((a["prim_id"] != 0xFFFFFFFF) == (h["prim_id"] != 0xFFFFFFFF)).all()
 
 
-@pytest.mark.parametrize("name", ["cornell", "medium", "icosphere", "arealight"])
+@pytest.mark.parametrize("name", ["cornell", "medium", "icosphere", "arealight", "ggx"])
 def test_render_matches_oracle_per_path(gpu, oracle_lib, name):
     sc = small(name)
     with gpu.Context(sc) as ctx:
@@ -142,7 +144,7 @@ def test_gpu_matches_reference_statistics(gpu, name):
     assert r["one_sided_bins"] == 0, r
 
 
-@pytest.mark.parametrize("workload", ["cornell", "icosphere", "medium"])
+@pytest.mark.parametrize("workload", ["cornell", "icosphere", "medium", "guided"])
 def test_full_size_properties(gpu, workload):
     """Benchmark-size renders: weights, steady = sum over time, finiteness, determinism."""
     sc = S.WORKLOADS[workload]()
@@ -158,7 +160,7 @@ def test_full_size_properties(gpu, workload):
     assert np.isfinite(f["streak"]).all() and (f["streak"] >= 0).all()
     tsum = f["streak"].sum(axis=2)
     assert np.allclose(tsum, f["steady"], rtol=1e-4, atol=1e-9)
-    assert np.array_equal(f2["steady"], f["steady"])       # same seed, same walks, same order
+    assert np.allclose(f2["steady"], f["steady"], rtol=1e-5, atol=1e-12)   # same walks; atomics reorder sums
     assert st["paths"] == sc.width * sc.height * spp * sc.incoming_samples
     assert f["steady"].sum() > 0
 

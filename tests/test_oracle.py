@@ -170,3 +170,48 @@ def test_oracle_bvh_stats_and_counts(oracle_lib):
     # any-hit agrees with closest-hit on whether something is hit
     ha = o.trace(rays, any_hit=True)
     assert ((ha["prim_id"] != 0xFFFFFFFF) == (h["prim_id"] != 0xFFFFFFFF)).all()
+
+
+def test_ggx_sampling_matches_evaluation_and_conserves_energy(oracle_lib):
+    """GGX (no reference counterpart): the visible-normal sample's weight times its pdf equals the
+    evaluated f*cos for the sampled direction, the directional albedo stays <= 1, and a nearly
+    smooth surface reflects F(cos) like a mirror."""
+    L = oracle_lib.lib()
+    rng = np.random.default_rng(3)
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    kd = f([0.9, 0.6, 0.3])
+    n = f([0.0, 1.0, 0.0])
+    for alpha in (0.05, 0.2, 0.6):
+        wis = []
+        for _ in range(300):
+            th = np.arccos(rng.uniform(0.05, 1.0))
+            ph = rng.uniform(0, 2 * np.pi)
+            wo = f([np.sin(th) * np.cos(ph), np.cos(th), np.sin(th) * np.sin(ph)])
+            wi = np.zeros(3, np.float32)
+            w = np.zeros(3, np.float32)
+            pdf = np.zeros(1, np.float32)
+            ok = L.orc_ggx_sample(kd.ctypes.data, alpha, n.ctypes.data, wo.ctypes.data, float(rng.random()),
+                                  float(rng.random()), wi.ctypes.data, w.ctypes.data, pdf.ctypes.data)
+            if not ok:
+                continue
+            ev = np.zeros(3, np.float32)
+            L.orc_ggx_eval_cos(kd.ctypes.data, alpha, n.ctypes.data, wo.ctypes.data, wi.ctypes.data, ev.ctypes.data)
+            assert np.allclose(w * pdf[0], ev, rtol=2e-3, atol=1e-7), (alpha, w * pdf[0], ev)
+            assert abs(np.linalg.norm(wi) - 1) < 1e-5 and wi[1] > 0
+        # directional albedo by Monte Carlo at a fixed direction
+        wo = f([np.sin(0.5), np.cos(0.5), 0.0])
+        acc = np.zeros(3)
+        N = 4000
+        for i in range(N):
+            wi = np.zeros(3, np.float32)
+            w = np.zeros(3, np.float32)
+            pdf = np.zeros(1, np.float32)
+            if L.orc_ggx_sample(kd.ctypes.data, alpha, n.ctypes.data, wo.ctypes.data, (i + 0.5) / N,
+                                float(rng.random()), wi.ctypes.data, w.ctypes.data, pdf.ctypes.data):
+                acc += w
+        alb = acc / N
+        assert (alb <= 1.0 + 1e-3).all()
+        if alpha == 0.05:
+            c = np.cos(0.5)
+            F = kd + (1 - kd) * (1 - c) ** 5
+            assert np.allclose(alb, F, rtol=0.02)
