@@ -221,6 +221,30 @@ tr_status tr_trace_rays_device(tr_ctx* ctx, const float* d_rays, uint32_t n, int
 tr_status tr_render_region_noalloc(tr_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
                                    uint64_t sample_begin, uint32_t sample_count, void* stream);
 
+/* ---- learned directional proposal (no counterpart in the reference renderer) -------------
+ * An MLP maps a surface vertex's features (64 BF16 values: sin/cos encoded position, position,
+ * normal, outgoing direction, normalised path length, zero padding) through three hidden
+ * layers of 64 ReLU units to 8 von Mises-Fisher lobes (per lobe: weight logit, unnormalised
+ * mean xyz, concentration before softplus).  Forward and hidden-layer backward run as BF16
+ * tcgen05 tensor-core kernels with FP32 accumulation; training minimises
+ * -sum_i w_i log q(dir_i | x_i) / sum_i w_i with Adam.
+ * Parameters (TR_GUIDE_PARAMS floats): weights [4][64 in][64 out], then biases [4][64]. */
+#define TR_GUIDE_PARAMS 16640
+#define TR_GUIDE_OUTPUTS 40
+typedef struct tr_guide tr_guide;
+tr_status tr_guide_create(int device, uint64_t seed, tr_guide** out);
+tr_status tr_guide_set_params(tr_guide* g, const float* params);
+tr_status tr_guide_get_params(tr_guide* g, float* params);
+/* d_features: device [n][64] bf16 (uint16 bits); d_out: device [n][40] float. */
+tr_status tr_guide_forward(tr_guide* g, const uint16_t* d_features, uint32_t n, float* d_out, void* stream);
+/* One training step on device batch (features [n][64] bf16, dirs [n][3], weights [n]):
+ * gradients into the guide (tr_guide_get_grads), then Adam with step size lr when lr > 0.
+ * *loss (may be NULL) receives the batch loss before the update. */
+tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features, const float* d_dirs, const float* d_weights,
+                              uint32_t n, float lr, float* loss, void* stream);
+tr_status tr_guide_get_grads(tr_guide* g, float* grads);
+tr_status tr_guide_destroy(tr_guide* g);
+
 tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
 
 /* Runs all later work of the context on the caller's CUDA stream (cudaStream_t as void*;

@@ -83,6 +83,14 @@ PROTOTYPES = {
     "tr_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
     "tr_render_region_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                            C.c_uint64, C.c_uint32, C.c_void_p]),
+    "tr_guide_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "tr_guide_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tr_guide_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tr_guide_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "tr_guide_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float,
+                                      C.POINTER(C.c_float), C.c_void_p]),
+    "tr_guide_get_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tr_guide_destroy": (C.c_int, [C.c_void_p]),
     "tr_stats_get": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "tr_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tr_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),

@@ -19,6 +19,7 @@
 #include "tr_device.cuh"
 #include "tr_kernels.cuh"
 #include "tr_film_io.h"
+#include "tr_guide.cuh"
 
 namespace {
 
@@ -708,6 +709,216 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
     }
     return TR_OK;
 }
+
+}  // extern "C"
+
+// -----------------------------------------------------------------------------------------
+// learned proposal network
+// -----------------------------------------------------------------------------------------
+struct tr_guide {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    float* params = nullptr;   // FP32 master copy
+    float* grads = nullptr;
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    uint8_t* w_fwd = nullptr;  // packed BF16 tiles
+    uint8_t* w_bwd = nullptr;
+    int* err = nullptr;
+    float* scalars = nullptr;  // [0] weight sum, [1] loss
+    uint32_t cap = 0;
+    uint4* act = nullptr;
+    float* out = nullptr;
+    uint4* dy_bf = nullptr;
+    float* dy_f = nullptr;
+    float* dh = nullptr;
+    uint32_t step = 0;
+    template <class T>
+    T* alloc(size_t n) {
+        T* p = dalloc<T>(n, bytes);
+        allocs.push_back(p);
+        return p;
+    }
+    void drop(void* p) {
+        if (!p) return;
+        cudaFree(p);
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
+    }
+    trg::GuideDev dev() const {
+        return trg::GuideDev{reinterpret_cast<const uint4*>(w_fwd), reinterpret_cast<const uint4*>(w_bwd),
+                             params + 4 * 4096};
+    }
+    void ensure(uint32_t n) {
+        if (cap >= n) return;
+        drop(act); drop(out); drop(dy_bf); drop(dy_f); drop(dh);
+        act = alloc<uint4>((size_t)3 * n * 8);
+        out = alloc<float>((size_t)n * trg::kOut);
+        dy_bf = alloc<uint4>((size_t)n * 8);
+        dy_f = alloc<float>((size_t)n * 64);
+        dh = alloc<float>((size_t)3 * n * 64);
+        cap = n;
+    }
+};
+
+namespace {
+tr_status guide_check_err(tr_guide* g, cudaStream_t s) {
+    int e = 0;
+    TR_CUDA(cudaMemcpyAsync(&e, g->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(cudaStreamSynchronize(s));
+    if (e) {
+        TR_CUDA(cudaMemsetAsync(g->err, 0, sizeof(int), s));
+        return fail(TR_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
+    }
+    return TR_OK;
+}
+}  // namespace
+
+extern "C" tr_status tr_guide_create(int device, uint64_t seed, tr_guide** out) {
+    if (!out) return fail(TR_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(TR_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(TR_ERR_NO_DEVICE, "device index out of range");
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, device);
+    if (prop.major != 10) return fail(TR_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+    tr_guide* g = new (std::nothrow) tr_guide();
+    if (!g) return fail(TR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    try {
+        g->device = device;
+        TR_CUDA(cudaSetDevice(device));
+        TR_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        g->params = g->alloc<float>(TR_GUIDE_PARAMS);
+        g->grads = g->alloc<float>(TR_GUIDE_PARAMS);
+        g->m1 = g->alloc<float>(TR_GUIDE_PARAMS);
+        g->m2 = g->alloc<float>(TR_GUIDE_PARAMS);
+        g->w_fwd = g->alloc<uint8_t>(4 * 8192);
+        g->w_bwd = g->alloc<uint8_t>(4 * 8192);
+        g->err = g->alloc<int>(1);
+        g->scalars = g->alloc<float>(4);
+        // He-uniform hidden layers; a small output layer so the first mixture is broad
+        std::vector<float> p(TR_GUIDE_PARAMS, 0.0f);
+        unsigned long long st = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+        auto uni = [&]() {
+            st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+            return (float)((st >> 40) & 0xFFFFFFull) / 16777216.0f * 2.0f - 1.0f;
+        };
+        for (int l = 0; l < 4; ++l) {
+            const float a = l < 3 ? std::sqrt(6.0f / 64.0f) : 0.05f;
+            for (int i = 0; i < 4096; ++i) p[(size_t)l * 4096 + i] = a * uni();
+        }
+        TR_CUDA(cudaMemcpy(g->params, p.data(), sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyHostToDevice));
+        TR_CUDA(cudaMemset(g->m1, 0, sizeof(float) * TR_GUIDE_PARAMS));
+        TR_CUDA(cudaMemset(g->m2, 0, sizeof(float) * TR_GUIDE_PARAMS));
+        TR_CUDA(cudaMemset(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS));
+        TR_CUDA(cudaMemset(g->err, 0, sizeof(int)));
+        TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, g->stream));
+        TR_CUDA(cudaStreamSynchronize(g->stream));
+    } catch (const CudaError& e) {
+        for (void* q : g->allocs) cudaFree(q);
+        delete g;
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    *out = g;
+    return TR_OK;
+}
+
+extern "C" tr_status tr_guide_set_params(tr_guide* g, const float* params) {
+    if (!g || !params) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+        TR_CUDA(cudaSetDevice(g->device));
+        TR_CUDA(cudaMemcpy(g->params, params, sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyHostToDevice));
+        TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, g->stream));
+        TR_CUDA(cudaStreamSynchronize(g->stream));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+extern "C" tr_status tr_guide_get_params(tr_guide* g, float* params) {
+    if (!g || !params) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+        TR_CUDA(cudaSetDevice(g->device));
+        TR_CUDA(cudaStreamSynchronize(g->stream));
+        TR_CUDA(cudaMemcpy(params, g->params, sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyDeviceToHost));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+extern "C" tr_status tr_guide_get_grads(tr_guide* g, float* grads) {
+    if (!g || !grads) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+        TR_CUDA(cudaSetDevice(g->device));
+        TR_CUDA(cudaStreamSynchronize(g->stream));
+        TR_CUDA(cudaMemcpy(grads, g->grads, sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyDeviceToHost));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+extern "C" tr_status tr_guide_forward(tr_guide* g, const uint16_t* d_features, uint32_t n, float* d_out, void* stream) {
+    if (!g || (n && (!d_features || !d_out))) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return TR_OK;
+    if ((reinterpret_cast<uintptr_t>(d_features) & 15u) != 0) return fail(TR_ERR_INVALID_ARGUMENT, "features must be 16-byte aligned");
+    try {
+        TR_CUDA(cudaSetDevice(g->device));
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+        TR_CUDA(trg::mlp_forward(g->dev(), reinterpret_cast<const uint4*>(d_features), n, d_out, nullptr, g->err, s));
+        return guide_check_err(g, s);
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+}
+
+extern "C" tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features, const float* d_dirs,
+                                         const float* d_weights, uint32_t n, float lr, float* loss, void* stream) {
+    if (!g || !n || !d_features || !d_dirs || !d_weights) return fail(TR_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+    if ((reinterpret_cast<uintptr_t>(d_features) & 15u) != 0) return fail(TR_ERR_INVALID_ARGUMENT, "features must be 16-byte aligned");
+    try {
+        TR_CUDA(cudaSetDevice(g->device));
+        g->ensure(n);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+        const uint4* x = reinterpret_cast<const uint4*>(d_features);
+        TR_CUDA(trg::mlp_forward(g->dev(), x, n, g->out, g->act, g->err, s));
+        TR_CUDA(cudaMemsetAsync(g->scalars, 0, 4 * sizeof(float), s));
+        TR_CUDA(trg::mix_grad(g->out, d_dirs, d_weights, n, g->scalars, g->dy_bf, g->dy_f, g->scalars + 1, s));
+        TR_CUDA(trg::mlp_backward(g->dev(), g->dy_bf, g->act, n, g->dh, g->err, s));
+        TR_CUDA(cudaMemsetAsync(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS, s));
+        float* gb = g->grads + 4 * 4096;
+        const size_t mrow = (size_t)n * 8;
+        TR_CUDA(trg::weight_grad(x, g->dh, n, g->grads, gb, s));                                   // layer 1
+        TR_CUDA(trg::weight_grad(g->act, g->dh + (size_t)n * 64, n, g->grads + 4096, gb + 64, s));      // layer 2
+        TR_CUDA(trg::weight_grad(g->act + mrow, g->dh + (size_t)2 * n * 64, n, g->grads + 8192, gb + 128, s));
+        TR_CUDA(trg::weight_grad(g->act + 2 * mrow, g->dy_f, n, g->grads + 12288, gb + 192, s));        // output
+        if (lr > 0.0f) {
+            g->step += 1;
+            TR_CUDA(trg::adam(g->params, g->grads, g->m1, g->m2, TR_GUIDE_PARAMS, lr, g->step, s));
+            TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, s));
+        }
+        if (loss) TR_CUDA(cudaMemcpyAsync(loss, g->scalars + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+        return guide_check_err(g, s);
+    } catch (const CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
+    }
+}
+
+extern "C" tr_status tr_guide_destroy(tr_guide* g) {
+    if (!g) return TR_OK;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    for (void* q : g->allocs) cudaFree(q);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return TR_OK;
+}
+
+extern "C" {
 
 tr_status tr_set_stream(tr_ctx* x, void* stream) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");

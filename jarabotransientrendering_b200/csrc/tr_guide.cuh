@@ -1,0 +1,43 @@
+// tr_guide.cuh - learned directional proposal: MLP (64 -> 3x64 ReLU -> 40) predicting a mixture
+// of 8 von Mises-Fisher lobes, trained online on the renderer's own radiance samples.
+// No counterpart in the reference renderer.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace trg {
+
+constexpr int kIn = 64;          // padded feature width
+constexpr int kHidden = 64;
+constexpr int kLobes = 8;
+constexpr int kOut = 5 * kLobes; // per lobe: weight logit, mean xyz (unnormalised), concentration
+constexpr int kLayers = 4;
+constexpr int kParams = kLayers * 64 * 64 + kLayers * 64;   // weights [l][in][out] then biases [l][out]
+constexpr int kTile = 128;       // rows per tcgen05 tile (MMA M)
+constexpr float kKappaMin = 0.05f, kKappaMax = 2000.0f;
+
+// Features of a surface vertex (46 used of 64, rest zero):
+//   [0,36)  sin/cos(2^k pi p_d), k = 0..5, d = x,y,z      (p normalised to the scene box)
+//   [36,39) p normalised, [39,42) geometric normal, [42,45) outgoing direction (towards the
+//   previous vertex), [45] path length / film time length
+constexpr int kFeatUsed = 46;
+
+struct GuideDev {
+    const uint4* w_fwd;    // 4 canonical K-major B tiles (Wt: [out][in]) bf16, 8 KB each
+    const uint4* w_bwd;    // 4 canonical K-major B tiles (W: [in][out]) bf16
+    const float* bias;     // [4][64]
+};
+
+cudaError_t mlp_forward(const GuideDev& g, const uint4* x, uint32_t m, float* out, uint4* act, int* err,
+                        cudaStream_t s);
+cudaError_t mlp_backward(const GuideDev& g, const uint4* dy, const uint4* act, uint32_t m, float* dh, int* err,
+                         cudaStream_t s);
+int mlp_grid(int device);
+cudaError_t pack_weights(const float* params, uint8_t* w_fwd, uint8_t* w_bwd, cudaStream_t s);
+cudaError_t mix_grad(const float* out, const float* dirs, const float* w, uint32_t m, float* wsum, uint4* dy_bf,
+                     float* dy_f, float* loss, cudaStream_t s);
+cudaError_t weight_grad(const uint4* prev, const float* grad, uint32_t m, float* gw, float* gb, cudaStream_t s);
+cudaError_t adam(float* params, const float* grads, float* m1, float* m2, uint32_t n, float lr, uint32_t step,
+                 cudaStream_t s);
+
+}  // namespace trg

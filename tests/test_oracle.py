@@ -215,3 +215,33 @@ def test_ggx_sampling_matches_evaluation_and_conserves_energy(oracle_lib):
             c = np.cos(0.5)
             F = kd + (1 - kd) * (1 - c) ** 5
             assert np.allclose(alb, F, rtol=0.02)
+
+
+def test_guide_oracle_gradient_matches_finite_differences():
+    """The proposal network's analytic gradient (oracle/guide_oracle.py) agrees with central
+    differences of its own loss (computed without BF16 rounding of the perturbed weights)."""
+    from oracle import guide_oracle as G
+    rng = np.random.default_rng(0)
+    n = 64
+    params = rng.normal(0, 0.2, G.NP).astype(np.float32)
+    x = G.bf16(rng.normal(0, 1, (n, 64)).astype(np.float32))
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    w = rng.random(n) + 0.1
+    _, dout = G.loss_and_dout(G.forward(params, x)[0], dirs, w)
+    out = G.forward(params, x)[0].astype(np.float64)
+    eps = 1e-4
+    for j in [0, 1, 2, 3, 4, 7, 13, 21, 39]:
+        e = np.zeros_like(out)
+        e[:, j] = eps
+        lp = G.loss_and_dout(out + e, dirs, w)[0]
+        lm = G.loss_and_dout(out - e, dirs, w)[0]
+        num = (lp - lm) / (2 * eps)
+        assert abs(num - dout[:, j].sum()) < 1e-5 + 1e-3 * abs(num), (j, num, dout[:, j].sum())
+    # vMF density integrates to one (Monte Carlo over the sphere)
+    mu = np.array([[0.0, 0.0, 1.0]])
+    for kappa in (0.1, 3.0, 50.0):
+        v = rng.normal(size=(200000, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        dens = np.exp(G.log_vmf(kappa, v @ mu[0]))
+        assert abs(dens.mean() * 4 * np.pi - 1.0) < 0.03
