@@ -119,9 +119,16 @@ typedef struct tr_integrator {
     uint32_t max_bounces;
     uint32_t sqrt_spp;
     uint32_t incoming_samples;
-    uint32_t reserved;
+    uint32_t flags;             /* TR_FLAG_* */
     uint64_t seed;
 } tr_integrator;
+
+/* Lambertian directions in an orthonormal frame around the normal.  Without the flag the
+ * frame of Intersection::set_coordinate_system (src/RayTracing/Intersection.h:167-178) is
+ * reproduced exactly, including its non-orthogonal branch, so results match the reference;
+ * that frame's true sampling density is not cos/pi, so guided rendering (which combines
+ * densities by MIS) requires this flag, as does the plain render it is compared against. */
+#define TR_FLAG_ORTHONORMAL_FRAME 1u
 
 /* ---- ray-batch interface (correctness batch of World::first_intersection / intersects) --- */
 
@@ -150,6 +157,9 @@ typedef struct tr_stats {
      * measured with CUDA events around each launch on the render stream                      */
     double   raygen_ms, extend_ms, shade_ms, shadow_ms, splat_ms;
     uint64_t extend_launches, shadow_launches;
+    double   guide_ms;         /* proposal inference + guided sampling (profiling on)        */
+    uint64_t train_steps;      /* proposal training steps run by the last tr_render call     */
+    float    train_loss;       /* loss of the last training step                             */
 } tr_stats;
 
 /* ---- lifetime ----------------------------------------------------------------------------- */
@@ -244,6 +254,15 @@ tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features, const flo
                               uint32_t n, float lr, float* loss, void* stream);
 tr_status tr_guide_get_grads(tr_guide* g, float* grads);
 tr_status tr_guide_destroy(tr_guide* g);
+
+/* Renders the context with the learned proposal: surface directions are drawn from the
+ * mixture with probability mix_prob and from the BSDF otherwise, combined by one-sample MIS
+ * (balance heuristic) so the film converges to the same image as without a guide.  When
+ * train_pool > 0, every tr_render call collects up to train_pool (vertex, direction, weight)
+ * samples from its own paths and then trains the guide on them (Adam, learning_rate, batches
+ * of 65,536).  Needs TR_FLAG_ORTHONORMAL_FRAME.  guide = NULL detaches.  The guide must live
+ * on the context's device and outlive its use. */
+tr_status tr_set_guide(tr_ctx* ctx, tr_guide* guide, float mix_prob, float learning_rate, uint32_t train_pool);
 
 tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
 

@@ -47,7 +47,7 @@ class Film(C.Structure):
 
 class Integrator(C.Structure):
     _fields_ = [("max_bounces", C.c_uint32), ("sqrt_spp", C.c_uint32), ("incoming_samples", C.c_uint32),
-                ("reserved", C.c_uint32), ("seed", C.c_uint64)]
+                ("flags", C.c_uint32), ("seed", C.c_uint64)]
 
 
 class Hit(C.Structure):
@@ -61,7 +61,8 @@ class Stats(C.Structure):
                 ("device_bytes", C.c_uint64), ("kernel_launches", C.c_uint64),
                 ("raygen_ms", C.c_double), ("extend_ms", C.c_double), ("shade_ms", C.c_double),
                 ("shadow_ms", C.c_double), ("splat_ms", C.c_double),
-                ("extend_launches", C.c_uint64), ("shadow_launches", C.c_uint64)]
+                ("extend_launches", C.c_uint64), ("shadow_launches", C.c_uint64),
+                ("guide_ms", C.c_double), ("train_steps", C.c_uint64), ("train_loss", C.c_float)]
 
 
 TR_OK = 0
@@ -91,6 +92,7 @@ PROTOTYPES = {
                                       C.POINTER(C.c_float), C.c_void_p]),
     "tr_guide_get_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tr_guide_destroy": (C.c_int, [C.c_void_p]),
+    "tr_set_guide": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_uint32]),
     "tr_stats_get": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "tr_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tr_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),

@@ -57,6 +57,8 @@ constexpr size_t kSplatSmemBudget = 56 * 1024;   // four 512-thread splat CTAs p
 
 }  // namespace
 
+struct tr_guide;
+
 struct tr_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -96,6 +98,15 @@ struct tr_ctx {
     uint32_t* d_cursor = nullptr;
 
     tr_stats stats{};
+    // learned proposal (tr_set_guide)
+    tr_guide* guide = nullptr;
+    float guide_mix = 0.5f, guide_lr = 1e-3f;
+    uint32_t guide_pool = 0;
+    trk::GuideWave gw{};
+    uint32_t gw_capacity = 0;
+    uint32_t* pool_state = nullptr;       // [0] pool fill, [1] entries with targets
+    float last_train_loss = 0.0f;
+    uint32_t train_steps = 0;
     cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null
     bool profiling = false;
     std::vector<cudaEvent_t> prof_events; // pool of timing events
@@ -170,6 +181,7 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     if (it->sqrt_spp == 0 || it->incoming_samples == 0)
         return fail(TR_ERR_INVALID_ARGUMENT, "sqrt_spp and incoming_samples must be >= 1");
     if (it->max_bounces > kMaxBounces) return fail(TR_ERR_INVALID_ARGUMENT, "max_bounces must be <= 63");
+    if (it->flags & ~TR_FLAG_ORTHONORMAL_FRAME) return fail(TR_ERR_INVALID_ARGUMENT, "unknown integrator flags");
     if (!std::isfinite(c->focal_distance)) return fail(TR_ERR_INVALID_ARGUMENT, "camera focal distance not finite");
     return TR_OK;
 }
@@ -210,6 +222,29 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.capacity = capacity;
 }
 
+void ensure_guided(tr_ctx* x, uint32_t capacity) {
+    if (x->gw_capacity >= capacity && x->gw.pool_cap == x->guide_pool && x->pool_state) return;
+    auto drop = [&](void* p) {
+        if (!p) return;
+        cudaFree(p);
+        x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), p), x->allocs.end());
+    };
+    trk::GuideWave& g = x->gw;
+    drop(g.gq); drop(g.pool_feat); drop(g.pool_dir); drop(g.pool_w); drop(g.pool_meta);
+    g.gq = x->alloc<uint32_t>(capacity);
+    const uint32_t pc = std::max<uint32_t>(1u, x->guide_pool);
+    g.pool_feat = x->alloc<uint4>((size_t)pc * 8);
+    g.pool_dir = x->alloc<float>((size_t)pc * 3);
+    g.pool_w = x->alloc<float>(pc);
+    g.pool_meta = x->alloc<uint4>(pc);
+    g.pool_cap = x->guide_pool;
+    if (!x->pool_state) x->pool_state = x->alloc<uint32_t>(2);
+    x->gw_capacity = capacity;
+}
+
+trg::GuideDev guide_dev(tr_guide* g);
+int* guide_err(tr_guide* g);
+
 trk::Params make_params(tr_ctx* x) {
     trk::Params p{};
     p.scene = x->scene;
@@ -226,8 +261,16 @@ trk::Params make_params(tr_ctx* x) {
     p.max_bounces = x->integ.max_bounces;
     p.sqrt_spp = x->integ.sqrt_spp;
     p.bvh_depth = x->bvh_depth;
+    p.flags = x->integ.flags;
+    if (x->guide) {
+        p.guide = x->gw;
+        p.guide.net = guide_dev(x->guide);
+        p.guide.err = guide_err(x->guide);
+    }
     return p;
 }
+
+tr_status guide_after_render(tr_ctx* x, cudaStream_t s);
 
 tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
                         uint64_t s0, uint32_t ns_total) {
@@ -242,6 +285,14 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     uint32_t cap = (uint32_t)std::min<uint64_t>(total_slots, kDefaultCapacity);
     cap = std::max<uint32_t>(cap, ninc);
     ensure_wave(x, cap);
+    const bool guided = x->guide != nullptr;
+    if (guided) {
+        ensure_guided(x, cap);
+        // about 1.5 guided vertices per path; keep enough of them to fill the training pool
+        x->gw.keep_prob = x->guide_pool ? std::min(1.0f, (float)x->guide_pool / (1.5f * (float)total_slots)) : 0.0f;
+        x->gw.mix_prob = x->guide_mix;
+        TR_CUDA(cudaMemsetAsync(x->pool_state, 0, 2 * sizeof(uint32_t), x->s()));
+    }
     // samples per pixel per batch, and pixels per batch
     uint32_t ns_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(ns_total, cap / ninc));
     cudaStream_t strm = x->s();
@@ -283,7 +334,15 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             for (uint32_t d = 0; d < x->integ.max_bounces; ++d) {
                 timed(1, [&] { return trk::launch_extend(p, (int)d, x->trace_grid, strm); });
                 timed(2, [&] { return trk::launch_shade(p, (int)d, strm); });
+                if (guided) {
+                    timed(5, [&] { return trk::launch_guide(p, (int)d, x->pool_state, strm); });
+                    launches += 1;
+                }
                 timed(3, [&] { return trk::launch_shadow(p, (int)d, x->trace_grid, strm); });
+            }
+            if (guided && x->guide_pool) {
+                TR_CUDA(trk::launch_train_gather(p, x->pool_state, strm));
+                launches += 2;
             }
             timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm); });
             launches += 2 + 3ull * x->integ.max_bounces;
@@ -295,7 +354,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     TR_CUDA(cudaEventSynchronize(x->ev1));
     float ms = 0.f;
     TR_CUDA(cudaEventElapsedTime(&ms, x->ev0, x->ev1));
-    double kms[5] = {0, 0, 0, 0, 0};
+    double kms[6] = {0, 0, 0, 0, 0, 0};
     for (const Mark& m : marks) {
         float e = 0.f;
         TR_CUDA(cudaEventElapsedTime(&e, x->prof_events[m.ev], x->prof_events[m.ev + 1]));
@@ -303,6 +362,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     }
     x->stats.raygen_ms = kms[0]; x->stats.extend_ms = kms[1]; x->stats.shade_ms = kms[2];
     x->stats.shadow_ms = kms[3]; x->stats.splat_ms = kms[4];
+    x->stats.guide_ms = kms[5];
     x->stats.kernel_launches = launches;
     x->stats.extend_launches = ext_l;
     x->stats.shadow_launches = sh_l;
@@ -314,6 +374,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     x->stats.paths += total_slots;
     x->stats.camera_samples += win_pix * ns_total;
     x->stats.render_ms = ms;
+    if (guided) return guide_after_render(x, strm);
     return TR_OK;
 }
 
@@ -430,6 +491,18 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         sc.mats = x->d_mats; sc.mats2 = x->d_mats2; sc.lights = x->d_lights;
         sc.num_lights = s->num_lights;
         sc.bvh_depth = x->bvh_depth;
+        {
+            float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+            for (uint32_t i = 0; i < s->num_vertices; ++i)
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = std::min(lo[k], s->vertices[3 * (size_t)i + k]);
+                    hi[k] = std::max(hi[k], s->vertices[3 * (size_t)i + k]);
+                }
+            for (int k = 0; k < 3; ++k) {
+                sc.bmin[k] = lo[k];
+                sc.binv[k] = hi[k] > lo[k] ? 1.0f / (hi[k] - lo[k]) : 1.0f;
+            }
+        }
         sc.medium = s->medium.enabled ? 1u : 0u;
         if (sc.medium) {
             trd::f3 st = trd::mk(s->medium.sigma_a[0] + s->medium.sigma_s[0], s->medium.sigma_a[1] + s->medium.sigma_s[1],
@@ -669,6 +742,7 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
         if (st != TR_OK) return st;
         cudaStream_t strm = stream ? static_cast<cudaStream_t>(stream) : x->s();
         trk::Params p = make_params(x);
+        p.guide = trk::GuideWave{};      // the fixed array holds no proposal buffers: plain sampling
         trk::Wave& w = p.wave;
         unsigned char* c = base;
         auto take = [&](size_t bytes) { unsigned char* r = c; c += na_align(bytes); return r; };
@@ -915,6 +989,51 @@ extern "C" tr_status tr_guide_destroy(tr_guide* g) {
     for (void* q : g->allocs) cudaFree(q);
     if (g->stream) cudaStreamDestroy(g->stream);
     delete g;
+    return TR_OK;
+}
+
+namespace {
+trg::GuideDev guide_dev(tr_guide* g) { return g->dev(); }
+int* guide_err(tr_guide* g) { return g->err; }
+
+// After a guided render: surface an MMA timeout, then train on the collected pool.
+tr_status guide_after_render(tr_ctx* x, cudaStream_t s) {
+    tr_status st = guide_check_err(x->guide, s);
+    if (st != TR_OK) return st;
+    x->stats.train_steps = 0;
+    if (!x->guide_pool) return TR_OK;
+    uint32_t fill = 0;
+    TR_CUDA(cudaMemcpyAsync(&fill, x->pool_state, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(cudaStreamSynchronize(s));
+    const uint32_t n = std::min(fill, x->guide_pool);
+    const uint32_t batch = 65536;
+    for (uint32_t off = 0; off + 1024 <= n; off += batch) {
+        const uint32_t m = std::min(batch, n - off);
+        float loss = 0.0f;
+        st = tr_guide_train_step(x->guide, reinterpret_cast<const uint16_t*>(x->gw.pool_feat + (size_t)off * 8),
+                                 x->gw.pool_dir + (size_t)off * 3, x->gw.pool_w + off, m, x->guide_lr, &loss, s);
+        if (st != TR_OK) return st;
+        x->stats.train_steps += 1;
+        x->stats.train_loss = loss;
+    }
+    return TR_OK;
+}
+}  // namespace
+
+extern "C" tr_status tr_set_guide(tr_ctx* x, tr_guide* g, float mix_prob, float lr, uint32_t train_pool) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    if (!g) { x->guide = nullptr; return TR_OK; }
+    if (!(x->integ.flags & TR_FLAG_ORTHONORMAL_FRAME))
+        return fail(TR_ERR_INVALID_ARGUMENT, "guided rendering needs TR_FLAG_ORTHONORMAL_FRAME (MIS needs the exact BSDF density)");
+    if (g->device != x->device) return fail(TR_ERR_INVALID_ARGUMENT, "guide and context are on different devices");
+    if (!(mix_prob > 0.0f && mix_prob < 1.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "mix_prob must be in (0, 1)");
+    if (!(lr >= 0.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "learning rate must be >= 0");
+    if (train_pool > (1u << 24)) return fail(TR_ERR_INVALID_ARGUMENT, "train_pool too large");
+    x->guide = g;
+    x->guide_mix = mix_prob;
+    x->guide_lr = lr;
+    x->guide_pool = train_pool;
+    x->gw_capacity = 0;             // (re)allocate guided buffers on the next render
     return TR_OK;
 }
 

@@ -12,151 +12,22 @@
 // records an error, waits (bounded) for its MMAs, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "tr_guide.cuh"
+#include "tr_guide_math.cuh"
+#include "tr_tcgen05.cuh"
 
 namespace trg {
 
-// ---------------------------------------------------------------------------------------------
-// PTX wrappers
-// ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_relinquish() {
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                          uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-        : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr)
-        : "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// UMMA shared-memory descriptor, K-major, no swizzle: core matrices of 8 rows x 16 bytes,
-// LBO = distance between the two K-halves of one K=16 step (128 B), SBO = distance between
-// 8-row groups (1024 B for a 64-wide K tile); bits 46-47 = 1 (sm100 descriptor version).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-    const uint64_t start = (addr >> 4) & 0x3FFFu;
-    const uint64_t lbo = 128u >> 4;
-    const uint64_t sbo = 1024u >> 4;
-    return start | (lbo << 16) | (sbo << 32) | (1ull << 46);
-}
-// instruction descriptor: D = F32, A = B = BF16, both K-major, N = 64, M = 128
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
-
-// byte offset of element (row, k) of a [rows][64] bf16 tile in the canonical layout
-__host__ __device__ __forceinline__ uint32_t canon_off(uint32_t row, uint32_t k) {
-    return (row >> 3) * 1024u + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
-}
-
-constexpr uint32_t kSpin = 1u << 24;    // bounded mbarrier wait
-
-__device__ __forceinline__ uint32_t pack2(float a, float b) {
-    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<uint32_t*>(&h);
-}
-__device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
-__device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
-
-// Issues the four K=16 MMAs of one layer and waits (bounded) for them; returns false on timeout.
-// Called by all threads; thread 0 issues and waits, the others meet it at the barrier.
-__device__ __forceinline__ bool layer_mma(uint32_t taddr, uint32_t a_addr, uint32_t b_addr, uint64_t* bar,
-                                          uint32_t& phase, volatile int* s_ok) {
-    fence_proxy_async();
-    tc_fence_before();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        tc_fence_after();
-#pragma unroll
-        for (uint32_t k = 0; k < 4; ++k)
-            umma_bf16(taddr, smem_desc(a_addr + k * 256u), smem_desc(b_addr + k * 256u), kIdesc, k > 0 ? 1u : 0u);
-        umma_commit(bar);
-        uint32_t it = 0;
-        bool done = false;
-        while (!(done = mbar_try_wait(bar, phase)) && ++it < kSpin) {}
-        *s_ok = done ? 1 : 0;
-    }
-    __syncthreads();
-    phase ^= 1u;
-    tc_fence_after();
-    return *s_ok != 0;
-}
-
-__device__ __forceinline__ void drain_and_free(uint32_t taddr, uint64_t* bar, uint32_t phase, bool ok) {
-    if (!ok && threadIdx.x == 0) {               // let in-flight MMAs land before freeing TMEM
-        uint32_t it = 0;
-        while (!mbar_try_wait(bar, phase ^ 1u) && ++it < kSpin) {}
-    }
-    tc_fence_before();
-    __syncthreads();
-    if ((threadIdx.x >> 5) == 0) tmem_dealloc(taddr, 64);
-}
-
-// shared memory: 4 weight tiles (32 KB) | A tile (16 KB) | bias (1 KB) | mbarrier | tmem slot | flag
-constexpr uint32_t kSmemW = 0, kSmemA = 32768, kSmemBias = 49152, kSmemBar = 50176, kSmemSlot = 50184,
-                   kSmemOk = 50188, kSmemBytes = 50192;
-
-__device__ __forceinline__ void stage_weights(uint8_t* smem, const uint4* w, const float* bias) {
-    uint4* sw = reinterpret_cast<uint4*>(smem + kSmemW);
-    for (uint32_t i = threadIdx.x; i < 2048u; i += blockDim.x) sw[i] = __ldg(&w[i]);
-    float* sb = reinterpret_cast<float*>(smem + kSmemBias);
-    for (uint32_t i = threadIdx.x; i < 256u; i += blockDim.x) sb[i] = __ldg(&bias[i]);
-}
-
-__device__ __forceinline__ void store_row_a(uint8_t* sA, uint32_t row, const uint4* v) {
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) *reinterpret_cast<uint4*>(sA + (row >> 3) * 1024u + c * 128u + (row & 7u) * 16u) = v[c];
-}
 
 // ---------------------------------------------------------------------------------------------
 // forward: out[m][0..40) = L4(relu(L3(relu(L2(relu(L1(x)))))));  act (optional) = H1, H2, H3
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) k_mlp_fwd(GuideDev g, const uint4* __restrict__ x, uint32_t m,
-                                                    float* __restrict__ out, uint4* __restrict__ act, int* err) {
+__global__ void __launch_bounds__(128, 4) k_mlp_fwd(GuideDev g, const uint4* __restrict__ x, uint32_t m,
+                                                    const uint32_t* __restrict__ m_dev, float* __restrict__ out,
+                                                    uint4* __restrict__ act, int* err) {
+    if (m_dev) m = min(m, *m_dev);      // row count produced on the device (guided rendering)
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sA = smem + kSmemA;
     const float* sB = reinterpret_cast<const float*>(smem + kSmemBias);
@@ -215,7 +86,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(GuideDev g, const uint4* __r
 // backward through the hidden layers: given dY = dL/d(out) (bf16, cols >= 40 zero) and the
 // stored activations, dh[2] = dH3 = (dY W4^T) * 1[H3>0], dh[1] = dH2, dh[0] = dH1 (FP32).
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) k_mlp_bwd(GuideDev g, const uint4* __restrict__ dy,
+__global__ void __launch_bounds__(128, 4) k_mlp_bwd(GuideDev g, const uint4* __restrict__ dy,
                                                     const uint4* __restrict__ act, uint32_t m,
                                                     float* __restrict__ dh, int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -273,14 +144,37 @@ __global__ void __launch_bounds__(128, 1) k_mlp_bwd(GuideDev g, const uint4* __r
     drain_and_free(taddr, bar, phase, ok);
 }
 
-int mlp_grid(int device) {
-    int sms = 0;
+int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem) {
+    int sms = 1, smem_sm = 0, regs_sm = 0, warps_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    return sms > 0 ? sms : 1;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device);
+    cudaDeviceGetAttribute(&warps_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return sms > 0 ? sms : 1;
+    const int per_cta_smem = (int)dyn_smem + (int)fa.sharedSizeBytes + 1024;     // 1 KB reserved per CTA
+    const int regs = fa.numRegs > 0 ? ((fa.numRegs + 7) / 8) * 8 : 1;
+    int per_sm = std::min(smem_sm / per_cta_smem, regs_sm / (regs * threads));
+    per_sm = std::min(per_sm, warps_sm / threads);
+    per_sm = std::min(per_sm, 512 / 64);                                          // 64 TMEM columns each
+    if (per_sm < 1) per_sm = 1;
+    return (sms > 0 ? sms : 1) * per_sm;
+}
+
+int mlp_grid(int device) {
+    static int grid = 0;
+    if (!grid) grid = resident_grid(device, reinterpret_cast<const void*>(k_mlp_fwd), 128, kSmemBytes);
+    return grid;
+}
+
+static int mlp_bwd_grid(int device) {
+    static int grid = 0;
+    if (!grid) grid = resident_grid(device, reinterpret_cast<const void*>(k_mlp_bwd), 128, kSmemBytes);
+    return grid;
 }
 
 cudaError_t mlp_forward(const GuideDev& g, const uint4* x, uint32_t m, float* out, uint4* act, int* err,
-                        cudaStream_t s) {
+                        cudaStream_t s, const uint32_t* m_dev) {
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
@@ -291,7 +185,7 @@ cudaError_t mlp_forward(const GuideDev& g, const uint4* x, uint32_t m, float* ou
     cudaGetDevice(&dev);
     const uint32_t tiles = (m + kTile - 1) / kTile;
     const uint32_t grid = tiles < (uint32_t)mlp_grid(dev) ? tiles : (uint32_t)mlp_grid(dev);
-    k_mlp_fwd<<<grid, 128, kSmemBytes, s>>>(g, x, m, out, act, err);
+    k_mlp_fwd<<<grid, 128, kSmemBytes, s>>>(g, x, m, m_dev, out, act, err);
     return cudaGetLastError();
 }
 
@@ -306,7 +200,7 @@ cudaError_t mlp_backward(const GuideDev& g, const uint4* dy, const uint4* act, u
     int dev = 0;
     cudaGetDevice(&dev);
     const uint32_t tiles = (m + kTile - 1) / kTile;
-    const uint32_t grid = tiles < (uint32_t)mlp_grid(dev) ? tiles : (uint32_t)mlp_grid(dev);
+    const uint32_t grid = tiles < (uint32_t)mlp_bwd_grid(dev) ? tiles : (uint32_t)mlp_bwd_grid(dev);
     k_mlp_bwd<<<grid, 128, kSmemBytes, s>>>(g, dy, act, m, dh, err);
     return cudaGetLastError();
 }
@@ -322,36 +216,6 @@ __global__ void k_pack_weights(const float* __restrict__ params, uint8_t* __rest
     // forward B tile: rows = output, K = input;  backward B tile: rows = input, K = output
     *reinterpret_cast<__nv_bfloat16*>(w_fwd + l * 8192u + canon_off(o, in)) = v;
     *reinterpret_cast<__nv_bfloat16*>(w_bwd + l * 8192u + canon_off(in, o)) = v;
-}
-
-// vMF mixture decoding shared by sampling and training
-struct Lobe { float pi, mx, my, mz, kappa, mnorm, sig; };
-
-__device__ __forceinline__ float softplusf(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
-
-__device__ __forceinline__ void decode_mixture(const float* o, Lobe* L) {
-    float amax = -3.4e38f;
-#pragma unroll
-    for (int j = 0; j < kLobes; ++j) amax = fmaxf(amax, o[5 * j]);
-    float sum = 0.0f;
-#pragma unroll
-    for (int j = 0; j < kLobes; ++j) { L[j].pi = expf(o[5 * j] - amax); sum += L[j].pi; }
-#pragma unroll
-    for (int j = 0; j < kLobes; ++j) {
-        L[j].pi /= sum;
-        const float x = o[5 * j + 1], y = o[5 * j + 2], z = o[5 * j + 3];
-        float n = sqrtf(x * x + y * y + z * z);
-        if (!(n > 1e-6f)) { L[j].mx = 0.0f; L[j].my = 0.0f; L[j].mz = 1.0f; n = 1e-6f; }
-        else { L[j].mx = x / n; L[j].my = y / n; L[j].mz = z / n; }
-        L[j].mnorm = n;
-        const float kr = o[5 * j + 4];
-        L[j].kappa = fminf(softplusf(kr) + kKappaMin, kKappaMax);
-        L[j].sig = (softplusf(kr) + kKappaMin < kKappaMax) ? 1.0f / (1.0f + expf(-kr)) : 0.0f;
-    }
-}
-// log of the normalised vMF density, stable for small and large kappa
-__device__ __forceinline__ float log_vmf(float kappa, float cosang) {
-    return logf(kappa) - 1.83787706f /* log 2pi */ - log1pf(-expf(-2.0f * kappa)) + kappa * (cosang - 1.0f);
 }
 
 // training loss -(w/W) log q(dir) and its gradient w.r.t. the 40 raw outputs; dy bf16 (and

@@ -28,11 +28,15 @@ struct GuideDev {
     const float* bias;     // [4][64]
 };
 
+// m_dev (optional): the row count in device memory, at most m (rows beyond it are skipped)
 cudaError_t mlp_forward(const GuideDev& g, const uint4* x, uint32_t m, float* out, uint4* act, int* err,
-                        cudaStream_t s);
+                        cudaStream_t s, const uint32_t* m_dev = nullptr);
 cudaError_t mlp_backward(const GuideDev& g, const uint4* dy, const uint4* act, uint32_t m, float* dh, int* err,
                          cudaStream_t s);
 int mlp_grid(int device);
+// CTAs of `kernel` that fit on the device at once (SMs x CTAs per SM, from the kernel's
+// registers and shared memory), for persistent tile loops
+int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem);
 cudaError_t pack_weights(const float* params, uint8_t* w_fwd, uint8_t* w_bwd, cudaStream_t s);
 cudaError_t mix_grad(const float* out, const float* dirs, const float* w, uint32_t m, float* wsum, uint4* dy_bf,
                      float* dy_f, float* loss, cudaStream_t s);

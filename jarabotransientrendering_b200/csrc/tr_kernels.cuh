@@ -3,6 +3,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "tr_guide.cuh"
+
 namespace trk {
 
 constexpr int kStack = 64;          // max traversal stack entries per thread (BVH depth + 1)
@@ -26,6 +28,24 @@ struct SceneDev {
     float lambda;             // mean extinction avg(sigma_t)
     float g;
     uint32_t bvh_depth;       // deepest leaf; the traversal stack holds bvh_depth + 1 entries
+    float bmin[3], binv[3];   // scene box (feature normalisation of the learned proposal)
+};
+
+constexpr uint32_t kFlagOrthoFrame = 1u;   // TR_FLAG_ORTHONORMAL_FRAME
+
+// Guided mode state (all null when rendering without the learned proposal).
+struct GuideWave {
+    uint32_t* gq;             // [capacity] slots whose direction waits for the proposal
+    trg::GuideDev net;        // network weights (canonical tiles) and biases
+    int* err;                 // set to 1 when a tensor-core wait times out
+    float mix_prob;           // probability of sampling the proposal (else the BSDF)
+    // training pool
+    uint4* pool_feat;         // [pool_cap][64] bf16
+    float* pool_dir;          // [pool_cap][3]
+    float* pool_w;            // [pool_cap] target weight (filled by k_train_gather)
+    uint4* pool_meta;         // [pool_cap] slot, depth, throughput luminance (bits), unused
+    uint32_t pool_cap;
+    float keep_prob;          // probability that a guided vertex becomes a training sample
 };
 
 struct CameraDev {
@@ -79,15 +99,19 @@ struct Params {
     uint32_t max_bounces;
     uint32_t sqrt_spp;
     uint32_t bvh_depth;
+    uint32_t flags;
+    GuideWave guide;
 };
 
 // counters layout (uint32): [0, 64) extend counts per depth, [64, 128) shadow counts per
-// depth, [128, 192) extend fetch cursors, [192, 256) shadow fetch cursors.
-constexpr int kCounters = 256;
+// depth, [128, 192) extend fetch cursors, [192, 256) shadow fetch cursors, [256, 320)
+// guided-vertex counts per depth; training-pool fill lives in its own counter.
+constexpr int kCounters = 320;
 __host__ __device__ constexpr int cnt_ext(int d) { return d; }
 __host__ __device__ constexpr int cnt_sh(int d) { return 64 + d; }
 __host__ __device__ constexpr int cur_ext(int d) { return 128 + d; }
 __host__ __device__ constexpr int cur_sh(int d) { return 192 + d; }
+__host__ __device__ constexpr int cnt_guide(int d) { return 256 + d; }
 
 // host launchers (tr_kernels.cu)
 cudaError_t launch_raygen(const Params& p, cudaStream_t s);
@@ -97,6 +121,9 @@ cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);
+// fused proposal inference + one-sample MIS direction sampling of the guided vertices of `depth`
+cudaError_t launch_guide(const Params& p, int depth, uint32_t* pool_state, cudaStream_t s);
+cudaError_t launch_train_gather(const Params& p, uint32_t* pool_state, cudaStream_t s);
 int trace_grid_size(int device, uint32_t bvh_depth);
 size_t trace_smem_bytes(uint32_t bvh_depth);
 size_t splat_smem_bytes(uint32_t T, int pixels_per_cta);

@@ -68,7 +68,7 @@ class Context:
         pos, nv, uv, vv, fd = scene.camera.basis()
         cam = _abi.Camera(_abi.f3(*pos), _abi.f3(*nv), _abi.f3(*uv), _abi.f3(*vv), float(fd))
         film = _abi.Film(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset)
-        integ = _abi.Integrator(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, 0, scene.seed)
+        integ = _abi.Integrator(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, scene.flags, scene.seed)
         h = C.c_void_p()
         _abi.check(L.tr_create(C.byref(sc), C.byref(cam), C.byref(film), C.byref(integ), device, C.byref(h)))
         self.h = h
@@ -122,6 +122,12 @@ class Context:
         _abi.check(_abi.lib().tr_trace_rays_device(self.h, C.c_void_p(d_rays_ptr), n, int(any_hit),
                                                    C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr)))
 
+    def set_guide(self, guide, mix_prob=0.5, learning_rate=1e-3, train_pool=262144):
+        """Render with the learned proposal (tr_set_guide); guide=None detaches."""
+        _abi.check(_abi.lib().tr_set_guide(self.h, guide.h if guide is not None else None, mix_prob,
+                                           learning_rate, train_pool))
+        self._guide = guide
+
     def stats(self):
         s = _abi.Stats()
         _abi.check(_abi.lib().tr_stats_get(self.h, C.byref(s)))
@@ -137,6 +143,38 @@ class Context:
 
     def __exit__(self, *a):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Guide:
+    """Learned directional proposal: MLP -> mixture of 8 von Mises-Fisher lobes (tr_guide_*)."""
+
+    PARAMS = 16640
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        h = C.c_void_p()
+        _abi.check(_abi.lib().tr_guide_create(device, seed, C.byref(h)))
+        self.h = h
+
+    def params(self):
+        p = np.zeros(self.PARAMS, np.float32)
+        _abi.check(_abi.lib().tr_guide_get_params(self.h, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.PARAMS
+        _abi.check(_abi.lib().tr_guide_set_params(self.h, p.ctypes.data))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.lib().tr_guide_destroy(self.h)
+            self.h = None
 
     def __del__(self):
         try:

@@ -45,6 +45,8 @@ MAT_GGX = 1
 LIGHT_POINT = 0
 LIGHT_RECT = 1
 
+FLAG_ORTHONORMAL_FRAME = 1
+
 
 @dataclasses.dataclass
 class Material:
@@ -128,6 +130,7 @@ class Scene:
     incoming_samples: int
     medium: Optional[Medium] = None
     seed: int = 1
+    flags: int = 0            # FLAG_ORTHONORMAL_FRAME: Lambertian sampling in an orthonormal frame
 
     # ---- flattened arrays (what the C ABI takes) -------------------------
     def flatten(self):

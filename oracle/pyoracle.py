@@ -51,7 +51,7 @@ class FilmS(C.Structure):
 
 class IntegratorS(C.Structure):
     _fields_ = [("max_bounces", C.c_uint32), ("sqrt_spp", C.c_uint32), ("incoming_samples", C.c_uint32),
-                ("reserved", C.c_uint32), ("seed", C.c_uint64)]
+                ("flags", C.c_uint32), ("seed", C.c_uint64)]
 
 
 class Hit(C.Structure):
@@ -144,7 +144,7 @@ class Oracle:
         pos, nv, uv, vv, fd = scene.camera.basis()
         cam = CameraS(f3(*pos), f3(*nv), f3(*uv), f3(*vv), float(fd))
         film = FilmS(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset)
-        integ = IntegratorS(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, 0, scene.seed)
+        integ = IntegratorS(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, scene.flags, scene.seed)
         h = C.c_void_p()
         rc = lib().orc_create(C.byref(s), C.byref(cam), C.byref(film), C.byref(integ), C.byref(h))
         if rc != 0:

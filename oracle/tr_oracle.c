@@ -757,6 +757,14 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
         v3 fa; float pa; v3 nd;
         if (surface && ggx) {
             if (!ggx_sample(kd, alpha, n, wo, sp, cp, x2, &nd, &fa, &pa)) break;
+        } else if (surface && (x->integ.flags & ORC_FLAG_ORTHONORMAL_FRAME)) {
+            /* cosine sampling in an orthonormal frame (Duff et al. 2017) */
+            float ct = sqrtf(x2);
+            float stt = sqrtf(1.0f - ct * ct);
+            frame3 Fr = make_frame(n);
+            nd = to_world(&Fr, mk(cp * stt, sp * stt, ct));
+            fa = mk((kd.x * INV_PI_F) * ct, (kd.y * INV_PI_F) * ct, (kd.z * INV_PI_F) * ct);
+            pa = ct * INV_PI_F;
         } else if (surface) {
             /* Lambertian cosine sampling in the frame of Intersection::set_coordinate_system */
             float ct = sqrtf(x2);

@@ -57,7 +57,8 @@ typedef struct orc_scene {
 } orc_scene;
 typedef struct orc_camera { float position[3]; float nv[3]; float uv[3]; float vv[3]; float focal_distance; } orc_camera;
 typedef struct orc_film { uint32_t width, height, time_bins; float exposure; float offset; } orc_film;
-typedef struct orc_integrator { uint32_t max_bounces, sqrt_spp, incoming_samples, reserved; uint64_t seed; } orc_integrator;
+typedef struct orc_integrator { uint32_t max_bounces, sqrt_spp, incoming_samples, flags; uint64_t seed; } orc_integrator;
+#define ORC_FLAG_ORTHONORMAL_FRAME 1u
 typedef struct orc_hit { float t; uint32_t prim_id; float u, v; } orc_hit;
 
 typedef struct orc_ctx orc_ctx;

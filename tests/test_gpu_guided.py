@@ -1,0 +1,119 @@
+"""GPU tests of guided rendering: the learned proposal combined with BSDF sampling by one-sample
+MIS must leave the estimator unbiased (guided and plain films agree statistically, whether the
+network is untrained or trained online during the renders), and the orthonormal-frame plain
+sampler it is compared against is bit-for-bit the oracle's."""
+import numpy as np
+import pytest
+
+from jarabotransientrendering_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+RTOL_TILE = 2e-5
+
+
+def guided_scene(width=32, height=32, time_bins=128, exposure=0.04):
+    sc = S.guided(width=width, height=height, time_bins=time_bins, exposure=exposure, sqrt_spp=4, max_bounces=6)
+    sc.flags = S.FLAG_ORTHONORMAL_FRAME
+    return sc
+
+
+def test_orthonormal_frame_matches_oracle(gpu, oracle_lib):
+    for sc in (S.cornell(width=24, height=24, time_bins=256, exposure=0.02, sqrt_spp=4), guided_scene(24, 24, 256, 0.02)):
+        sc.flags = S.FLAG_ORTHONORMAL_FRAME
+        with gpu.Context(sc) as ctx:
+            ctx.render(0, 16)
+            fg = ctx.film()
+        fo = oracle_lib.Oracle(sc).render(sample_count=16, nthreads=8)
+        assert ((fg["streak"] != 0) == (fo["streak"] != 0)).all()
+        assert np.allclose(fg["streak"], fo["streak"], rtol=RTOL_TILE, atol=1e-12)
+
+
+def _films(gpu, sc, K, spp, guide=None, train_pool=0):
+    out = []
+    with gpu.Context(sc) as ctx:
+        if guide is not None:
+            ctx.set_guide(guide, mix_prob=0.5, learning_rate=1e-3, train_pool=train_pool)
+        for k in range(K):
+            ctx.clear()
+            ctx.render(spp * k, spp)
+            out.append(ctx.film(steady=False, weight=False)["streak"])
+        st = ctx.stats()
+    return np.array(out), st
+
+
+def _z(a, b):
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    m = se > 0
+    return (a.mean(0) - b.mean(0))[m] / se[m]
+
+
+def _compare(a, b, tile=8, window=8):
+    """Two-sample z-scores of aggregates that each sum thousands of paths, so are close to
+    normal: total energy, 8x8-pixel tiles and 8-bin time windows. Single bins or pixels are
+    sparse and heavy-tailed, and their tails differ between the samplers (one-sample MIS with an
+    untrained mixture gives rarer, larger contributions than BSDF sampling), which skews their
+    z-scores even when both estimators are unbiased."""
+    K, H, W, T, _ = a.shape
+
+    def tiles(x):
+        return x.sum(axis=(3, 4)).reshape(len(x), H // tile, tile, W // tile, tile).sum(axis=(2, 4)).reshape(len(x), -1)
+
+    def windows(x):
+        return x.sum(axis=(1, 2, 4)).reshape(len(x), T // window, window).sum(axis=2)
+
+    ez = _z(a.sum(axis=(1, 2, 3, 4)), b.sum(axis=(1, 2, 3, 4)))[0]
+    zt, zw = _z(tiles(a), tiles(b)), _z(windows(a), windows(b))
+    return {"energy_z": float(ez), "energy_rel": float(a.sum() / b.sum() * len(b) / len(a) - 1),
+            "tile_max_z": float(np.abs(zt).max()), "tile_mean_z": float(zt.mean()),
+            "window_max_z": float(np.abs(zw).max()), "window_mean_z": float(zw.mean())}
+
+
+@pytest.mark.parametrize("train", [False, True])
+def test_guided_render_is_unbiased(gpu, train):
+    sc = guided_scene()
+    K = 40
+    plain, _ = _films(gpu, sc, K, 64)
+    g = gpu.Guide(seed=5)
+    try:
+        guided, st = _films(gpu, sc, K, 64, guide=g, train_pool=32768 if train else 0)
+    finally:
+        g.close()
+    r = _compare(guided, plain)
+    assert abs(r["energy_z"]) < 4.0 and abs(r["energy_rel"]) < 0.05, r
+    assert r["tile_max_z"] < 4.5 and r["window_max_z"] < 4.5, r
+    if train:
+        assert st["train_steps"] >= 1 and np.isfinite(st["train_loss"])
+
+
+def test_guided_training_updates_the_network(gpu):
+    sc = guided_scene(64, 64, 128, 0.04)
+    g = gpu.Guide(seed=9)
+    try:
+        p0 = g.params()
+        with gpu.Context(sc) as ctx:
+            ctx.set_guide(g, mix_prob=0.5, learning_rate=1e-3, train_pool=65536)
+            losses = []
+            for k in range(6):
+                ctx.render(16 * k, 16)
+                st = ctx.stats()
+                assert st["train_steps"] >= 1
+                losses.append(st["train_loss"])
+            f = ctx.film()
+        p1 = g.params()
+    finally:
+        g.close()
+    assert np.isfinite(losses).all()
+    assert np.abs(p1 - p0).max() > 1e-4
+    assert np.isfinite(f["streak"]).all() and f["streak"].sum() > 0
+
+
+def test_guide_requires_orthonormal_frame(gpu):
+    sc = S.guided(width=16, height=16, time_bins=64, exposure=0.08, sqrt_spp=2)
+    g = gpu.Guide()
+    try:
+        with gpu.Context(sc) as ctx:
+            with pytest.raises(gpu.TransientError):
+                ctx.set_guide(g)
+    finally:
+        g.close()
