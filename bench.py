@@ -31,6 +31,8 @@ B_SHADOW = 48 + 64 * 16.98375084460311 + 48 * 6.767252594318216       # 1459.8 B
 TRAFFIC_PER_EXTEND_LAUNCH = None
 
 WORKLOAD = "icosphere"
+# throughput (value, paths/s) plus the "convergence" object: time to 5% rel-L2, guided vs plain
+METRIC = "paths/s; time to 5% rel-L2 streak-film error, guided vs plain, 1 B200"
 
 
 def parse():
@@ -42,6 +44,10 @@ def parse():
     ap.add_argument("--spp-per-step", type=int, default=None, help="default: the workload's 256")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-convergence", action="store_true",
+                    help="skip the time-to-5%%-rel-L2 comparison of guided and plain sampling")
+    ap.add_argument("--convergence-ref-spp", type=int, default=131072,
+                    help="samples per pixel of each of the two halves of the converged reference")
     return ap.parse_args()
 
 
@@ -153,7 +159,7 @@ def run_reference(args, rank, world):
     rows = max(1, args.steps)
     cb = cpu_reference(sc, rows, procs)
     paths_per_step = sc.paths_per_frame()
-    line = {"impl": "reference", "metric": "paths/s", "value": cb["value"], "unit": "paths/s", "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "paths/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": paths_per_step / cb["value"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8",
@@ -161,6 +167,50 @@ def run_reference(args, rank, world):
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def convergence(args, device):
+    """Time to 5% rel-L2 of the streak film, plain BSDF sampling vs the learned proposal, on the
+    guided workload (GGX floor, 0.05 x 0.05 area light hidden behind an occluder slab, 512 x 512,
+    2048 bins).  Reference: the plain tracer, two independent halves of ``convergence_ref_spp``
+    samples per pixel (its own noise is subtracted from the error).  Both samplers render passes of
+    64 samples per pixel from a fresh context and network; the guided run trains online (batches
+    of 65,536 samples, Adam lr 3e-3, mixture probability 0.7) and drops its first 1,024 samples
+    per pixel after training on them.  Time = host wall clock of the render calls (training
+    included); the error evaluation between passes is not timed."""
+    import torch
+    from jarabotransientrendering_b200 import convergence as CV, renderer as R, scenes as S
+    sc = S.guided()
+    sc.flags = S.FLAG_ORTHONORMAL_FRAME
+    t0 = time.perf_counter()
+    ref = CV.Reference(sc, args.convergence_ref_spp, device=device)
+    ref_s = time.perf_counter() - t0
+    plain = CV.time_to_error(sc, ref, target=0.05, pass_spp=64, max_spp=262144, device=device)
+    g = R.Guide(device=device, seed=1)
+    try:
+        guided = CV.time_to_error(sc, ref, target=0.05, pass_spp=64, max_spp=262144, guide=g, mix_prob=0.7,
+                                  learning_rate=3e-3, train_pool=262144, device=device, warmup_spp=1024)
+    finally:
+        g.close()
+    ref_noise = ref.rel_noise
+    del ref
+    torch.cuda.empty_cache()
+
+    def leg(r):
+        return {"seconds": r["seconds"], "spp": r["spp"], "warmup_spp": r["warmup_spp"],
+                "paths_per_s": r["paths_per_s"], "train_steps": r["train_steps"],
+                "rel_l2_at_stop": r["curve"][-1][2] if r["curve"] else None}
+    res = {"metric": "seconds to 5% rel-L2 streak-film error (lower is better)", "unit": "s",
+           "workload": "guided: Cornell box, GGX floor (alpha 0.2), 0.05x0.05 area light behind an occluder "
+                       "slab, 512x512, 2048 bins x 0.0025, depth 8, orthonormal shading frames",
+           "reference": {"tracer": "plain", "spp": 2 * args.convergence_ref_spp, "rel_noise": ref_noise,
+                         "seconds": ref_s},
+           "plain": leg(plain),
+           "guided": dict(leg(guided), mix_prob=0.7, learning_rate=3e-3, train_batch=65536),
+           "passes_spp": 64}
+    if plain["seconds"] and guided["seconds"]:
+        res["speedup_guided_vs_plain"] = plain["seconds"] / guided["seconds"]
+    return res
 
 
 def main():
@@ -252,7 +302,7 @@ def main():
                 "kernel_ms_per_step": {k: v / args.steps for k, v in kern.items()},
                 "queries_per_step": {"closest": closest / args.steps, "shadow": shadow / args.steps}}
 
-    out = {"metric": "paths/s", "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+    out = {"metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8",
@@ -307,6 +357,11 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         procs = max(1, min(os.cpu_count() or 1, 32))
         out["cpu_baseline"] = cpu_reference(sc, 1, procs)
+    if rank == 0 and world == 1 and not args.no_convergence:
+        try:
+            out["convergence"] = convergence(args, local)
+        except Exception as e:            # reported, not fatal: the throughput line stands
+            out["convergence"] = {"error": f"{type(e).__name__}: {e}"}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

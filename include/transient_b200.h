@@ -235,7 +235,7 @@ tr_status tr_render_region_noalloc(tr_ctx* ctx, uint32_t x0, uint32_t y0, uint32
  * An MLP maps a surface vertex's features (64 BF16 values: sin/cos encoded position, position,
  * normal, outgoing direction, normalised path length, zero padding) through three hidden
  * layers of 64 ReLU units to 8 von Mises-Fisher lobes (per lobe: weight logit, unnormalised
- * mean xyz, concentration before softplus).  Forward and hidden-layer backward run as BF16
+ * mean xyz, raw concentration r with kappa = 0.05 + 2000 sigmoid(r - 8)).  Forward and hidden-layer backward run as BF16
  * tcgen05 tensor-core kernels with FP32 accumulation; training minimises
  * -sum_i w_i log q(dir_i | x_i) / sum_i w_i with Adam.
  * Parameters (TR_GUIDE_PARAMS floats): weights [4][64 in][64 out], then biases [4][64]. */

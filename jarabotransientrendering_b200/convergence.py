@@ -83,30 +83,49 @@ class Reference:
 def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp: int = 4,
                   max_spp: int = 4096, guide: Optional[R.Guide] = None, mix_prob: float = 0.5,
                   learning_rate: float = 1e-3, train_pool: int = 262144, device: int = 0,
-                  sample_offset: int = 1 << 20):
+                  sample_offset: int = 1 << 20, warmup_spp: int = 0):
     """Renders ``scene`` progressively, ``pass_spp`` samples per pixel per pass, until the film's
     rel-L2 against ``ref`` is at most ``target`` (or ``max_spp`` is reached). Sample indices start
     at ``sample_offset``, so the passes are independent of the reference's samples.
 
+    With a learned proposal, the first ``warmup_spp`` samples per pixel train the network and are
+    then dropped from the film (the film is cleared once), as in the iterative schemes of path
+    guiding; their render and training time counts like every other pass.
+
     Returns {"seconds": render wall time to the target (None if not reached), "spp": samples per
-    pixel then, "paths_per_s", "curve": [(spp, seconds, rel_l2), ...]}."""
+    pixel in the film then, "warmup_spp", "paths_per_s", "curve": [(spp in film, seconds, rel_l2),
+    ...], "train_steps", "train_loss"}."""
     torch = _torch()
     curve = []
     buf = None
     spent = 0.0
     reached = None
     train_steps = 0
+    rendered = 0
     with R.Context(scene, device) as ctx:
         if guide is not None:
             ctx.set_guide(guide, mix_prob=mix_prob, learning_rate=learning_rate, train_pool=train_pool)
+        else:
+            warmup_spp = 0
+        while rendered < warmup_spp:
+            n = min(pass_spp, warmup_spp - rendered)
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            ctx.render(sample_offset + rendered, n)
+            spent += time.perf_counter() - t0
+            rendered += n
+            train_steps += ctx.stats()["train_steps"]
+        if warmup_spp:
+            ctx.clear()
         spp = 0
         while spp < max_spp:
             n = min(pass_spp, max_spp - spp)
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
-            ctx.render(sample_offset + spp, n)
+            ctx.render(sample_offset + rendered, n)
             spent += time.perf_counter() - t0
             spp += n
+            rendered += n
             st = ctx.stats()
             train_steps += st["train_steps"]
             buf = film_device(ctx, buf)
@@ -115,7 +134,8 @@ def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp
             if err <= target:
                 reached = (spent, spp)
                 break
-    paths = spp * scene.width * scene.height * scene.incoming_samples
+        train_loss = ctx.stats()["train_loss"]
+    paths = rendered * scene.width * scene.height * scene.incoming_samples
     return {"seconds": reached[0] if reached else None, "spp": reached[1] if reached else None,
-            "paths_per_s": paths / spent if spent > 0 else 0.0, "curve": curve,
-            "train_steps": train_steps, "train_loss": st["train_loss"]}
+            "warmup_spp": warmup_spp, "paths_per_s": paths / spent if spent > 0 else 0.0, "curve": curve,
+            "train_steps": train_steps, "train_loss": train_loss}

@@ -230,8 +230,8 @@ void ensure_guided(tr_ctx* x, uint32_t capacity) {
         x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), p), x->allocs.end());
     };
     trk::GuideWave& g = x->gw;
-    drop(g.gq); drop(g.pool_feat); drop(g.pool_dir); drop(g.pool_w); drop(g.pool_meta);
-    g.gq = x->alloc<uint32_t>(capacity);
+    drop(g.vrec); drop(g.pool_feat); drop(g.pool_dir); drop(g.pool_w); drop(g.pool_meta);
+    g.vrec = x->alloc<uint4>((size_t)capacity * 5);
     const uint32_t pc = std::max<uint32_t>(1u, x->guide_pool);
     g.pool_feat = x->alloc<uint4>((size_t)pc * 8);
     g.pool_dir = x->alloc<float>((size_t)pc * 3);
@@ -950,31 +950,42 @@ extern "C" tr_status tr_guide_forward(tr_guide* g, const uint16_t* d_features, u
     }
 }
 
+namespace {
+// Enqueues one training step (forward, loss gradient, backward, weight gradients, Adam, weight
+// repacking) on stream s without waiting for it; the loss lands in g->scalars[1].
+void train_enqueue(tr_guide* g, const uint4* x, const float* d_dirs, const float* d_weights, uint32_t n, float lr,
+                   cudaStream_t s) {
+    g->ensure(n);
+    TR_CUDA(trg::mlp_forward(g->dev(), x, n, g->out, g->act, g->err, s));
+    TR_CUDA(cudaMemsetAsync(g->scalars, 0, 4 * sizeof(float), s));
+    TR_CUDA(trg::mix_grad(g->out, d_dirs, d_weights, n, g->scalars, g->dy_bf, g->dy_f, g->scalars + 1, s));
+    TR_CUDA(trg::mlp_backward(g->dev(), g->dy_bf, g->act, n, g->dh, g->err, s));
+    TR_CUDA(cudaMemsetAsync(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS, s));
+    float* gb = g->grads + 4 * 4096;
+    const size_t mrow = (size_t)n * 8;
+    trg::DwLayers dw{};
+    dw.prev[0] = x;                  dw.grad[0] = g->dh;
+    dw.prev[1] = g->act;             dw.grad[1] = g->dh + (size_t)n * 64;
+    dw.prev[2] = g->act + mrow;      dw.grad[2] = g->dh + (size_t)2 * n * 64;
+    dw.prev[3] = g->act + 2 * mrow;  dw.grad[3] = g->dy_f;                    // output layer
+    for (int l = 0; l < 4; ++l) { dw.gw[l] = g->grads + 4096 * l; dw.gb[l] = gb + 64 * l; }
+    TR_CUDA(trg::weight_grad(dw, n, s));
+    if (lr > 0.0f) {
+        g->step += 1;
+        TR_CUDA(trg::adam(g->params, g->grads, g->m1, g->m2, TR_GUIDE_PARAMS, lr, g->step, s));
+        TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, s));
+    }
+}
+}  // namespace
+
 extern "C" tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features, const float* d_dirs,
                                          const float* d_weights, uint32_t n, float lr, float* loss, void* stream) {
     if (!g || !n || !d_features || !d_dirs || !d_weights) return fail(TR_ERR_INVALID_ARGUMENT, "null argument or empty batch");
     if ((reinterpret_cast<uintptr_t>(d_features) & 15u) != 0) return fail(TR_ERR_INVALID_ARGUMENT, "features must be 16-byte aligned");
     try {
         TR_CUDA(cudaSetDevice(g->device));
-        g->ensure(n);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
-        const uint4* x = reinterpret_cast<const uint4*>(d_features);
-        TR_CUDA(trg::mlp_forward(g->dev(), x, n, g->out, g->act, g->err, s));
-        TR_CUDA(cudaMemsetAsync(g->scalars, 0, 4 * sizeof(float), s));
-        TR_CUDA(trg::mix_grad(g->out, d_dirs, d_weights, n, g->scalars, g->dy_bf, g->dy_f, g->scalars + 1, s));
-        TR_CUDA(trg::mlp_backward(g->dev(), g->dy_bf, g->act, n, g->dh, g->err, s));
-        TR_CUDA(cudaMemsetAsync(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS, s));
-        float* gb = g->grads + 4 * 4096;
-        const size_t mrow = (size_t)n * 8;
-        TR_CUDA(trg::weight_grad(x, g->dh, n, g->grads, gb, s));                                   // layer 1
-        TR_CUDA(trg::weight_grad(g->act, g->dh + (size_t)n * 64, n, g->grads + 4096, gb + 64, s));      // layer 2
-        TR_CUDA(trg::weight_grad(g->act + mrow, g->dh + (size_t)2 * n * 64, n, g->grads + 8192, gb + 128, s));
-        TR_CUDA(trg::weight_grad(g->act + 2 * mrow, g->dy_f, n, g->grads + 12288, gb + 192, s));        // output
-        if (lr > 0.0f) {
-            g->step += 1;
-            TR_CUDA(trg::adam(g->params, g->grads, g->m1, g->m2, TR_GUIDE_PARAMS, lr, g->step, s));
-            TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, s));
-        }
+        train_enqueue(g, reinterpret_cast<const uint4*>(d_features), d_dirs, d_weights, n, lr, s);
         if (loss) TR_CUDA(cudaMemcpyAsync(loss, g->scalars + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
         return guide_check_err(g, s);
     } catch (const CudaError& e) {
@@ -998,23 +1009,31 @@ int* guide_err(tr_guide* g) { return g->err; }
 
 // After a guided render: surface an MMA timeout, then train on the collected pool.
 tr_status guide_after_render(tr_ctx* x, cudaStream_t s) {
-    tr_status st = guide_check_err(x->guide, s);
-    if (st != TR_OK) return st;
     x->stats.train_steps = 0;
-    if (!x->guide_pool) return TR_OK;
+    if (!x->guide_pool) return guide_check_err(x->guide, s);
+    // one synchronisation for the render's MMA status and the pool fill ...
+    int e = 0;
     uint32_t fill = 0;
+    TR_CUDA(cudaMemcpyAsync(&e, x->guide->err, sizeof(int), cudaMemcpyDeviceToHost, s));
     TR_CUDA(cudaMemcpyAsync(&fill, x->pool_state, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     TR_CUDA(cudaStreamSynchronize(s));
+    if (e) return guide_check_err(x->guide, s);
+    // ... the training steps are enqueued back to back, and one more for their status and loss
     const uint32_t n = std::min(fill, x->guide_pool);
     const uint32_t batch = 65536;
-    for (uint32_t off = 0; off + 1024 <= n; off += batch) {
-        const uint32_t m = std::min(batch, n - off);
-        float loss = 0.0f;
-        st = tr_guide_train_step(x->guide, reinterpret_cast<const uint16_t*>(x->gw.pool_feat + (size_t)off * 8),
-                                 x->gw.pool_dir + (size_t)off * 3, x->gw.pool_w + off, m, x->guide_lr, &loss, s);
-        if (st != TR_OK) return st;
-        x->stats.train_steps += 1;
-        x->stats.train_loss = loss;
+    try {
+        for (uint32_t off = 0; off + 1024 <= n; off += batch) {
+            const uint32_t m = std::min(batch, n - off);
+            train_enqueue(x->guide, x->gw.pool_feat + (size_t)off * 8, x->gw.pool_dir + (size_t)off * 3,
+                          x->gw.pool_w + off, m, x->guide_lr, s);
+            x->stats.train_steps += 1;
+        }
+    } catch (const CudaError& err) {
+        return fail(err.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, err.what());
+    }
+    if (x->stats.train_steps) {
+        TR_CUDA(cudaMemcpyAsync(&x->stats.train_loss, x->guide->scalars + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+        return guide_check_err(x->guide, s);
     }
     return TR_OK;
 }
@@ -1032,8 +1051,7 @@ extern "C" tr_status tr_set_guide(tr_ctx* x, tr_guide* g, float mix_prob, float 
     x->guide = g;
     x->guide_mix = mix_prob;
     x->guide_lr = lr;
-    x->guide_pool = train_pool;
-    x->gw_capacity = 0;             // (re)allocate guided buffers on the next render
+    x->guide_pool = train_pool;     // ensure_guided reallocates the pool when its size changes
     return TR_OK;
 }
 

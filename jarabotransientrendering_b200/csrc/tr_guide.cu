@@ -281,47 +281,56 @@ __global__ void k_sum(const float* __restrict__ w, uint32_t m, float* __restrict
     if ((threadIdx.x & 31u) == 0) atomicAdd(out, s);
 }
 
-// weight gradient of layer l: gw[in][out] += sum_rows prev[row][in] * grad[row][out];
-// gb[out] += sum_rows grad[row][out].  prev is bf16 (x or stored activation), grad FP32.
-// 256 threads, 64 rows per block; each thread owns a 4x4 patch of the 64x64 gradient.
+// weight gradients of all four layers in one launch (blockIdx.y = layer):
+// gw[in][out] = sum_rows prev[row][in] * grad[row][out], gb[out] = sum_rows grad[row][out];
+// prev is bf16 (x or a stored activation), grad FP32.  256 threads per block; each thread
+// owns a 4x4 patch of the 64x64 gradient and keeps it in registers while the block walks its
+// 64-row chunks (grid-stride), so each block adds its partial sums to global memory once.
 constexpr uint32_t kDwRows = 64;
-__global__ void __launch_bounds__(256) k_dw(const uint4* __restrict__ prev, const float* __restrict__ grad, uint32_t m,
-                                            float* __restrict__ gw, float* __restrict__ gb) {
+__global__ void __launch_bounds__(256) k_dw(DwLayers L, uint32_t m) {
     __shared__ float sp[kDwRows][65];
     __shared__ float sg[kDwRows][65];
-    const uint32_t r0 = blockIdx.x * kDwRows;
-    for (uint32_t e = threadIdx.x; e < kDwRows * 8u; e += blockDim.x) {
-        const uint32_t r = e >> 3, c = e & 7u, row = r0 + r;
-        const uint4 v = row < m ? __ldg(&prev[(size_t)row * 8 + c]) : make_uint4(0, 0, 0, 0);
-        const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) { sp[r][8 * c + 2 * q] = bf_lo(vw[q]); sp[r][8 * c + 2 * q + 1] = bf_hi(vw[q]); }
-    }
-    for (uint32_t e = threadIdx.x; e < kDwRows * 64u; e += blockDim.x) {
-        const uint32_t r = e >> 6, c = e & 63u, row = r0 + r;
-        sg[r][c] = row < m ? grad[(size_t)row * 64 + c] : 0.0f;
-    }
-    __syncthreads();
+    const uint32_t l = blockIdx.y;
+    const uint4* __restrict__ prev = L.prev[l];
+    const float* __restrict__ grad = L.grad[l];
     const uint32_t ti = (threadIdx.x >> 4) * 4u, to = (threadIdx.x & 15u) * 4u;
     float acc[4][4] = {};
-    for (uint32_t r = 0; r < kDwRows; ++r) {
-        float a[4], b[4];
+    float sb = 0.0f;
+    for (uint32_t r0 = blockIdx.x * kDwRows; r0 < m; r0 += gridDim.x * kDwRows) {
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < kDwRows * 8u; e += blockDim.x) {
+            const uint32_t r = e >> 3, c = e & 7u, row = r0 + r;
+            const uint4 v = row < m ? __ldg(&prev[(size_t)row * 8 + c]) : make_uint4(0, 0, 0, 0);
+            const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q) { a[q] = sp[r][ti + q]; b[q] = sg[r][to + q]; }
+            for (int q = 0; q < 4; ++q) { sp[r][8 * c + 2 * q] = bf_lo(vw[q]); sp[r][8 * c + 2 * q + 1] = bf_hi(vw[q]); }
+        }
+        for (uint32_t e = threadIdx.x; e < kDwRows * 16u; e += blockDim.x) {
+            const uint32_t r = e >> 4, c = (e & 15u) * 4u, row = r0 + r;
+            const float4 v = row < m ? __ldg(reinterpret_cast<const float4*>(grad + (size_t)row * 64 + c))
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+            sg[r][c] = v.x; sg[r][c + 1] = v.y; sg[r][c + 2] = v.z; sg[r][c + 3] = v.w;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (uint32_t r = 0; r < kDwRows; ++r) {
+            float a[4], b[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+            for (int q = 0; q < 4; ++q) { a[q] = sp[r][ti + q]; b[q] = sg[r][to + q]; }
 #pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(a[u], b[v], acc[u][v]);
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(a[u], b[v], acc[u][v]);
+        }
+        if (threadIdx.x < 64u)
+            for (uint32_t r = 0; r < kDwRows; ++r) sb += sg[r][threadIdx.x];
     }
+    float* gw = L.gw[l];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) atomicAdd(&gw[(ti + u) * 64u + to + v], acc[u][v]);
-    if (threadIdx.x < 64u) {
-        float sb = 0.0f;
-        for (uint32_t r = 0; r < kDwRows; ++r) sb += sg[r][threadIdx.x];
-        atomicAdd(&gb[threadIdx.x], sb);
-    }
+    if (threadIdx.x < 64u) atomicAdd(&L.gb[l][threadIdx.x], sb);
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master parameters
@@ -348,9 +357,16 @@ cudaError_t mix_grad(const float* out, const float* dirs, const float* w, uint32
     k_mix_grad<<<(m + 127) / 128, 128, 0, s>>>(out, dirs, w, m, wsum, dy_bf, dy_f, loss);
     return cudaGetLastError();
 }
-cudaError_t weight_grad(const uint4* prev, const float* grad, uint32_t m, float* gw, float* gb, cudaStream_t s) {
+cudaError_t weight_grad(const DwLayers& L, uint32_t m, cudaStream_t s) {
     if (m == 0) return cudaSuccess;
-    k_dw<<<(m + kDwRows - 1) / kDwRows, 256, 0, s>>>(prev, grad, m, gw, gb);
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // four blocks per SM over the four layers
+    uint32_t gx = (uint32_t)sms;
+    const uint32_t chunks = (m + kDwRows - 1) / kDwRows;
+    if (gx > chunks) gx = chunks;
+    k_dw<<<dim3(gx, 4), 256, 0, s>>>(L, m);
     return cudaGetLastError();
 }
 cudaError_t adam(float* params, const float* grads, float* m1, float* m2, uint32_t n, float lr, uint32_t step,

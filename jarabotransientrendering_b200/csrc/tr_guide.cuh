@@ -14,7 +14,9 @@ constexpr int kOut = 5 * kLobes; // per lobe: weight logit, mean xyz (unnormalis
 constexpr int kLayers = 4;
 constexpr int kParams = kLayers * 64 * 64 + kLayers * 64;   // weights [l][in][out] then biases [l][out]
 constexpr int kTile = 128;       // rows per tcgen05 tile (MMA M)
-constexpr float kKappaMin = 0.05f, kKappaMax = 2000.0f;
+// concentration kappa = kKappaMin + kKappaMax * sigmoid(raw - kKappaShift): about exp(raw - 0.4)
+// for small kappa (scale-free Adam steps), smoothly saturating at kKappaMax
+constexpr float kKappaMin = 0.05f, kKappaMax = 2000.0f, kKappaShift = 8.0f;
 
 // Features of a surface vertex (46 used of 64, rest zero):
 //   [0,36)  sin/cos(2^k pi p_d), k = 0..5, d = x,y,z      (p normalised to the scene box)
@@ -40,7 +42,14 @@ int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem);
 cudaError_t pack_weights(const float* params, uint8_t* w_fwd, uint8_t* w_bwd, cudaStream_t s);
 cudaError_t mix_grad(const float* out, const float* dirs, const float* w, uint32_t m, float* wsum, uint4* dy_bf,
                      float* dy_f, float* loss, cudaStream_t s);
-cudaError_t weight_grad(const uint4* prev, const float* grad, uint32_t m, float* gw, float* gb, cudaStream_t s);
+// weight-gradient operands of the four layers: gw[l] += prev[l]^T grad[l], gb[l] += column sums
+struct DwLayers {
+    const uint4* prev[4];   // [m][64] bf16 layer inputs (features, H1, H2, H3)
+    const float* grad[4];   // [m][64] FP32 gradients w.r.t. the layer outputs
+    float* gw[4];
+    float* gb[4];
+};
+cudaError_t weight_grad(const DwLayers& L, uint32_t m, cudaStream_t s);
 cudaError_t adam(float* params, const float* grads, float* m1, float* m2, uint32_t n, float lr, uint32_t step,
                  cudaStream_t s);
 

@@ -11,23 +11,13 @@
 //            warp-aggregated atomics -> FP64 film in HBM)
 // Reference path: src/Integrator/BidirectionalPathTracing.h:485-692,975-1140 and
 // src/Film/StreakCameraFilm.h:139-192 (details at each kernel).
-#include <cuda_bf16.h>
-
+#include "tr_bsdf.cuh"
 #include "tr_device.cuh"
-#include "tr_guide_math.cuh"
-#include "tr_tcgen05.cuh"
 #include "tr_kernels.cuh"
 
 namespace trk {
 using namespace trd;
 
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
 
 // -----------------------------------------------------------------------------------------
 // BVH traversal: two-child 64-byte nodes, near-first, conservative slab test (Ize 2013),
@@ -235,119 +225,6 @@ __device__ __forceinline__ float hg_eval(float g, float cs) {
     return ((1.0f - gg) * kInv4Pi) / (b * sqrtf(b));
 }
 
-// GGX microfacet reflection (no reference counterpart): D, height-correlated Smith G2 and
-// Schlick F of Walter et al. 2007; visible-normal sampling of Heitz 2018 (JCGT 7(4)); local
-// frame around the geometric normal by Duff et al. 2017.  Reflection only; the back side absorbs.
-struct Frame3 { f3 t1, t2, n; };
-__device__ __forceinline__ Frame3 make_frame(f3 n) {
-    const float sg = copysignf(1.0f, n.z);
-    const float a = -1.0f / (sg + n.z);
-    const float b = n.x * n.y * a;
-    return Frame3{mk(1.0f + sg * n.x * n.x * a, sg * b, -sg * n.x), mk(b, sg + n.y * n.y * a, -n.y), n};
-}
-__device__ __forceinline__ f3 to_local(const Frame3& F, f3 w) { return mk(dot(w, F.t1), dot(w, F.t2), dot(w, F.n)); }
-__device__ __forceinline__ f3 to_world(const Frame3& F, f3 l) { return ((F.t1 * l.x) + (F.t2 * l.y)) + (F.n * l.z); }
-__device__ __forceinline__ float ggx_D(float a2, float hz) {
-    const float c = hz * hz;
-    const float d = c * (a2 - 1.0f) + 1.0f;
-    return a2 / ((3.14159274f * d) * d);
-}
-__device__ __forceinline__ float ggx_lambda(float a2, f3 w) {
-    const float t2 = (w.x * w.x + w.y * w.y) / (w.z * w.z);
-    return (-1.0f + sqrtf(1.0f + a2 * t2)) * 0.5f;
-}
-__device__ __forceinline__ float schlick(float f0, float c) {
-    const float m = 1.0f - c;
-    const float m2 = m * m;
-    return f0 + (1.0f - f0) * ((m2 * m2) * m);
-}
-// f(wo, wi) * max(0, n.wi)
-__device__ __forceinline__ f3 ggx_eval_cos(f3 kd, float alpha, f3 n, f3 wo_w, f3 wi_w) {
-    const Frame3 F = make_frame(n);
-    const f3 wo = to_local(F, wo_w), wi = to_local(F, wi_w);
-    if (!(wo.z > 0.0f) || !(wi.z > 0.0f)) return mk(0.0f, 0.0f, 0.0f);
-    const f3 h = normalize(wo + wi);
-    const float a2 = alpha * alpha;
-    const float D = ggx_D(a2, h.z);
-    const float G2 = 1.0f / ((1.0f + ggx_lambda(a2, wo)) + ggx_lambda(a2, wi));
-    float c = dot(wo, h);
-    if (c < 0.0f) c = 0.0f;
-    const float common = (D * G2) / (4.0f * wo.z);
-    return mk(schlick(kd.x, c) * common, schlick(kd.y, c) * common, schlick(kd.z, c) * common);
-}
-__device__ __forceinline__ bool ggx_sample(f3 kd, float alpha, f3 n, f3 wo_w, float sp, float cp, float x2,
-                                           f3& wi_w, f3& fa, float& pa) {
-    const Frame3 F = make_frame(n);
-    const f3 wo = to_local(F, wo_w);
-    if (!(wo.z > 0.0f)) return false;
-    const f3 Vh = normalize(mk(alpha * wo.x, alpha * wo.y, wo.z));
-    const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
-    const f3 T1 = lensq > 0.0f ? divs(mk(-Vh.y, Vh.x, 0.0f), sqrtf(lensq)) : mk(1.0f, 0.0f, 0.0f);
-    const f3 T2 = cross(Vh, T1);
-    const float r = sqrtf(x2);
-    const float t1 = r * cp;
-    float t2 = r * sp;
-    const float s = 0.5f * (1.0f + Vh.z);
-    t2 = (1.0f - s) * sqrtf(1.0f - t1 * t1) + s * t2;
-    const float tz2 = (1.0f - t1 * t1) - t2 * t2;
-    const float tz = sqrtf(tz2 > 0.0f ? tz2 : 0.0f);
-    const f3 Nh = ((T1 * t1) + (T2 * t2)) + (Vh * tz);
-    const f3 h = normalize(mk(alpha * Nh.x, alpha * Nh.y, Nh.z > 0.0f ? Nh.z : 0.0f));
-    float c = dot(wo, h);
-    const f3 wi = (h * (2.0f * c)) - wo;
-    if (!(wi.z > 0.0f)) return false;
-    const float a2 = alpha * alpha;
-    const float Lo = ggx_lambda(a2, wo), Li = ggx_lambda(a2, wi);
-    const float G1 = 1.0f / (1.0f + Lo);
-    const float G2 = 1.0f / ((1.0f + Lo) + Li);
-    const float pdf = (G1 * ggx_D(a2, h.z)) / (4.0f * wo.z);
-    const float w = G2 / G1;
-    if (c < 0.0f) c = 0.0f;
-    fa = mk((schlick(kd.x, c) * w) * pdf, (schlick(kd.y, c) * w) * pdf, (schlick(kd.z, c) * w) * pdf);
-    pa = pdf;
-    wi_w = normalize(to_world(F, wi));
-    return true;
-}
-
-__device__ __forceinline__ bool finite3(float a, float b, float c) {
-    return isfinite(a) && isfinite(b) && isfinite(c);
-}
-
-// Features of a surface vertex for the learned proposal (64 BF16 values, 46 used):
-// sin/cos(2^k pi p_d) for k = 0..5 (index 6k + 2d + {0,1}), p normalised to the scene box,
-// geometric normal, outgoing direction, path length / film time length.
-__device__ __forceinline__ void write_features(uint4* row, const SceneDev& sc, f3 pos, f3 nrm, f3 wo, float tn) {
-    float v[64];
-    const float pn[3] = {(pos.x - sc.bmin[0]) * sc.binv[0], (pos.y - sc.bmin[1]) * sc.binv[1],
-                         (pos.z - sc.bmin[2]) * sc.binv[2]};
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        const float f = (float)(1 << k);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            float sv, cv;
-            sincospif(f * pn[d], &sv, &cv);
-            v[6 * k + 2 * d] = sv;
-            v[6 * k + 2 * d + 1] = cv;
-        }
-    }
-    v[36] = pn[0]; v[37] = pn[1]; v[38] = pn[2];
-    v[39] = nrm.x; v[40] = nrm.y; v[41] = nrm.z;
-    v[42] = wo.x; v[43] = wo.y; v[44] = wo.z;
-    v[45] = tn;
-#pragma unroll
-    for (int k = 46; k < 64; ++k) v[k] = 0.0f;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        __nv_bfloat162 a = __floats2bfloat162_rn(v[8 * c], v[8 * c + 1]);
-        __nv_bfloat162 b = __floats2bfloat162_rn(v[8 * c + 2], v[8 * c + 3]);
-        __nv_bfloat162 e = __floats2bfloat162_rn(v[8 * c + 4], v[8 * c + 5]);
-        __nv_bfloat162 h = __floats2bfloat162_rn(v[8 * c + 6], v[8 * c + 7]);
-        row[c] = make_uint4(*reinterpret_cast<uint32_t*>(&a), *reinterpret_cast<uint32_t*>(&b),
-                            *reinterpret_cast<uint32_t*>(&e), *reinterpret_cast<uint32_t*>(&h));
-    }
-}
-
 template <bool kGuided>
 __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
     const SceneDev& sc = p.scene;
@@ -369,6 +246,7 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
     for (uint32_t base = warp_global * 32u; base < n; base += nwarps * 32u) {
         const uint32_t idx = base + lane;
         bool want_shadow = false, want_next = false, want_guide = false;
+        uint4 gv[5];                     // guided-vertex record (kGuided only)
         uint32_t slot = 0;
         float4 sh_o = make_float4(0, 0, 0, 0), sh_d = make_float4(0, 0, 0, 0), sh_L = make_float4(0, 0, 0, 0);
         if (idx < n) {
@@ -488,11 +366,15 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
                         const float albedo = surface ? avg3(kd)
                             : avg3(mk(sig_s.x / sig_t.x, sig_s.y / sig_t.y, sig_s.z / sig_t.z));
                         if (kGuided && surface && !(pcg_float(rng) > albedo)) {
-                            // ---- direction deferred to the learned proposal (k_guide_sample) ----
-                            p.wave.ray_o[slot] = make_float4(pos.x, pos.y, pos.z, 0.0f);
-                            p.wave.ray_d[slot] = make_float4(dir.x, dir.y, dir.z, time);
-                            p.wave.thr[slot] = make_float4(f.x, f.y, f.z, albedo);
+                            // ---- direction deferred to the learned proposal (k_guide) ----
                             want_guide = true;
+                            gv[0] = make_uint4(__float_as_uint(pos.x), __float_as_uint(pos.y), __float_as_uint(pos.z),
+                                               __float_as_uint(time));
+                            gv[1] = make_uint4(__float_as_uint(dir.x), __float_as_uint(dir.y), __float_as_uint(dir.z),
+                                               __float_as_uint(albedo));
+                            gv[2] = make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z),
+                                               __float_as_uint(__ldg(&sc.tri_ng[id]).w));
+                            gv[3] = make_uint4(__float_as_uint(nrm.x), __float_as_uint(nrm.y), __float_as_uint(nrm.z), slot);
                         } else if ((!kGuided || !surface) && !(pcg_float(rng) > albedo)) {
                             // ---- outgoing direction ----
                             const float x1 = pcg_float(rng), x2 = pcg_float(rng);
@@ -558,7 +440,11 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
                         }
                     }
                 }
-                p.wave.rng[slot] = rng.state;
+                if (kGuided && want_guide)
+                    gv[4] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
+                                       (uint32_t)(rng.inc >> 32));
+                else
+                    p.wave.rng[slot] = rng.state;
             }
         }
         // ---- warp-aggregated queue appends (order preserved within the warp) ----
@@ -584,227 +470,13 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
             uint32_t bg = 0;
             if (lane == 0 && mg) bg = atomicAdd(&p.wave.counters[cnt_guide(depth)], (uint32_t)__popc(mg));
             bg = __shfl_sync(kFull, bg, 0);
-            if (want_guide) p.guide.gq[bg + (uint32_t)__popc(mg & lt)] = slot;
+            if (want_guide) {
+                uint4* r = p.guide.vrec + (size_t)(bg + (uint32_t)__popc(mg & lt)) * 5;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) r[q] = gv[q];
+            }
         }
     }
-}
-
-// -----------------------------------------------------------------------------------------
-// guided direction sampling (no reference counterpart): one-sample multiple importance
-// sampling (Veach & Guibas 1995, balance heuristic) between the learned vMF mixture (chosen
-// with probability mix_prob) and the BSDF sampler, so the estimator stays unbiased whatever
-// the network predicts.  Directions below the surface carry no reflectance and end the path.
-// -----------------------------------------------------------------------------------------
-__device__ __forceinline__ float ggx_pdf(float alpha, f3 n, f3 wo_w, f3 wi_w) {
-    const Frame3 F = make_frame(n);
-    const f3 wo = to_local(F, wo_w), wi = to_local(F, wi_w);
-    if (!(wo.z > 0.0f) || !(wi.z > 0.0f)) return 0.0f;
-    const f3 h = normalize(wo + wi);
-    const float a2 = alpha * alpha;
-    const float G1 = 1.0f / (1.0f + ggx_lambda(a2, wo));
-    return (G1 * ggx_D(a2, h.z)) / (4.0f * wo.z);
-}
-
-// Fused proposal inference and sampling: one CTA of 128 threads owns 128 guided vertices at a
-// time.  Each thread gathers its vertex, writes its 64 BF16 features as row `tid` of the A tile
-// in shared memory, the four layers run on the tensor cores (trg::layer_mma, accumulators in
-// tensor memory), and the epilogue decodes the thread's mixture from the last layer's
-// accumulator row in registers and samples the direction.  Neither features nor mixtures touch
-// HBM.  Four CTAs per SM (50 KB shared memory, 64 TMEM columns each) overlap one CTA's MMA waits
-// with the others' gathers.
-__global__ void __launch_bounds__(128, 4) k_guide(Params p, int depth, uint32_t* pool_count) {
-    const GuideWave& G = p.guide;
-    const uint32_t n = p.wave.counters[cnt_guide(depth)];
-    if (blockIdx.x * (uint32_t)trg::kTile >= n) return;     // no tile for this CTA
-    extern __shared__ __align__(1024) uint8_t smem[];
-    const SceneDev& sc = p.scene;
-    uint8_t* sA = smem + trg::kSmemA;
-    const float* sB = reinterpret_cast<const float*>(smem + trg::kSmemBias);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + trg::kSmemBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + trg::kSmemSlot);
-    volatile int* s_ok = reinterpret_cast<volatile int*>(smem + trg::kSmemOk);
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    trg::stage_weights(smem, G.net.w_fwd, G.net.bias);
-    if (tid == 0) { trg::mbar_init(bar, 1); trg::fence_mbar_init(); }
-    if (warp == 0) { trg::tmem_alloc(tslot, 64); trg::tmem_relinquish(); }
-    trg::tc_fence_before();
-    __syncthreads();
-    trg::tc_fence_after();
-    const uint32_t taddr = *tslot;
-    const uint32_t lane_addr = taddr + ((32u * warp) << 16);
-    uint32_t phase = 0;
-    bool ok = true;
-
-    uint32_t* qout = p.wave.q[(depth + 1) & 1];
-    const bool medium = sc.medium != 0;
-    const uint32_t per_pix = p.batch.ns * p.batch.ninc;
-    const float total_time = (float)p.film.T * p.film.exposure + p.film.offset;
-    const float c = G.mix_prob;
-    const unsigned lane = tid & 31u;
-    for (uint32_t tile = blockIdx.x; tile * (uint32_t)trg::kTile < n && ok; tile += gridDim.x) {
-        const uint32_t idx = tile * (uint32_t)trg::kTile + tid;
-        const bool active = idx < n;
-        uint32_t slot = 0, mi = 0;
-        float4 ro = make_float4(0.f, 0.f, 0.f, 0.f), rd = ro, th = ro;
-        f3 nrm = mk(0.f, 0.f, 1.f);
-        {
-            uint4 feat[8];
-            if (active) {
-                slot = G.gq[idx];
-                ro = p.wave.ray_o[slot];
-                rd = p.wave.ray_d[slot];
-                th = p.wave.thr[slot];
-                const float4 ng = __ldg(&sc.tri_ng[__float_as_uint(p.wave.hit[slot].y)]);
-                nrm = mk(ng.x, ng.y, ng.z);
-                mi = __float_as_uint(ng.w);
-                write_features(feat, sc, mk(ro.x, ro.y, ro.z), nrm, mk(-rd.x, -rd.y, -rd.z), rd.w / total_time);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) feat[q] = make_uint4(0u, 0u, 0u, 0u);
-            }
-            trg::store_row_a(sA, tid, feat);
-        }
-        float o[48];
-        for (uint32_t l = 0; l < 4; ++l) {
-            ok = trg::layer_mma(taddr, trg::smem_u32(sA), trg::smem_u32(smem + trg::kSmemW + l * 8192u), bar, phase, s_ok);
-            if (!ok) break;
-            if (l < 3) {
-                float a[64];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) trg::tmem_ld16(lane_addr + 16u * j, a + 16 * j);
-                trg::tmem_wait_ld();
-                uint4 h[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    float t[8];
-#pragma unroll
-                    for (int e = 0; e < 8; ++e) t[e] = fmaxf(a[8 * q + e] + sB[l * 64 + 8 * q + e], 0.0f);
-                    h[q] = make_uint4(trg::pack2(t[0], t[1]), trg::pack2(t[2], t[3]), trg::pack2(t[4], t[5]),
-                                      trg::pack2(t[6], t[7]));
-                }
-                trg::store_row_a(sA, tid, h);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 3; ++j) trg::tmem_ld16(lane_addr + 16u * j, o + 16 * j);
-                trg::tmem_wait_ld();
-#pragma unroll
-                for (int j = 0; j < trg::kOut; ++j) o[j] += sB[3 * 64 + j];
-            }
-        }
-        if (!ok) break;
-
-        // ---- one-sample MIS between the mixture and the BSDF ----
-        bool want_next = false;
-        if (active) {
-            const float4 m = __ldg(&sc.mats[mi]);
-            const f3 kd = mk(m.x, m.y, m.z);
-            const bool ggx = __float_as_uint(m.w) == 1u;
-            const float alpha = ggx ? __ldg(&sc.mats2[mi]).x : 0.0f;
-            const f3 pos = mk(ro.x, ro.y, ro.z);
-            const f3 wo = mk(-rd.x, -rd.y, -rd.z);
-            const f3 f = mk(th.x, th.y, th.z);
-            const uint32_t pl = slot / per_pix;
-            const uint32_t sl = (slot - pl * per_pix) / p.batch.ninc;
-            const uint32_t wpix = p.batch.pix_begin + pl;
-            const uint32_t pixel = (p.batch.win_y0 + wpix / p.batch.win_w) * p.film.W +
-                                   (p.batch.win_x0 + wpix % p.batch.win_w);
-            Pcg rng;
-            rng.state = p.wave.rng[slot];
-            rng.inc = (cam_id(pixel, p.batch.s0 + sl) << 1u) | 1ull;
-            trg::Lobe L[trg::kLobes];
-            trg::decode_mixture(o, L);
-            f3 wi = mk(0.f, 0.f, 1.f);
-            bool alive = true;
-            if (pcg_float(rng) < c) {
-                const float u0 = pcg_float(rng), u1 = pcg_float(rng), u2 = pcg_float(rng);
-                float d[3];
-                trg::mixture_sample(L, u0, u1, u2, d);
-                wi = normalize(mk(d[0], d[1], d[2]));
-            } else {
-                const float x1 = pcg_float(rng), x2 = pcg_float(rng);
-                float sp, cp;
-                tr_sincos2pi(x1, &sp, &cp);
-                if (ggx) {
-                    f3 fa;
-                    float pa;
-                    alive = ggx_sample(kd, alpha, nrm, wo, sp, cp, x2, wi, fa, pa);
-                } else {
-                    const float ct = sqrtf(x2);
-                    const float stt = sqrtf(1.0f - ct * ct);
-                    wi = to_world(make_frame(nrm), mk(cp * stt, sp * stt, ct));
-                }
-            }
-            if (alive) {
-                f3 fcos;
-                float pb;
-                if (ggx) {
-                    fcos = ggx_eval_cos(kd, alpha, nrm, wo, wi);
-                    pb = ggx_pdf(alpha, nrm, wo, wi);
-                } else {
-                    const float cs = dot(nrm, wi);
-                    const float cl = cs > 0.0f ? cs : 0.0f;
-                    fcos = mk((kd.x * kInvPi) * cl, (kd.y * kInvPi) * cl, (kd.z * kInvPi) * cl);
-                    pb = cl * kInvPi;
-                }
-                const float pdf = c * trg::mixture_pdf(L, wi.x, wi.y, wi.z) + (1.0f - c) * pb;
-                if (pdf > 0.0f && (fcos.x > 0.0f || fcos.y > 0.0f || fcos.z > 0.0f) && isfinite(pdf)) {
-                    const f3 fn = mulv(f, fcos);
-                    const bool keep = G.pool_cap > 0 && pcg_float(rng) < G.keep_prob;
-                    float nds = __int_as_float(0x7f800000);
-                    if (medium) nds = -tr_log(pcg_float(rng)) / sc.lambda;
-                    p.wave.ray_o[slot] = make_float4(pos.x, pos.y, pos.z, nds);
-                    p.wave.ray_d[slot] = make_float4(wi.x, wi.y, wi.z, rd.w);
-                    p.wave.thr[slot] = make_float4(fn.x, fn.y, fn.z, th.w * pdf);
-                    want_next = true;
-                    if (keep) {
-                        const uint32_t k = atomicAdd(pool_count, 1u);
-                        if (k < G.pool_cap) {
-                            write_features(G.pool_feat + (size_t)k * 8, sc, pos, nrm, wo, rd.w / total_time);
-                            G.pool_dir[3 * (size_t)k] = wi.x;
-                            G.pool_dir[3 * (size_t)k + 1] = wi.y;
-                            G.pool_dir[3 * (size_t)k + 2] = wi.z;
-                            G.pool_meta[k] = make_uint4(slot, (uint32_t)depth, __float_as_uint(avg3(f)), 0u);
-                        }
-                    }
-                }
-            }
-            p.wave.rng[slot] = rng.state;
-        }
-        const unsigned mn = __ballot_sync(kFull, want_next);
-        uint32_t bn = 0;
-        if (lane == 0 && mn) bn = atomicAdd(&p.wave.counters[cnt_ext(depth + 1)], (uint32_t)__popc(mn));
-        bn = __shfl_sync(kFull, bn, 0);
-        if (want_next) qout[bn + (uint32_t)__popc(mn & lanemask_lt())] = slot;
-    }
-    if (!ok && tid == 0) atomicExch(G.err, 1);
-    trg::drain_and_free(taddr, bar, phase, ok);
-}
-
-// Training targets of this batch's pool entries: the luminance reaching the film through the
-// rest of the path (splat records of later bounces) relative to the throughput at the vertex,
-// i.e. an estimate of (incident radiance x f cos / sampling pdf) along the sampled direction.
-// pool_state[0] = entries filled, pool_state[1] = entries already given a target.
-__global__ void k_train_gather(Params p, const uint32_t* pool_state) {
-    const GuideWave& G = p.guide;
-    const uint32_t end = min(pool_state[0], G.pool_cap);
-    const uint32_t begin = pool_state[1];
-    const size_t rs = p.wave.capacity;
-    for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
-        const uint4 meta = G.pool_meta[i];
-        const uint32_t slot = meta.x, d = meta.y;
-        const float lumf = __uint_as_float(meta.z);
-        const uint32_t cnt = p.wave.rec_n[slot];
-        float sum = 0.0f;
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const float4 r = p.wave.rec[(size_t)k * rs + slot];
-            if ((__float_as_uint(r.w) >> 24) > d) sum += ((r.x + r.y) + r.z) / 3.0f;
-        }
-        G.pool_w[i] = lumf > 0.0f && isfinite(sum / lumf) ? sum / lumf : 0.0f;
-    }
-}
-
-__global__ void k_train_mark(uint32_t* pool_state, uint32_t cap) {
-    pool_state[1] = min(pool_state[0], cap);
 }
 
 // -----------------------------------------------------------------------------------------
@@ -947,26 +619,6 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_user(Sce
 // -----------------------------------------------------------------------------------------
 size_t trace_smem_bytes(uint32_t bvh_depth) { return (size_t)(bvh_depth + 1u) * kTraceBlock * sizeof(int); }
 
-cudaError_t launch_guide(const Params& p, int depth, uint32_t* pool_state, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_guide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trg::kSmemBytes);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const int grid = trg::resident_grid(dev, reinterpret_cast<const void*>(k_guide), 128, trg::kSmemBytes);
-    k_guide<<<grid, 128, trg::kSmemBytes, s>>>(p, depth, pool_state);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_train_gather(const Params& p, uint32_t* pool_state, cudaStream_t s) {
-    k_train_gather<<<256, 256, 0, s>>>(p, pool_state);
-    k_train_mark<<<1, 1, 0, s>>>(pool_state, p.guide.pool_cap);
-    return cudaGetLastError();
-}
-
 int trace_grid_size(int device, uint32_t bvh_depth) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -997,7 +649,7 @@ cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s) {
     const uint32_t need = (p.batch.n_slots + 255) / 256;
     if ((uint32_t)grid > need) grid = (int)need;
     if (grid < 1) grid = 1;
-    if (p.guide.gq) k_shade<true><<<grid, 256, 0, s>>>(p, depth);
+    if (p.guide.vrec) k_shade<true><<<grid, 256, 0, s>>>(p, depth);
     else k_shade<false><<<grid, 256, 0, s>>>(p, depth);
     return cudaGetLastError();
 }

@@ -35,7 +35,10 @@ constexpr uint32_t kFlagOrthoFrame = 1u;   // TR_FLAG_ORTHONORMAL_FRAME
 
 // Guided mode state (all null when rendering without the learned proposal).
 struct GuideWave {
-    uint32_t* gq;             // [capacity] slots whose direction waits for the proposal
+    // [capacity][5] guided-vertex records, one per vertex whose direction waits for the
+    // proposal, in queue order: (pos, time) (incoming dir, RR albedo) (throughput, material)
+    // (geometric normal, slot) (RNG state, RNG increment)
+    uint4* vrec;
     trg::GuideDev net;        // network weights (canonical tiles) and biases
     int* err;                 // set to 1 when a tensor-core wait times out
     float mix_prob;           // probability of sampling the proposal (else the BSDF)

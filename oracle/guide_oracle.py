@@ -6,7 +6,8 @@ accumulated in FP32 (here: float64, then compared with a tolerance), the output-
 feeds the hidden-layer backward as BF16 and the weight gradients as FP32.
 
 Mixture of 8 von Mises-Fisher lobes (per lobe: weight logit, unnormalised mean, concentration
-kappa = min(softplus(k) + 0.05, 2000)); density vMF(w; mu, kappa) =
+kappa = 0.05 + 2000 sigmoid(k - 8), log-like below a few hundred and smoothly saturating at
+2000); density vMF(w; mu, kappa) =
 kappa / (2 pi (1 - exp(-2 kappa))) * exp(kappa (mu.w - 1)); sampling follows Jakob 2012
 ("Numerically stable sampling of the von Mises Fisher distribution on S^2").
 """
@@ -16,6 +17,7 @@ import numpy as np
 
 NP = 16640
 KMIN, KMAX = 0.05, 2000.0
+KSHIFT = 8.0
 LOBES = 8
 
 
@@ -52,8 +54,8 @@ def forward(params, x):
     return out.astype(np.float32), acts
 
 
-def softplus(x):
-    return np.where(x > 20, x, np.log1p(np.exp(np.minimum(x, 20))))
+def sigmoid(x):
+    return 0.5 * (1.0 + np.tanh(0.5 * x))
 
 
 def decode(out):
@@ -65,10 +67,10 @@ def decode(out):
     n = np.linalg.norm(m, axis=2, keepdims=True)
     mu = np.where(n > 1e-6, m / np.maximum(n, 1e-30), np.array([0.0, 0.0, 1.0]))
     n = np.maximum(n, 1e-6)
-    sp = softplus(o[..., 4]) + KMIN
-    kappa = np.minimum(sp, KMAX)
-    sig = np.where(sp < KMAX, 1.0 / (1.0 + np.exp(-o[..., 4])), 0.0)
-    return pi, mu, n[..., 0], kappa, sig
+    s = sigmoid(o[..., 4] - KSHIFT)
+    kappa = KMIN + KMAX * s
+    dkappa = KMAX * s * (1.0 - s)                 # d kappa / d raw
+    return pi, mu, n[..., 0], kappa, dkappa
 
 
 def log_vmf(kappa, c):
