@@ -6,11 +6,15 @@ resolution but with a short film (`--bins` time bins), so that the device footpr
 while the traversal kernels see the real BVH and the real first-bounce ray distribution.
 
     python -m jarabotransientrendering_b200.profile_case --workload icosphere --spp 8 --bins 64
+
+`--guided` attaches a learned proposal (orthonormal shading frames, mixture probability
+`--mix`); with `--train-pool 0` the network stays at its seeded initialisation, otherwise it is
+trained after every pass.
 """
 import argparse
 
 from . import scenes as S
-from .renderer import Context
+from .renderer import Context, Guide
 
 
 def main():
@@ -19,15 +23,27 @@ def main():
     ap.add_argument("--spp", type=int, default=8)
     ap.add_argument("--bins", type=int, default=64)
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--guided", action="store_true")
+    ap.add_argument("--mix", type=float, default=0.7)
+    ap.add_argument("--train-pool", type=int, default=0)
     a = ap.parse_args()
     sc = S.WORKLOADS[a.workload]()
     sc.exposure = sc.exposure * sc.time_bins / a.bins
     sc.time_bins = a.bins
+    guide = None
+    if a.guided:
+        sc.flags |= S.FLAG_ORTHONORMAL_FRAME
+        guide = Guide(seed=1)
     with Context(sc) as ctx:
+        if guide is not None:
+            ctx.set_guide(guide, mix_prob=a.mix, learning_rate=3e-3, train_pool=a.train_pool)
         for r in range(a.repeat):
             ctx.render(r * a.spp, a.spp)
         st = ctx.stats()
-    print({k: st[k] for k in ("paths", "closest_rays", "shadow_rays", "splats", "render_ms", "bvh_nodes", "bvh_depth")})
+    print({k: st[k] for k in ("paths", "closest_rays", "shadow_rays", "splats", "render_ms", "bvh_nodes", "bvh_depth",
+                              "train_steps")})
+    if guide is not None:
+        guide.close()
 
 
 if __name__ == "__main__":
