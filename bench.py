@@ -48,6 +48,8 @@ def parse():
                     help="skip the time-to-5%%-rel-L2 comparison of guided and plain sampling")
     ap.add_argument("--convergence-ref-spp", type=int, default=131072,
                     help="samples per pixel of each of the two halves of the converged reference")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the 16-scene batched (CUDA-graph) throughput and accuracy leg")
     return ap.parse_args()
 
 
@@ -213,6 +215,106 @@ def convergence(args, device):
     return res
 
 
+def batched(args, device, frames=2):
+    """16 seeded scenes of uneven size (scenes.batch_scenes) rendered together: every wavefront
+    batch holds path slots of several scenes and is one replay of a captured CUDA graph; the
+    batch's queue capacity, shade block and film tile width come from the autotuner; one learned
+    proposal (scene index among its features) serves all scenes, trained online.  Reports the
+    aggregate paths/s of a frame (every scene at its own spp) by host wall clock, training
+    included, beside the same batch without the proposal and beside rendering the contexts one
+    after another; per scene, the accuracy of the batched guided film against the plain tracer."""
+    import torch
+    from jarabotransientrendering_b200 import convergence as CV, renderer as R, scenes as S
+    scs = S.batch_scenes()
+    n = len(scs)
+    spp = [sc.spp for sc in scs]
+    paths_frame = sum(sc.paths_per_frame() for sc in scs)
+    t0 = time.perf_counter()
+    ctxs = [R.Context(sc, device) for sc in scs]
+    create_s = time.perf_counter() - t0
+    g = R.Guide(device=device, seed=1)
+    res = {"workload": "16 seeded scenes: displaced icospheres (1,314-327,714 triangles) in Cornell rooms, "
+                       "albedo 0.2-0.8, 64^2-512^2, 256-4096 bins, 32-256 spp, 8 with homogeneous media",
+           "scenes": [{"triangles": sc.num_triangles, "res": sc.width, "bins": sc.time_bins,
+                       "spp": sc.spp * sc.incoming_samples, "medium": sc.medium is not None} for sc in scs],
+           "paths_per_frame": paths_frame, "create_s": create_s}
+    try:
+        B = R.Batch(ctxs)
+        B.set_guide(g, mix_prob=0.7, learning_rate=3e-3, train_pool=262144)
+        trial = [max(1, k // 16) for k in spp]
+        best, trials = B.autotune(0, trial)
+        res["autotune"] = {"best": best, "trials": trials, "trial_spp": trial}
+        nxt = [trials * t for t in trial]
+
+        def frame(b):
+            nonlocal nxt
+            torch.cuda.synchronize(device)
+            t = time.perf_counter()
+            b.render(nxt, spp)
+            dt = time.perf_counter() - t
+            nxt = [a + k for a, k in zip(nxt, spp)]
+            return dt
+
+        frame(B)                                  # warm-up frame (also trains the proposal)
+        for c in ctxs:
+            c.clear()
+        begin_timed = list(nxt)
+        wall = [frame(B) for _ in range(frames)]
+        st = B.stats()
+        res["guided"] = {"paths_per_s": paths_frame * frames / sum(wall), "ms_per_frame": 1e3 * sum(wall) / frames,
+                         "device_ms_last_frame": st["render_ms"], "graph_kernel_launches_per_frame": st["kernel_launches"],
+                         "train_steps_last_frame": st["train_steps"]}
+        guided_films = []
+        for c in ctxs:                            # keep the guided films (frames x spp per pixel)
+            guided_films.append(CV.film_device(c).to(torch.float32))
+            c.clear()
+        B.set_guide(None)
+        frame(B)
+        wall = [frame(B) for _ in range(frames)]
+        st = B.stats()
+        res["plain_batched"] = {"paths_per_s": paths_frame * frames / sum(wall), "ms_per_frame": 1e3 * sum(wall) / frames,
+                                "graph_kernel_launches_per_frame": st["kernel_launches"]}
+        B.close()
+        # one context after another (plain), same frame
+        for c in ctxs:
+            c.clear()
+        torch.cuda.synchronize(device)
+        t = time.perf_counter()
+        for c, k, a in zip(ctxs, spp, nxt):
+            c.render(a, k)
+        torch.cuda.synchronize(device)
+        seq = time.perf_counter() - t
+        nxt = [a + k for a, k in zip(nxt, spp)]
+        res["plain_sequential"] = {"paths_per_s": paths_frame / seq, "ms_per_frame": 1e3 * seq}
+        # accuracy per scene against the plain tracer: reference = plain, 4 x frames x spp
+        # per pixel; beside it an independent plain film with as many samples as the guided one
+        acc = []
+        for i, c in enumerate(ctxs):
+            c.clear()
+            c.render(nxt[i], 4 * frames * spp[i])
+            ref = CV.film_device(c).to(torch.float32) / (4 * frames * spp[i])
+            c.clear()
+            c.render(nxt[i] + 4 * frames * spp[i], frames * spp[i])
+            pl = CV.film_device(c).to(torch.float32) / (frames * spp[i])
+            gd = guided_films[i] / (frames * spp[i])
+            nref = float(torch.linalg.vector_norm(ref.double()))
+            acc.append({"energy_ratio_guided_vs_plain": float(gd.double().sum() / ref.double().sum()),
+                        "rel_l2_guided": float(torch.linalg.vector_norm((gd - ref).double())) / nref,
+                        "rel_l2_plain_same_spp": float(torch.linalg.vector_norm((pl - ref).double())) / nref})
+            del ref, pl, gd
+            guided_films[i] = None
+            torch.cuda.empty_cache()
+        res["accuracy_vs_plain"] = acc
+        res["speedup_batched_guided_vs_sequential_plain"] = res["guided"]["paths_per_s"] / res["plain_sequential"]["paths_per_s"]
+        res["timed_sample_begin"] = begin_timed[:1]
+    finally:
+        g.close()
+        for c in ctxs:
+            c.close()
+        torch.cuda.empty_cache()
+    return res
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -357,6 +459,11 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         procs = max(1, min(os.cpu_count() or 1, 32))
         out["cpu_baseline"] = cpu_reference(sc, 1, procs)
+    if rank == 0 and world == 1 and not args.no_batched:
+        try:
+            out["batched"] = batched(args, local)
+        except Exception as e:            # reported, not fatal: the throughput line stands
+            out["batched"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and not args.no_convergence:
         try:
             out["convergence"] = convergence(args, local)

@@ -191,7 +191,9 @@ tr_status tr_clear_film(tr_ctx* ctx);
  * Dividing streak/steady by weight gives what StreakCameraFilm::average_and_save_slice writes. */
 tr_status tr_get_film(tr_ctx* ctx, double* streak, double* steady, double* weight);
 
-/* Same as tr_get_film but into device memory owned by the caller (no host copy). */
+/* Same as tr_get_film but into device memory owned by the caller (no host copy).  Both copy on
+ * the context's stream after its pending renders and return when the copy is complete; the
+ * caller's own pending work on the destination must be finished first.                      */
 tr_status tr_get_film_device(tr_ctx* ctx, double* d_streak, double* d_steady, double* d_weight);
 
 /* Writes the averaged film the way the reference does: one RGBE .hdr streak image per
@@ -265,6 +267,44 @@ tr_status tr_guide_destroy(tr_guide* g);
 tr_status tr_set_guide(tr_ctx* ctx, tr_guide* guide, float mix_prob, float learning_rate, uint32_t train_pool);
 
 tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
+
+/* ---- multi-scene batches (no counterpart in the reference renderer) -------------------------
+ * The scenes of n contexts (each keeps its own BVH, materials, lights, medium, camera,
+ * integrator settings and film) are rendered together: a wavefront batch holds the path slots
+ * of up to 16 scenes, and the launches of one batch (ray generation, the per-depth extend /
+ * shade / [guide] / shadow kernels, splat) are captured once as a CUDA graph that is replayed
+ * for every batch; the kernels read the batch being rendered from device memory.  Each scene's
+ * film receives exactly the samples it would receive from tr_render on its own context (same
+ * per-path random streams).  The contexts must live on one device, outlive the batch, and not
+ * be rendered through their own calls while a batch call runs. */
+typedef struct tr_batch tr_batch;
+
+typedef struct tr_batch_config {
+    uint32_t capacity;       /* path slots per wavefront batch (queue size), 65,536 .. 8,388,608 */
+    uint32_t shade_block;    /* threads per shade block: 128 or 256 */
+    uint32_t splat_div;      /* film tile width = each scene's automatic width / splat_div (1, 2, 4, ...) */
+    uint32_t use_graph;      /* 1: replay the batch launches from a captured CUDA graph; 0: launch directly */
+} tr_batch_config;
+
+tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out);
+tr_status tr_batch_set_config(tr_batch* b, const tr_batch_config* cfg);
+tr_status tr_batch_get_config(tr_batch* b, tr_batch_config* cfg);
+/* Adds camera samples [sample_begin[i], sample_begin[i] + sample_count[i]) of every pixel of
+ * scene i to context i's film (a count of 0 skips the scene).                               */
+tr_status tr_batch_render(tr_batch* b, const uint64_t* sample_begin, const uint32_t* sample_count);
+/* Project autotuner: times candidate configurations (queue capacity, shade block, film tile
+ * width), trial k rendering samples [sample_begin[i] + k*trial_samples[i], +trial_samples[i])
+ * of scene i, keeps the fastest configuration and returns it in best.  The trial renders add
+ * to the films like any render; *trials_run = number of trials.                              */
+tr_status tr_batch_autotune(tr_batch* b, const uint64_t* sample_begin, const uint32_t* trial_samples,
+                            tr_batch_config* best, uint32_t* trials_run);
+/* As tr_set_guide, for all scenes of the batch: one network serves every scene (its features
+ * carry the scene index).  Every context needs TR_FLAG_ORTHONORMAL_FRAME.                     */
+tr_status tr_batch_set_guide(tr_batch* b, tr_guide* guide, float mix_prob, float learning_rate, uint32_t train_pool);
+/* Counters of the batch (paths, rays, splats accumulated; render_ms, kernel_launches,
+ * train_steps of the last tr_batch_render call).                                             */
+tr_status tr_batch_stats(tr_batch* b, tr_stats* out);
+tr_status tr_batch_destroy(tr_batch* b);
 
 /* Runs all later work of the context on the caller's CUDA stream (cudaStream_t as void*;
  * NULL restores the context's own stream).  The stream must belong to the context's device. */

@@ -5,12 +5,12 @@ The compute path is libtransient_b200.so (CUDA, sm_100a) behind the C ABI of
 include/transient_b200.h; this package is its host-side binding.
 """
 from . import scenes
-from .renderer import (Context, Guide, World, Lambertian, GGX, PointLightSource, RectangularAreaLightSource,
+from .renderer import (Context, Batch, Guide, World, Lambertian, GGX, PointLightSource, RectangularAreaLightSource,
                        HenyeyGreenstein, HomogeneousMedium, PinholeCamera, StreakCameraFilm,
                        StratifiedSampler, BidirectionalPathTracing, TransientRenderer, HIT_DTYPE, INVALID_ID)
 from ._abi import TransientError, LIB_PATH
 
-__all__ = ["scenes", "Context", "Guide", "World", "Lambertian", "GGX", "PointLightSource", "RectangularAreaLightSource",
+__all__ = ["scenes", "Context", "Batch", "Guide", "World", "Lambertian", "GGX", "PointLightSource", "RectangularAreaLightSource",
            "HenyeyGreenstein", "HomogeneousMedium", "PinholeCamera", "StreakCameraFilm", "StratifiedSampler",
            "BidirectionalPathTracing", "TransientRenderer", "TransientError", "HIT_DTYPE", "INVALID_ID",
            "LIB_PATH"]

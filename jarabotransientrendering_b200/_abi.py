@@ -65,6 +65,11 @@ class Stats(C.Structure):
                 ("guide_ms", C.c_double), ("train_steps", C.c_uint64), ("train_loss", C.c_float)]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("shade_block", C.c_uint32), ("splat_div", C.c_uint32),
+                ("use_graph", C.c_uint32)]
+
+
 TR_OK = 0
 STATUS = {0: "TR_OK", 1: "TR_ERR_INVALID_ARGUMENT", 2: "TR_ERR_CUDA", 3: "TR_ERR_OUT_OF_MEMORY",
           4: "TR_ERR_NOT_SUPPORTED", 5: "TR_ERR_TIMEOUT", 6: "TR_ERR_NO_DEVICE", 7: "TR_ERR_IO"}
@@ -94,6 +99,15 @@ PROTOTYPES = {
     "tr_guide_destroy": (C.c_int, [C.c_void_p]),
     "tr_set_guide": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_uint32]),
     "tr_stats_get": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    "tr_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)]),
+    "tr_batch_set_config": (C.c_int, [C.c_void_p, C.POINTER(BatchConfig)]),
+    "tr_batch_get_config": (C.c_int, [C.c_void_p, C.POINTER(BatchConfig)]),
+    "tr_batch_render": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "tr_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                    C.POINTER(BatchConfig), C.POINTER(C.c_uint32)]),
+    "tr_batch_set_guide": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_uint32]),
+    "tr_batch_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    "tr_batch_destroy": (C.c_int, [C.c_void_p]),
     "tr_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "tr_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "tr_destroy": (C.c_int, [C.c_void_p]),

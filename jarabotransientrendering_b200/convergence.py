@@ -33,6 +33,8 @@ def film_device(ctx: R.Context, out=None):
     if out is None:
         out = torch.empty((sc.height, sc.width, sc.time_bins, 3), dtype=torch.float64,
                           device=f"cuda:{ctx.device}")
+    # the library writes `out` on its own stream: torch's pending work on that memory first
+    torch.cuda.current_stream(ctx.device).synchronize()
     R._abi.check(R._abi.lib().tr_get_film_device(ctx.h, R.C.c_void_p(out.data_ptr()), None, None))
     return out
 

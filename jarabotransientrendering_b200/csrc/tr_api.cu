@@ -17,119 +17,22 @@
 
 #include "bvh_build.h"
 #include "tr_device.cuh"
-#include "tr_kernels.cuh"
 #include "tr_film_io.h"
-#include "tr_guide.cuh"
+#include "tr_internal.h"
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
+namespace tri {
 tr_status fail(tr_status s, const std::string& msg) {
     g_last_error = msg;
     return s;
 }
+}  // namespace tri
 
-struct CudaError : std::runtime_error {
-    cudaError_t code;
-    CudaError(cudaError_t c, const char* what) : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
-};
+using namespace tri;
 
-#define TR_CUDA(call)                                           \
-    do {                                                        \
-        cudaError_t e_ = (call);                                \
-        if (e_ != cudaSuccess) throw CudaError(e_, #call);      \
-    } while (0)
-
-template <class T>
-T* dalloc(size_t count, size_t& total) {
-    if (count == 0) count = 1;
-    void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e != cudaSuccess) throw CudaError(e, "cudaMalloc");
-    total += count * sizeof(T);
-    return static_cast<T*>(p);
-}
-
-constexpr uint32_t kMaxBounces = 63;            // counters hold 64 depths
-constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batch
-constexpr size_t kSplatSmemBudget = 56 * 1024;   // four 512-thread splat CTAs per SM
-
-}  // namespace
-
-struct tr_guide;
-
-struct tr_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    size_t bytes = 0;
-    std::vector<void*> allocs;
-
-    // scene
-    float4* d_nodes = nullptr;
-    float4* d_tris = nullptr;
-    float4* d_tri_ng = nullptr;
-    float4* d_mats = nullptr;
-    float4* d_mats2 = nullptr;
-    float4* d_lights = nullptr;
-    trk::SceneDev scene{};
-    uint32_t nt = 0, bvh_nodes = 0, bvh_depth = 0;
-    double bvh_ms = 0.0;
-
-    tr_camera cam{};
-    tr_film film{};
-    tr_integrator integ{};
-
-    // film
-    double* d_streak = nullptr;
-    double* d_steady = nullptr;
-    double* d_weight = nullptr;
-
-    // wavefront state
-    trk::Wave wave{};
-    int trace_grid = 0;
-    int splat_g = 1;
-
-    // ray-batch scratch
-    float* d_rays = nullptr;
-    void* d_hits = nullptr;
-    uint32_t ray_cap = 0;
-    uint32_t* d_cursor = nullptr;
-
-    tr_stats stats{};
-    // learned proposal (tr_set_guide)
-    tr_guide* guide = nullptr;
-    float guide_mix = 0.5f, guide_lr = 1e-3f;
-    uint32_t guide_pool = 0;
-    trk::GuideWave gw{};
-    uint32_t gw_capacity = 0;
-    uint32_t* pool_state = nullptr;       // [0] pool fill, [1] entries with targets
-    float last_train_loss = 0.0f;
-    uint32_t train_steps = 0;
-    cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null
-    bool profiling = false;
-    std::vector<cudaEvent_t> prof_events; // pool of timing events
-    cudaStream_t s() const { return user_stream ? user_stream : stream; }
-
-    template <class T>
-    T* alloc(size_t n) {
-        T* p = dalloc<T>(n, bytes);
-        allocs.push_back(p);
-        return p;
-    }
-    void release() {
-        for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
-        prof_events.clear();
-        for (void* p : allocs) cudaFree(p);
-        allocs.clear();
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (stream) cudaStreamDestroy(stream);
-        ev0 = ev1 = nullptr;
-        stream = nullptr;
-    }
-};
 
 namespace {
 
@@ -190,6 +93,10 @@ void upload(void* dst, const void* src, size_t bytes) {
     TR_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
 }
 
+}  // namespace
+
+namespace tri {
+
 void ensure_wave(tr_ctx* x, uint32_t capacity) {
     if (x->wave.capacity >= capacity) return;
     // grow: drop the old buffers (they are only scratch between calls)
@@ -242,9 +149,6 @@ void ensure_guided(tr_ctx* x, uint32_t capacity) {
     x->gw_capacity = capacity;
 }
 
-trg::GuideDev guide_dev(tr_guide* g);
-int* guide_err(tr_guide* g);
-
 trk::Params make_params(tr_ctx* x) {
     trk::Params p{};
     p.scene = x->scene;
@@ -269,6 +173,10 @@ trk::Params make_params(tr_ctx* x) {
     }
     return p;
 }
+
+}  // namespace tri
+
+namespace {
 
 tr_status guide_after_render(tr_ctx* x, cudaStream_t s);
 
@@ -588,11 +496,15 @@ static tr_status copy_film(tr_ctx* x, double* streak, double* steady, double* we
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
     try {
         TR_CUDA(cudaSetDevice(x->device));
-        TR_CUDA(cudaStreamSynchronize(x->s()));
+        // on the context's stream (after its renders), and complete before returning: a
+        // device-to-device cudaMemcpy would return early and could race with a later
+        // tr_clear_film on the context's stream
+        cudaStream_t s = x->s();
         const size_t npix = (size_t)x->film.width * x->film.height;
-        if (streak) TR_CUDA(cudaMemcpy(streak, x->d_streak, npix * x->film.time_bins * 3u * sizeof(double), kind));
-        if (steady) TR_CUDA(cudaMemcpy(steady, x->d_steady, npix * 3u * sizeof(double), kind));
-        if (weight) TR_CUDA(cudaMemcpy(weight, x->d_weight, npix * sizeof(double), kind));
+        if (streak) TR_CUDA(cudaMemcpyAsync(streak, x->d_streak, npix * x->film.time_bins * 3u * sizeof(double), kind, s));
+        if (steady) TR_CUDA(cudaMemcpyAsync(steady, x->d_steady, npix * 3u * sizeof(double), kind, s));
+        if (weight) TR_CUDA(cudaMemcpyAsync(weight, x->d_weight, npix * sizeof(double), kind, s));
+        TR_CUDA(cudaStreamSynchronize(s));
     } catch (const CudaError& e) {
         return fail(TR_ERR_CUDA, e.what());
     }
@@ -789,54 +701,8 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
 // -----------------------------------------------------------------------------------------
 // learned proposal network
 // -----------------------------------------------------------------------------------------
-struct tr_guide {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::vector<void*> allocs;
-    size_t bytes = 0;
-    float* params = nullptr;   // FP32 master copy
-    float* grads = nullptr;
-    float* m1 = nullptr;
-    float* m2 = nullptr;
-    uint8_t* w_fwd = nullptr;  // packed BF16 tiles
-    uint8_t* w_bwd = nullptr;
-    int* err = nullptr;
-    float* scalars = nullptr;  // [0] weight sum, [1] loss
-    uint32_t cap = 0;
-    uint4* act = nullptr;
-    float* out = nullptr;
-    uint4* dy_bf = nullptr;
-    float* dy_f = nullptr;
-    float* dh = nullptr;
-    uint32_t step = 0;
-    template <class T>
-    T* alloc(size_t n) {
-        T* p = dalloc<T>(n, bytes);
-        allocs.push_back(p);
-        return p;
-    }
-    void drop(void* p) {
-        if (!p) return;
-        cudaFree(p);
-        allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
-    }
-    trg::GuideDev dev() const {
-        return trg::GuideDev{reinterpret_cast<const uint4*>(w_fwd), reinterpret_cast<const uint4*>(w_bwd),
-                             params + 4 * 4096};
-    }
-    void ensure(uint32_t n) {
-        if (cap >= n) return;
-        drop(act); drop(out); drop(dy_bf); drop(dy_f); drop(dh);
-        act = alloc<uint4>((size_t)3 * n * 8);
-        out = alloc<float>((size_t)n * trg::kOut);
-        dy_bf = alloc<uint4>((size_t)n * 8);
-        dy_f = alloc<float>((size_t)n * 64);
-        dh = alloc<float>((size_t)3 * n * 64);
-        cap = n;
-    }
-};
 
-namespace {
+namespace tri {
 tr_status guide_check_err(tr_guide* g, cudaStream_t s) {
     int e = 0;
     TR_CUDA(cudaMemcpyAsync(&e, g->err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -847,7 +713,7 @@ tr_status guide_check_err(tr_guide* g, cudaStream_t s) {
     }
     return TR_OK;
 }
-}  // namespace
+}  // namespace tri
 
 extern "C" tr_status tr_guide_create(int device, uint64_t seed, tr_guide** out) {
     if (!out) return fail(TR_ERR_INVALID_ARGUMENT, "out is null");
@@ -950,7 +816,7 @@ extern "C" tr_status tr_guide_forward(tr_guide* g, const uint16_t* d_features, u
     }
 }
 
-namespace {
+namespace tri {
 // Enqueues one training step (forward, loss gradient, backward, weight gradients, Adam, weight
 // repacking) on stream s without waiting for it; the loss lands in g->scalars[1].
 void train_enqueue(tr_guide* g, const uint4* x, const float* d_dirs, const float* d_weights, uint32_t n, float lr,
@@ -976,7 +842,7 @@ void train_enqueue(tr_guide* g, const uint4* x, const float* d_dirs, const float
         TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, s));
     }
 }
-}  // namespace
+}  // namespace tri
 
 extern "C" tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features, const float* d_dirs,
                                          const float* d_weights, uint32_t n, float lr, float* loss, void* stream) {
@@ -1003,39 +869,45 @@ extern "C" tr_status tr_guide_destroy(tr_guide* g) {
     return TR_OK;
 }
 
-namespace {
+namespace tri {
 trg::GuideDev guide_dev(tr_guide* g) { return g->dev(); }
 int* guide_err(tr_guide* g) { return g->err; }
 
-// After a guided render: surface an MMA timeout, then train on the collected pool.
-tr_status guide_after_render(tr_ctx* x, cudaStream_t s) {
-    x->stats.train_steps = 0;
-    if (!x->guide_pool) return guide_check_err(x->guide, s);
+tr_status train_on_pool(tr_guide* g, const trk::GuideWave& gw, const uint32_t* pool_state, uint32_t pool, float lr,
+                        cudaStream_t s, tr_stats& stats) {
+    stats.train_steps = 0;
+    if (!pool) return guide_check_err(g, s);
     // one synchronisation for the render's MMA status and the pool fill ...
     int e = 0;
     uint32_t fill = 0;
-    TR_CUDA(cudaMemcpyAsync(&e, x->guide->err, sizeof(int), cudaMemcpyDeviceToHost, s));
-    TR_CUDA(cudaMemcpyAsync(&fill, x->pool_state, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(cudaMemcpyAsync(&e, g->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(cudaMemcpyAsync(&fill, pool_state, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     TR_CUDA(cudaStreamSynchronize(s));
-    if (e) return guide_check_err(x->guide, s);
+    if (e) return guide_check_err(g, s);
     // ... the training steps are enqueued back to back, and one more for their status and loss
-    const uint32_t n = std::min(fill, x->guide_pool);
+    const uint32_t n = std::min(fill, pool);
     const uint32_t batch = 65536;
     try {
         for (uint32_t off = 0; off + 1024 <= n; off += batch) {
             const uint32_t m = std::min(batch, n - off);
-            train_enqueue(x->guide, x->gw.pool_feat + (size_t)off * 8, x->gw.pool_dir + (size_t)off * 3,
-                          x->gw.pool_w + off, m, x->guide_lr, s);
-            x->stats.train_steps += 1;
+            train_enqueue(g, gw.pool_feat + (size_t)off * 8, gw.pool_dir + (size_t)off * 3, gw.pool_w + off, m, lr, s);
+            stats.train_steps += 1;
         }
     } catch (const CudaError& err) {
         return fail(err.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, err.what());
     }
-    if (x->stats.train_steps) {
-        TR_CUDA(cudaMemcpyAsync(&x->stats.train_loss, x->guide->scalars + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
-        return guide_check_err(x->guide, s);
+    if (stats.train_steps) {
+        TR_CUDA(cudaMemcpyAsync(&stats.train_loss, g->scalars + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+        return guide_check_err(g, s);
     }
     return TR_OK;
+}
+}  // namespace tri
+
+namespace {
+// After a guided render: surface an MMA timeout, then train on the collected pool.
+tr_status guide_after_render(tr_ctx* x, cudaStream_t s) {
+    return train_on_pool(x->guide, x->gw, x->pool_state, x->guide_pool, x->guide_lr, s, x->stats);
 }
 }  // namespace
 

@@ -15,10 +15,12 @@ using namespace trd;
 
 // Features of a surface vertex for the learned proposal (64 BF16 values, 46 used):
 // sin/cos(2^k pi p_d) for k = 0..5 (index 6k + 2d + {0,1}), p normalised to the scene box,
-// geometric normal, outgoing direction, path length / film time length.  Octave k+1 follows
+// geometric normal, outgoing direction, path length / film time length; in multi-scene mode
+// [46 + scene] = 1 (one network serves up to 16 scenes).  Octave k+1 follows
 // from octave k by the double-angle identities (sin 2x = 2 sin x cos x, cos 2x = 1 - 2 sin^2 x);
 // the rounding error doubles per octave, about 3e-6 at k = 5, far below BF16 resolution.
-__device__ __forceinline__ void write_features(uint4* row, const SceneDev& sc, f3 pos, f3 nrm, f3 wo, float tn) {
+__device__ __forceinline__ void write_features(uint4* row, const SceneDev& sc, f3 pos, f3 nrm, f3 wo, float tn,
+                                               int scene_onehot = -1) {
     float v[64];
     const float pn[3] = {(pos.x - sc.bmin[0]) * sc.binv[0], (pos.y - sc.bmin[1]) * sc.binv[1],
                          (pos.z - sc.bmin[2]) * sc.binv[2]};
@@ -40,7 +42,7 @@ __device__ __forceinline__ void write_features(uint4* row, const SceneDev& sc, f
     v[42] = wo.x; v[43] = wo.y; v[44] = wo.z;
     v[45] = tn;
 #pragma unroll
-    for (int k = 46; k < 64; ++k) v[k] = 0.0f;
+    for (int k = 46; k < 64; ++k) v[k] = k - 46 == scene_onehot ? 1.0f : 0.0f;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         __nv_bfloat162 a = __floats2bfloat162_rn(v[8 * c], v[8 * c + 1]);
@@ -127,12 +129,12 @@ __device__ __forceinline__ bool ggx_sample_fast(const GgxVertex& g, float sp, fl
 // accumulator row in registers and samples the direction.  Neither features nor mixtures touch
 // HBM.  Four CTAs per SM (50 KB shared memory, 64 TMEM columns each) overlap one CTA's MMA waits
 // with the others' gathers.
-__global__ void __launch_bounds__(128, 4) k_guide(Params p, int depth, uint32_t* pool_count) {
+template <bool kMulti>
+__global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params p, int depth, uint32_t* pool_count) {
     const GuideWave& G = p.guide;
     const uint32_t n = p.wave.counters[cnt_guide(depth)];
     if (blockIdx.x * (uint32_t)trg::kTile >= n) return;     // no tile for this CTA
     extern __shared__ __align__(1024) uint8_t smem[];
-    const SceneDev& sc = p.scene;
     uint8_t* sA = smem + trg::kSmemA;
     const float* sB = reinterpret_cast<const float*>(smem + trg::kSmemBias);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + trg::kSmemBar);
@@ -151,9 +153,20 @@ __global__ void __launch_bounds__(128, 4) k_guide(Params p, int depth, uint32_t*
     bool ok = true;
 
     uint32_t* qout = p.wave.q[(depth + 1) & 1];
-    const bool medium = sc.medium != 0;
-    const float total_time = (float)p.film.T * p.film.exposure + p.film.offset;
     const float c = G.mix_prob;
+    // scene, film length and scene feature of a slot: the launch's own in single-scene mode
+    struct SlotScene { const SceneDev* sc; float total_time; int onehot; };
+    auto scene_of = [&](uint32_t slot) {
+        SlotScene r{&p.scene, (float)p.film.T * p.film.exposure + p.film.offset, -1};
+        if constexpr (kMulti) {
+            const Batch& Bs = seg_of_slot(cur_batch(p), slot);
+            const SceneSlot& S = p.multi.scenes[Bs.scene];
+            r.sc = &S.scene;
+            r.total_time = (float)S.film.T * S.film.exposure + S.film.offset;
+            r.onehot = (int)Bs.scene;
+        }
+        return r;
+    };
     const unsigned lane = tid & 31u;
     for (uint32_t tile = blockIdx.x; tile * (uint32_t)trg::kTile < n && ok; tile += gridDim.x) {
         const uint32_t idx = tile * (uint32_t)trg::kTile + tid;
@@ -167,8 +180,9 @@ __global__ void __launch_bounds__(128, 4) k_guide(Params p, int depth, uint32_t*
                 const float4 r0 = __ldg(reinterpret_cast<const float4*>(rec));
                 const float4 r1 = __ldg(reinterpret_cast<const float4*>(rec + 1));
                 const float4 r3 = __ldg(reinterpret_cast<const float4*>(rec + 3));
-                write_features(feat, sc, mk(r0.x, r0.y, r0.z), mk(r3.x, r3.y, r3.z), mk(-r1.x, -r1.y, -r1.z),
-                               r0.w / total_time);
+                const SlotScene ss = scene_of(__float_as_uint(r3.w));
+                write_features(feat, *ss.sc, mk(r0.x, r0.y, r0.z), mk(r3.x, r3.y, r3.z), mk(-r1.x, -r1.y, -r1.z),
+                               r0.w / ss.total_time, ss.onehot);
             } else {
 #pragma unroll
                 for (int q = 0; q < 8; ++q) feat[q] = make_uint4(0u, 0u, 0u, 0u);
@@ -214,6 +228,9 @@ __global__ void __launch_bounds__(128, 4) k_guide(Params p, int depth, uint32_t*
             const float4 rn = __ldg(reinterpret_cast<const float4*>(rec + 3));
             const uint4 rr = __ldg(rec + 4);
             slot = __float_as_uint(rn.w);
+            const SlotScene ss = scene_of(slot);
+            const SceneDev& sc = *ss.sc;
+            const bool medium = sc.medium != 0;
             const uint32_t mi = __float_as_uint(th.w);
             const f3 nrm = mk(rn.x, rn.y, rn.z);
             const float4 m = __ldg(&sc.mats[mi]);
@@ -274,7 +291,8 @@ __global__ void __launch_bounds__(128, 4) k_guide(Params p, int depth, uint32_t*
                     if (keep) {
                         const uint32_t k = atomicAdd(pool_count, 1u);
                         if (k < G.pool_cap) {
-                            write_features(G.pool_feat + (size_t)k * 8, sc, pos, nrm, wo, time / total_time);
+                            write_features(G.pool_feat + (size_t)k * 8, sc, pos, nrm, wo, time / ss.total_time,
+                                           ss.onehot);
                             G.pool_dir[3 * (size_t)k] = wi.x;
                             G.pool_dir[3 * (size_t)k + 1] = wi.y;
                             G.pool_dir[3 * (size_t)k + 2] = wi.z;
@@ -328,14 +346,23 @@ __global__ void k_train_mark(uint32_t* pool_state, uint32_t cap) {
 cudaError_t launch_guide(const Params& p, int depth, uint32_t* pool_state, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_guide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trg::kSmemBytes);
+        cudaError_t e = cudaFuncSetAttribute(k_guide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trg::kSmemBytes);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_guide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trg::kSmemBytes);
         if (e != cudaSuccess) return e;
         attr = true;
     }
     int dev = 0;
     cudaGetDevice(&dev);
-    const int grid = trg::resident_grid(dev, reinterpret_cast<const void*>(k_guide), 128, trg::kSmemBytes);
-    k_guide<<<grid, 128, trg::kSmemBytes, s>>>(p, depth, pool_state);
+    if (p.multi.scenes) {
+        static int grid = 0;
+        if (!grid) grid = trg::resident_grid(dev, reinterpret_cast<const void*>(k_guide<true>), 128, trg::kSmemBytes);
+        k_guide<true><<<grid, 128, trg::kSmemBytes, s>>>(p, depth, pool_state);
+    } else {
+        static int grid = 0;
+        if (!grid) grid = trg::resident_grid(dev, reinterpret_cast<const void*>(k_guide<false>), 128, trg::kSmemBytes);
+        k_guide<false><<<grid, 128, trg::kSmemBytes, s>>>(p, depth, pool_state);
+    }
     return cudaGetLastError();
 }
 

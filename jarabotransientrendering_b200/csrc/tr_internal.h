@@ -1,0 +1,184 @@
+// tr_internal.h - host-side internals shared by the C ABI translation units (tr_api.cu: one
+// scene per context; tr_batch.cu: many contexts rendered in shared wavefront batches).
+#pragma once
+#include "transient_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "tr_guide.cuh"
+#include "tr_kernels.cuh"
+
+namespace tri {
+
+// records msg as the thread's last error (tr_last_error) and returns s
+tr_status fail(tr_status s, const std::string& msg);
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* what) : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+#define TR_CUDA(call)                                           \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) throw CudaError(e_, #call);      \
+    } while (0)
+
+template <class T>
+T* dalloc(size_t count, size_t& total) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) throw CudaError(e, "cudaMalloc");
+    total += count * sizeof(T);
+    return static_cast<T*>(p);
+}
+
+constexpr uint32_t kMaxBounces = 63;            // counters hold 64 depths
+constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batch
+constexpr size_t kSplatSmemBudget = 56 * 1024;   // four 512-thread splat CTAs per SM
+
+}  // namespace tri
+
+using tri::dalloc;
+
+struct tr_guide {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    float* params = nullptr;   // FP32 master copy
+    float* grads = nullptr;
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    uint8_t* w_fwd = nullptr;  // packed BF16 tiles
+    uint8_t* w_bwd = nullptr;
+    int* err = nullptr;
+    float* scalars = nullptr;  // [0] weight sum, [1] loss
+    uint32_t cap = 0;
+    uint4* act = nullptr;
+    float* out = nullptr;
+    uint4* dy_bf = nullptr;
+    float* dy_f = nullptr;
+    float* dh = nullptr;
+    uint32_t step = 0;
+    template <class T>
+    T* alloc(size_t n) {
+        T* p = tri::dalloc<T>(n, bytes);
+        allocs.push_back(p);
+        return p;
+    }
+    void drop(void* p) {
+        if (!p) return;
+        cudaFree(p);
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
+    }
+    trg::GuideDev dev() const {
+        return trg::GuideDev{reinterpret_cast<const uint4*>(w_fwd), reinterpret_cast<const uint4*>(w_bwd),
+                             params + 4 * 4096};
+    }
+    void ensure(uint32_t n) {
+        if (cap >= n) return;
+        drop(act); drop(out); drop(dy_bf); drop(dy_f); drop(dh);
+        act = alloc<uint4>((size_t)3 * n * 8);
+        out = alloc<float>((size_t)n * trg::kOut);
+        dy_bf = alloc<uint4>((size_t)n * 8);
+        dy_f = alloc<float>((size_t)n * 64);
+        dh = alloc<float>((size_t)3 * n * 64);
+        cap = n;
+    }
+};
+
+struct tr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    // scene
+    float4* d_nodes = nullptr;
+    float4* d_tris = nullptr;
+    float4* d_tri_ng = nullptr;
+    float4* d_mats = nullptr;
+    float4* d_mats2 = nullptr;
+    float4* d_lights = nullptr;
+    trk::SceneDev scene{};
+    uint32_t nt = 0, bvh_nodes = 0, bvh_depth = 0;
+    double bvh_ms = 0.0;
+
+    tr_camera cam{};
+    tr_film film{};
+    tr_integrator integ{};
+
+    // film
+    double* d_streak = nullptr;
+    double* d_steady = nullptr;
+    double* d_weight = nullptr;
+
+    // wavefront state
+    trk::Wave wave{};
+    int trace_grid = 0;
+    int splat_g = 1;
+
+    // ray-batch scratch
+    float* d_rays = nullptr;
+    void* d_hits = nullptr;
+    uint32_t ray_cap = 0;
+    uint32_t* d_cursor = nullptr;
+
+    tr_stats stats{};
+    // learned proposal (tr_set_guide)
+    tr_guide* guide = nullptr;
+    float guide_mix = 0.5f, guide_lr = 1e-3f;
+    uint32_t guide_pool = 0;
+    trk::GuideWave gw{};
+    uint32_t gw_capacity = 0;
+    uint32_t* pool_state = nullptr;       // [0] pool fill, [1] entries with targets
+    float last_train_loss = 0.0f;
+    uint32_t train_steps = 0;
+    cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events; // pool of timing events
+    cudaStream_t s() const { return user_stream ? user_stream : stream; }
+
+    template <class T>
+    T* alloc(size_t n) {
+        T* p = tri::dalloc<T>(n, bytes);
+        allocs.push_back(p);
+        return p;
+    }
+    void release() {
+        for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
+        prof_events.clear();
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+        ev0 = ev1 = nullptr;
+        stream = nullptr;
+    }
+};
+
+namespace tri {
+
+void ensure_wave(tr_ctx* x, uint32_t capacity);
+void ensure_guided(tr_ctx* x, uint32_t capacity);
+trk::Params make_params(tr_ctx* x);
+trg::GuideDev guide_dev(tr_guide* g);
+int* guide_err(tr_guide* g);
+tr_status guide_check_err(tr_guide* g, cudaStream_t s);
+// enqueues one training step of the proposal on stream s (no host synchronisation)
+void train_enqueue(tr_guide* g, const uint4* x, const float* d_dirs, const float* d_weights, uint32_t n, float lr,
+                   cudaStream_t s);
+// trains the proposal on the pool a guided render collected (`fill` = pool_state on the device)
+tr_status train_on_pool(tr_guide* g, const trk::GuideWave& gw, const uint32_t* pool_state, uint32_t pool,
+                        float lr, cudaStream_t s, tr_stats& stats);
+
+}  // namespace tri

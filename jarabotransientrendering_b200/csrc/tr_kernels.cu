@@ -98,28 +98,42 @@ done:
 // (PinholeCamera.h:82-91); per-path PCG32 stream; free flight in a world medium
 // (BidirectionalPathTracing.h:240-268).
 // -----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_raygen(Params p) {
-    const Batch& B = p.batch;
+template <bool kMulti>
+__global__ void __launch_bounds__(256) k_raygen(const __grid_constant__ Params p) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n_slots) return;
+    const Batch* Bp = &p.batch;
+    const SceneSlot* SS = nullptr;
+    if constexpr (kMulti) {
+        const BatchDesc& BD = cur_batch(p);
+        if (i >= BD.n_slots) return;
+        Bp = &seg_of_slot(BD, i);
+        SS = p.multi.scenes + Bp->scene;
+    } else {
+        if (i >= p.batch.n_slots) return;
+    }
+    const Batch& B = *Bp;
+    const FilmDev& film = kMulti ? SS->film : p.film;
+    const CameraDev& c = kMulti ? SS->cam : p.cam;
+    const unsigned long long seed = kMulti ? SS->seed : p.seed;
     const uint32_t per_pix = B.ns * B.ninc;
-    const uint32_t pl = i / per_pix;
-    const uint32_t rem = i - pl * per_pix;
+    const uint32_t li = i - B.slot_begin;
+    const uint32_t pl = li / per_pix;
+    const uint32_t rem = li - pl * per_pix;
     const uint32_t sl = rem / B.ninc;
     const uint32_t j = rem - sl * B.ninc;
     const uint32_t wpix = B.pix_begin + pl;
     const uint32_t py = B.win_y0 + wpix / B.win_w;
     const uint32_t px = B.win_x0 + wpix % B.win_w;
     const unsigned long long s = B.s0 + sl;
-    const uint32_t W = p.film.W, H = p.film.H;
+    const uint32_t W = film.W, H = film.H;
     const uint32_t pixel = py * W + px;
 
-    const uint32_t strata = p.sqrt_spp;
+    const uint32_t strata = kMulti ? SS->sqrt_spp : p.sqrt_spp;
     const uint32_t spp = strata * strata;
     const uint32_t st = (uint32_t)(s % spp);
     const uint32_t subx = st % strata, suby = st / strata;
     Pcg cr;
-    pcg_seed(cr, p.seed, cam_id(pixel, s));
+    pcg_seed(cr, seed, cam_id(pixel, s));
     const float inv = 1.0f / (float)strata;
     const float shx = ((float)subx + pcg_float(cr)) * inv;
     const float shy = ((float)suby + pcg_float(cr)) * inv;
@@ -129,17 +143,17 @@ __global__ void __launch_bounds__(256) k_raygen(Params p) {
     const float ratio = Wf / Hf;
     const float imx = (posx - Wf / 2.0f) / Wf;
     const float imy = ((posy - Hf / 2.0f) / Hf) / ratio;
-    const CameraDev& c = p.cam;
     const f3 nv = mk(c.nv[0], c.nv[1], c.nv[2]);
     const f3 uv = mk(c.uv[0], c.uv[1], c.uv[2]);
     const f3 vv = mk(c.vv[0], c.vv[1], c.vv[2]);
     const f3 dd = ((nv * c.fd) + ((uv * 2.0f) * imx)) - ((vv * 2.0f) * imy);
     const f3 d = normalize(dd);
 
+    const SceneDev& sc = kMulti ? SS->scene : p.scene;
     Pcg r;
-    pcg_seed(r, p.seed + (unsigned long long)(j + 1) * kGolden64, cam_id(pixel, s));
+    pcg_seed(r, seed + (unsigned long long)(j + 1) * kGolden64, cam_id(pixel, s));
     float dsamp = __int_as_float(0x7f800000);
-    if (p.scene.medium) dsamp = -tr_log(pcg_float(r)) / p.scene.lambda;
+    if (sc.medium) dsamp = -tr_log(pcg_float(r)) / sc.lambda;
 
     p.wave.ray_o[i] = make_float4(c.pos[0], c.pos[1], c.pos[2], dsamp);
     p.wave.ray_d[i] = make_float4(d.x, d.y, d.z, 0.0f);
@@ -151,9 +165,12 @@ __global__ void __launch_bounds__(256) k_raygen(Params p) {
 // -----------------------------------------------------------------------------------------
 // extend / shadow: persistent warps fetch 32 queue entries at a time.
 // -----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(Params p, int depth) {
+template <bool kMulti>
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(const __grid_constant__ Params p, int depth) {
     extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
-    const uint32_t n = depth == 0 ? p.batch.n_slots : p.wave.counters[cnt_ext(depth)];
+    uint32_t n0 = p.batch.n_slots;
+    if constexpr (kMulti) n0 = cur_batch(p).n_slots;
+    const uint32_t n = depth == 0 ? n0 : p.wave.counters[cnt_ext(depth)];
     const uint32_t* q = p.wave.q[depth & 1];
     const unsigned lane = threadIdx.x & 31u;
     uint32_t* cursor = &p.wave.counters[cur_ext(depth)];
@@ -166,18 +183,21 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(Params 
         const uint32_t idx = base + lane;
         if (idx < n) {
             const uint32_t slot = depth == 0 ? idx : q[idx];
+            const SceneDev* sc = &p.scene;
+            if constexpr (kMulti) sc = &p.multi.scenes[seg_of_slot(cur_batch(p), slot).scene].scene;
             const float4 o = p.wave.ray_o[slot];
             const float4 d = p.wave.ray_d[slot];
             WRay r;
             wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
             float t, u, v;
-            const uint32_t id = traverse<false>(p.scene, r, o.w, t, u, v, stack + threadIdx.x, kTraceBlock);
+            const uint32_t id = traverse<false>(*sc, r, o.w, t, u, v, stack + threadIdx.x, kTraceBlock);
             p.wave.hit[slot] = make_float4(t, __uint_as_float(id), u, v);
         }
     }
 }
 
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(Params p, int depth) {
+template <bool kMulti>
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(const __grid_constant__ Params p, int depth) {
     extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
     const uint32_t n = p.wave.counters[cnt_sh(depth)];
     const unsigned lane = threadIdx.x & 31u;
@@ -194,10 +214,13 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(Params 
         if (idx < n) {
             const float4 o = p.wave.sh_o[idx];
             const float4 d = p.wave.sh_d[idx];
+            const SceneDev* sc = &p.scene;
+            if constexpr (kMulti)
+                sc = &p.multi.scenes[seg_of_slot(cur_batch(p), __float_as_uint(p.wave.sh_L[idx].w)).scene].scene;
             WRay r;
             wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
             float t, u, v;
-            const uint32_t id = traverse<true>(p.scene, r, o.w, t, u, v, stack + threadIdx.x, kTraceBlock);
+            const uint32_t id = traverse<true>(*sc, r, o.w, t, u, v, stack + threadIdx.x, kTraceBlock);
             if (id == kInvalid) {
                 const float4 L = p.wave.sh_L[idx];
                 const uint32_t slot = __float_as_uint(L.w);
@@ -225,23 +248,16 @@ __device__ __forceinline__ float hg_eval(float g, float cs) {
     return ((1.0f - gg) * kInv4Pi) / (b * sqrtf(b));
 }
 
-template <bool kGuided>
-__global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
-    const SceneDev& sc = p.scene;
-    const uint32_t n = depth == 0 ? p.batch.n_slots : p.wave.counters[cnt_ext(depth)];
+template <bool kGuided, bool kMulti>
+__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p, int depth) {
+    uint32_t n0 = p.batch.n_slots;
+    if constexpr (kMulti) n0 = cur_batch(p).n_slots;
+    const uint32_t n = depth == 0 ? n0 : p.wave.counters[cnt_ext(depth)];
     const uint32_t* qin = p.wave.q[depth & 1];
     uint32_t* qout = p.wave.q[(depth + 1) & 1];
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const bool medium = sc.medium != 0;
-    const f3 sig_s = mk(sc.sig_s[0], sc.sig_s[1], sc.sig_s[2]);
-    const f3 sig_t = mk(sc.sig_t[0], sc.sig_t[1], sc.sig_t[2]);
-    const float lambda = sc.lambda;
-    const float g = sc.g;
-    const float total_time = (float)p.film.T * p.film.exposure + p.film.offset;
-    const float inv_inc = 1.0f / (float)p.batch.ninc;
-    const uint32_t per_pix = p.batch.ns * p.batch.ninc;
 
     for (uint32_t base = warp_global * 32u; base < n; base += nwarps * 32u) {
         const uint32_t idx = base + lane;
@@ -251,6 +267,28 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
         float4 sh_o = make_float4(0, 0, 0, 0), sh_d = make_float4(0, 0, 0, 0), sh_L = make_float4(0, 0, 0, 0);
         if (idx < n) {
             slot = depth == 0 ? idx : qin[idx];
+            // the slot's segment (pixels, samples) and scene: the launch's own in single-scene
+            // mode, looked up in the current batch descriptor in multi-scene mode
+            const Batch* Bp = &p.batch;
+            const SceneSlot* SS = nullptr;
+            if constexpr (kMulti) {
+                Bp = &seg_of_slot(cur_batch(p), slot);
+                SS = p.multi.scenes + Bp->scene;
+            }
+            const Batch& B = *Bp;
+            const SceneDev& sc = kMulti ? SS->scene : p.scene;
+            const FilmDev& film = kMulti ? SS->film : p.film;
+            const uint32_t max_bounces = kMulti ? SS->max_bounces : p.max_bounces;
+            const uint32_t flags = kMulti ? SS->flags : p.flags;
+            const bool medium = sc.medium != 0;
+            const f3 sig_s = mk(sc.sig_s[0], sc.sig_s[1], sc.sig_s[2]);
+            const f3 sig_t = mk(sc.sig_t[0], sc.sig_t[1], sc.sig_t[2]);
+            const float lambda = sc.lambda;
+            const float g = sc.g;
+            const float total_time = (float)film.T * film.exposure + film.offset;
+            const float inv_inc = 1.0f / (float)B.ninc;
+            const uint32_t per_pix = B.ns * B.ninc;
+            const uint32_t lslot = slot - B.slot_begin;
             const float4 h = p.wave.hit[slot];
             const float4 ro = p.wave.ray_o[slot];
             const float4 rd = p.wave.ray_d[slot];
@@ -261,14 +299,13 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
             const bool surface = hit && (!medium || h.x < dsamp);
             if (medium || hit) {
                 // per-path RNG: state in memory, increment from the camera sample
-                const uint32_t pl = slot / per_pix;
-                const uint32_t sl = (slot - pl * per_pix) / p.batch.ninc;
-                const uint32_t wpix = p.batch.pix_begin + pl;
-                const uint32_t pixel = (p.batch.win_y0 + wpix / p.batch.win_w) * p.film.W +
-                                       (p.batch.win_x0 + wpix % p.batch.win_w);
+                const uint32_t pl = lslot / per_pix;
+                const uint32_t sl = (lslot - pl * per_pix) / B.ninc;
+                const uint32_t wpix = B.pix_begin + pl;
+                const uint32_t pixel = (B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
                 Pcg rng;
                 rng.state = p.wave.rng[slot];
-                rng.inc = (cam_id(pixel, p.batch.s0 + sl) << 1u) | 1ull;
+                rng.inc = (cam_id(pixel, B.s0 + sl) << 1u) | 1ull;
 
                 float dist, pd;
                 if (surface) { dist = h.x; pd = medium ? tr_exp(-(dist * lambda)) : 1.0f; }
@@ -350,8 +387,8 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
                             const float Lg = (f.y * (fe.y * (irr.y * att.y))) * scale;
                             const float Lb = (f.z * (fe.z * (irr.z * att.z))) * scale;
                             const float tt = time + dl;
-                            const float ps = (tt - p.film.offset) / p.film.exposure;
-                            if (ps < (float)p.film.T && ps >= 0.0f && finite3(Lr, Lg, Lb) &&
+                            const float ps = (tt - film.offset) / film.exposure;
+                            if (ps < (float)film.T && ps >= 0.0f && finite3(Lr, Lg, Lb) &&
                                 (Lr != 0.0f || Lg != 0.0f || Lb != 0.0f)) {
                                 want_shadow = true;
                                 sh_o = make_float4(lp.x, lp.y, lp.z, dl - kSigmaVis);
@@ -361,7 +398,7 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
                             }
                         }
                     }
-                    if ((uint32_t)depth + 1u < p.max_bounces) {
+                    if ((uint32_t)depth + 1u < max_bounces) {
                         // ---- Russian roulette ----
                         const float albedo = surface ? avg3(kd)
                             : avg3(mk(sig_s.x / sig_t.x, sig_s.y / sig_t.y, sig_s.z / sig_t.z));
@@ -385,7 +422,7 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
                             bool alive = true;
                             if (surface && ggx) {
                                 alive = ggx_sample(kd, alpha, nrm, wo, sp, cp, x2, nd, fa, pa);
-                            } else if (surface && (p.flags & kFlagOrthoFrame)) {
+                            } else if (surface && (flags & kFlagOrthoFrame)) {
                                 // cosine sampling in an orthonormal frame (Duff et al. 2017)
                                 const float ct = sqrtf(x2);
                                 const float stt = sqrtf(1.0f - ct * ct);
@@ -486,12 +523,27 @@ __global__ void __launch_bounds__(256) k_shade(Params p, int depth) {
 // A CTA owns `G` whole pixels of the batch, accumulates their records in an FP32 shared-memory
 // tile (warp-aggregated atomics on equal (pixel, bin) keys) and adds the tile to the FP64 film.
 // -----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSplatBlock) k_splat(Params p, int G) {
+template <bool kMulti>
+__global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ Params p, int G_launch) {
     extern __shared__ __align__(16) float tile[];
-    const uint32_t T = p.film.T;
+    // the block's segment and film: the launch's own in single-scene mode; in multi-scene mode
+    // from the current batch's block table, each segment with its own film-tile width
+    const Batch* Bp = &p.batch;
+    const FilmDev* Fp = &p.film;
+    uint32_t G = (uint32_t)G_launch, blk = blockIdx.x;
+    if constexpr (kMulti) {
+        const BatchDesc& BD = cur_batch(p);
+        if (blockIdx.x >= BD.n_blocks) return;
+        Bp = &seg_of_block(BD, blockIdx.x);
+        Fp = &p.multi.scenes[Bp->scene].film;
+        G = Bp->splat_g;
+        blk = blockIdx.x - Bp->blk_begin;
+    }
+    const Batch& B = *Bp;
+    const FilmDev& film = *Fp;
+    const uint32_t T = film.T;
     const uint32_t TT = T * 3u;
-    const Batch& B = p.batch;
-    const uint32_t pix0 = blockIdx.x * (uint32_t)G;
+    const uint32_t pix0 = blk * G;
     if (pix0 >= B.npix) return;
     const uint32_t gp = min((uint32_t)G, B.npix - pix0);
     float* steady = tile + (size_t)G * TT;
@@ -503,7 +555,7 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(Params p, int G) {
     __syncthreads();
     const uint32_t per_pix = B.ns * B.ninc;
     const uint32_t nslots = gp * per_pix;
-    const uint32_t slot0 = pix0 * per_pix;
+    const uint32_t slot0 = B.slot_begin + pix0 * per_pix;
     const size_t rs = p.wave.capacity;           // records are [bounce][slot]
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt = lanemask_lt();
@@ -560,8 +612,8 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(Params p, int G) {
     // independent loads in flight per thread
     for (uint32_t pl = 0; pl < gp; ++pl) {
         const uint32_t wpix = B.pix_begin + pix0 + pl;
-        const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * p.film.W + (B.win_x0 + wpix % B.win_w);
-        double* dst = p.film.streak + pixel * TT;
+        const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
+        double* dst = film.streak + pixel * TT;
         const float* src = tile + (size_t)pl * TT;
         for (uint32_t e0 = threadIdx.x; e0 < TT; e0 += 4u * blockDim.x) {
             float v[4];
@@ -579,8 +631,8 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(Params p, int G) {
             }
         }
         if (threadIdx.x == 0) {
-            p.film.weight[pixel] += (double)B.ns;
-            for (int c = 0; c < 3; ++c) p.film.steady[pixel * 3 + c] += (double)steady[pl * 3 + c];
+            film.weight[pixel] += (double)B.ns;
+            for (int c = 0; c < 3; ++c) film.steady[pixel * 3 + c] += (double)steady[pl * 3 + c];
         }
     }
 }
@@ -619,10 +671,17 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_user(Sce
 // -----------------------------------------------------------------------------------------
 size_t trace_smem_bytes(uint32_t bvh_depth) { return (size_t)(bvh_depth + 1u) * kTraceBlock * sizeof(int); }
 
-int trace_grid_size(int device, uint32_t bvh_depth) {
-    int sms = 0, per_sm = 0;
+int trace_grid_size(int device, uint32_t bvh_depth, bool multi) {
+    int sms = 0, per_sm = 0, per_sm_sh = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend, kTraceBlock, trace_smem_bytes(bvh_depth));
+    if (multi) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend<true>, kTraceBlock, trace_smem_bytes(bvh_depth));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_sh, k_shadow<true>, kTraceBlock, trace_smem_bytes(bvh_depth));
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend<false>, kTraceBlock, trace_smem_bytes(bvh_depth));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_sh, k_shadow<false>, kTraceBlock, trace_smem_bytes(bvh_depth));
+    }
+    per_sm = per_sm_sh < per_sm ? per_sm_sh : per_sm;
     if (per_sm < 1) per_sm = 1;
     return sms * per_sm;
 }
@@ -632,40 +691,67 @@ size_t splat_smem_bytes(uint32_t T, int G) {
     return (((size_t)G * T * 3u + 3u * (size_t)G) * sizeof(float) + 15u) & ~size_t(15);
 }
 
+// Kernel variants: multi-scene when the parameters carry a scene table (tr_batch), else the
+// single-scene kernels.  Multi-scene grids cover the wave's capacity / the plan's largest batch,
+// because the per-batch counts live in device memory (the launches are replayed from a graph).
 cudaError_t launch_raygen(const Params& p, cudaStream_t s) {
-    const uint32_t n = p.batch.n_slots;
-    k_raygen<<<(n + 255) / 256, 256, 0, s>>>(p);
+    if (p.multi.scenes) {
+        k_raygen<true><<<(p.wave.capacity + 255) / 256, 256, 0, s>>>(p);
+    } else {
+        const uint32_t n = p.batch.n_slots;
+        k_raygen<false><<<(n + 255) / 256, 256, 0, s>>>(p);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s) {
-    k_extend<<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
+    if (p.multi.scenes) k_extend<true><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
+    else k_extend<false><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
 }
 cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s) {
     int dev = 0, grid = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&grid, cudaDevAttrMultiProcessorCount, dev);
-    grid *= 8;
-    const uint32_t need = (p.batch.n_slots + 255) / 256;
+    const bool multi = p.multi.scenes != nullptr;
+    const int block = multi && p.multi.shade_block ? (int)p.multi.shade_block : 256;
+    grid *= 8 * 256 / block;
+    const uint32_t need = ((multi ? p.wave.capacity : p.batch.n_slots) + block - 1) / block;
     if ((uint32_t)grid > need) grid = (int)need;
     if (grid < 1) grid = 1;
-    if (p.guide.vrec) k_shade<true><<<grid, 256, 0, s>>>(p, depth);
-    else k_shade<false><<<grid, 256, 0, s>>>(p, depth);
+    if (multi) {
+        if (p.guide.vrec) k_shade<true, true><<<grid, block, 0, s>>>(p, depth);
+        else k_shade<false, true><<<grid, block, 0, s>>>(p, depth);
+    } else {
+        if (p.guide.vrec) k_shade<true, false><<<grid, block, 0, s>>>(p, depth);
+        else k_shade<false, false><<<grid, block, 0, s>>>(p, depth);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s) {
-    k_shadow<<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
+    if (p.multi.scenes) k_shadow<true><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
+    else k_shadow<false><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
 }
 cudaError_t launch_splat(const Params& p, int G, cudaStream_t s) {
-    const size_t smem = splat_smem_bytes(p.film.T, G);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_splat, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(k_splat<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(k_splat<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         attr_set = true;
     }
-    const uint32_t blocks = (p.batch.npix + (uint32_t)G - 1) / (uint32_t)G;
-    k_splat<<<blocks, kSplatBlock, smem, s>>>(p, G);
+    if (p.multi.scenes) {
+        k_splat<true><<<p.multi.max_splat_blocks, kSplatBlock, p.multi.splat_smem, s>>>(p, 0);
+    } else {
+        const size_t smem = splat_smem_bytes(p.film.T, G);
+        const uint32_t blocks = (p.batch.npix + (uint32_t)G - 1) / (uint32_t)G;
+        k_splat<false><<<blocks, kSplatBlock, smem, s>>>(p, G);
+    }
+    return cudaGetLastError();
+}
+// last node of a multi-scene batch: the next replay renders the next batch descriptor
+__global__ void k_advance(uint32_t* cur) { *cur += 1u; }
+cudaError_t launch_advance(uint32_t* cur, cudaStream_t s) {
+    k_advance<<<1, 1, 0, s>>>(cur);
     return cudaGetLastError();
 }
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit, void* out,

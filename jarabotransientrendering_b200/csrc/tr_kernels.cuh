@@ -55,18 +55,30 @@ struct CameraDev {
     float pos[3], nv[3], uv[3], vv[3], fd;
 };
 
-// One wavefront batch: pixels [0, npix) of a pixel list (window rows, row-major) times
-// camera samples [s0, s0+ns) times incoming samples [0, ninc).
-// slot = ((pixel_local * ns) + s_local) * ninc + j
+// One contiguous slot range of one scene within a wavefront batch: pixels [0, npix) of a
+// pixel list (window rows, row-major) times camera samples [s0, s0+ns) times incoming samples
+// [0, ninc); slot = slot_begin + ((pixel_local * ns) + s_local) * ninc + j.
 struct Batch {
     uint32_t win_x0, win_y0, win_w;     // pixel list = window rows, row-major
-    uint32_t pix_begin;                 // first window-local pixel index of this batch
+    uint32_t pix_begin;                 // first window-local pixel index of this segment
     uint32_t npix;
     unsigned long long s0;
     uint32_t ns, ninc;
-    uint32_t n_slots;
+    uint32_t n_slots;                   // slots of this segment (= of the batch in single-scene mode)
+    uint32_t slot_begin;                // first slot (0 in single-scene mode)
+    uint32_t scene;                     // index into MultiDev::scenes (0 in single-scene mode)
+    uint32_t blk_begin;                 // first splat block of this segment
+    uint32_t splat_g;                   // pixels per splat block (film tile width)
 };
 
+// Multi-scene rendering (tr_batch): per-scene data and the batch descriptors live in device
+// memory; the kernels of one batch read descriptor *cur, so one captured CUDA graph replays
+// every batch (its last node advances *cur).
+constexpr int kMaxSegments = 16;
+struct BatchDesc {
+    uint32_t nseg, n_slots, n_blocks, max_depth;
+    Batch seg[kMaxSegments];
+};
 struct Wave {
     float4* ray_o;            // o.xyz, tfar (sampled free-flight distance or +inf)
     float4* ray_d;            // d.xyz, accumulated time
@@ -92,6 +104,25 @@ struct FilmDev {
     float exposure, offset;
 };
 
+struct SceneSlot {            // one scene of a multi-scene batch
+    SceneDev scene;
+    CameraDev cam;
+    FilmDev film;
+    unsigned long long seed;
+    uint32_t max_bounces, sqrt_spp, flags, pad;
+};
+
+struct MultiDev {
+    const SceneSlot* scenes;
+    const BatchDesc* batches;
+    uint32_t* cur;               // index of the batch being rendered
+    uint32_t nscenes;
+    // launch shapes (host side): grids cover the largest batch of the plan
+    uint32_t max_splat_blocks;
+    uint32_t splat_smem;         // bytes: largest film tile of the plan
+    uint32_t shade_block;        // threads per shade block (128 or 256)
+};
+
 struct Params {
     SceneDev scene;
     CameraDev cam;
@@ -104,7 +135,32 @@ struct Params {
     uint32_t bvh_depth;
     uint32_t flags;
     GuideWave guide;
+    MultiDev multi;              // used by the kMulti kernel variants only
 };
+
+// ---- per-slot view (device) ------------------------------------------------------------
+#ifdef __CUDACC__
+__device__ __forceinline__ const BatchDesc& cur_batch(const Params& p) { return p.multi.batches[*p.multi.cur]; }
+
+// segment holding `slot` (segments are contiguous and ordered by slot_begin)
+__device__ __forceinline__ const Batch& seg_of_slot(const BatchDesc& B, uint32_t slot) {
+    uint32_t lo = 0, hi = B.nseg;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (B.seg[mid].slot_begin <= slot) lo = mid; else hi = mid;
+    }
+    return B.seg[lo];
+}
+// segment owning splat block `blk`
+__device__ __forceinline__ const Batch& seg_of_block(const BatchDesc& B, uint32_t blk) {
+    uint32_t lo = 0, hi = B.nseg;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (B.seg[mid].blk_begin <= blk) lo = mid; else hi = mid;
+    }
+    return B.seg[lo];
+}
+#endif
 
 // counters layout (uint32): [0, 64) extend counts per depth, [64, 128) shadow counts per
 // depth, [128, 192) extend fetch cursors, [192, 256) shadow fetch cursors, [256, 320)
@@ -122,12 +178,13 @@ cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s);
 cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s);
+cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);
 // fused proposal inference + one-sample MIS direction sampling of the guided vertices of `depth`
 cudaError_t launch_guide(const Params& p, int depth, uint32_t* pool_state, cudaStream_t s);
 cudaError_t launch_train_gather(const Params& p, uint32_t* pool_state, cudaStream_t s);
-int trace_grid_size(int device, uint32_t bvh_depth);
+int trace_grid_size(int device, uint32_t bvh_depth, bool multi = false);
 size_t trace_smem_bytes(uint32_t bvh_depth);
 size_t splat_smem_bytes(uint32_t T, int pixels_per_cta);
 

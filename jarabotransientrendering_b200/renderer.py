@@ -151,6 +151,79 @@ class Context:
             pass
 
 
+class Batch:
+    """Several contexts rendered together in shared wavefront batches, one captured CUDA graph
+    replayed per batch (``tr_batch_*``).  Each context's film receives exactly the samples a
+    ``Context.render`` of the same sample range would give it."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.h.value for c in self.contexts])
+        h = C.c_void_p()
+        _abi.check(_abi.lib().tr_batch_create(arr, len(self.contexts), C.byref(h)))
+        self.h = h
+
+    def _arrays(self, begin, count):
+        n = len(self.contexts)
+        begin = [begin] * n if np.isscalar(begin) else list(begin)
+        count = [count] * n if np.isscalar(count) else list(count)
+        assert len(begin) == n and len(count) == n
+        return (C.c_uint64 * n)(*begin), (C.c_uint32 * n)(*count)
+
+    def render(self, sample_begin, sample_count):
+        """Adds samples [sample_begin[i], sample_begin[i] + sample_count[i]) of every pixel of
+        scene i (scalars apply to every scene)."""
+        b, c = self._arrays(sample_begin, sample_count)
+        _abi.check(_abi.lib().tr_batch_render(self.h, b, c))
+        return self
+
+    def config(self):
+        cfg = _abi.BatchConfig()
+        _abi.check(_abi.lib().tr_batch_get_config(self.h, C.byref(cfg)))
+        return {k: getattr(cfg, k) for k, _ in _abi.BatchConfig._fields_}
+
+    def set_config(self, **kw):
+        cur = self.config()
+        cur.update(kw)
+        cfg = _abi.BatchConfig(*[cur[k] for k, _ in _abi.BatchConfig._fields_])
+        _abi.check(_abi.lib().tr_batch_set_config(self.h, C.byref(cfg)))
+
+    def autotune(self, sample_begin, trial_samples):
+        """Runs the autotuner (trial renders add to the films); returns (best config, trials)."""
+        b, c = self._arrays(sample_begin, trial_samples)
+        best = _abi.BatchConfig()
+        trials = C.c_uint32()
+        _abi.check(_abi.lib().tr_batch_autotune(self.h, b, c, C.byref(best), C.byref(trials)))
+        return {k: getattr(best, k) for k, _ in _abi.BatchConfig._fields_}, trials.value
+
+    def set_guide(self, guide, mix_prob=0.5, learning_rate=1e-3, train_pool=262144):
+        _abi.check(_abi.lib().tr_batch_set_guide(self.h, guide.h if guide is not None else None, mix_prob,
+                                                 learning_rate, train_pool))
+        self._guide = guide
+
+    def stats(self):
+        s = _abi.Stats()
+        _abi.check(_abi.lib().tr_batch_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in _abi.Stats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.lib().tr_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Guide:
     """Learned directional proposal: MLP -> mixture of 8 von Mises-Fisher lobes (tr_guide_*)."""
 

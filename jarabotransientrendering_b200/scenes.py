@@ -409,6 +409,47 @@ def guided(seed=1, width=512, height=512, time_bins=2048, exposure=0.0025, max_b
                  exposure, 0.0, max_bounces, sqrt_spp, incoming_samples, None, seed)
 
 
+def batch_scene(index, seed=1):
+    """One scene of the seeded 16-scene batch workload: a displaced icosphere (subdivision
+    3..7, radius 0.2) in the Cornell room with its two boxes, every surface Lambertian with a
+    seeded albedo in [0.2, 0.8]; point light below the ceiling; resolution 64^2..512^2, 256..4096
+    time bins over the same 5.12 path-length units, 32..256 samples per pixel (non-square counts
+    as sqrt_spp^2 x 2 incoming paths), depth 8; odd scenes fill the room with a homogeneous
+    medium (sigma_s in [0.1, 1.0], sigma_a = sigma_s / 10, HG g in [-0.3, 0.6]).  Orthonormal
+    Lambertian frames, so the learned proposal can be attached."""
+    rng = np.random.default_rng(9000 + 131 * seed + index)
+    subdiv = 3 + index % 5
+    res = int(rng.choice((64, 128, 256, 512)))
+    bins = int(rng.choice((256, 512, 1024, 2048, 4096)))
+    # bound the film: at most 2^30 bins (6.4 GB FP64) per scene
+    while res * res * bins > (1 << 30):
+        bins //= 2
+    sqrt_spp, inc = ((4, 2), (8, 1), (8, 2), (16, 1))[int(rng.integers(0, 4))]     # 32, 64, 128, 256 spp
+    mats: List[Material] = []
+    meshes = _cornell_meshes(seed + index, mats)
+    for m in mats:
+        a = rng.uniform(0.2, 0.8)
+        m.kd = tuple(float(a * c / 0.75) for c in m.kd)
+    mats.append(Material(MAT_LAMBERTIAN, (float(rng.uniform(0.2, 0.8)),) * 3))
+    centre = (float(rng.uniform(0.35, 0.65)), 0.3, float(rng.uniform(0.3, 0.6)))
+    sv, st = displaced_icosphere(subdiv, centre, 0.2, 0.05, 3, 2.0, seed=2000 + 17 * seed + index)
+    meshes.append(Mesh("icosphere", sv, st, len(mats) - 1))
+    light = Light(LIGHT_POINT, (0.5, 0.99, 0.5), (1.0, 1.0, 1.0))
+    med = None
+    if index % 2 == 1:
+        sig_s = float(rng.uniform(0.1, 1.0))
+        med = Medium((sig_s / 10,) * 3, (sig_s,) * 3, float(rng.uniform(-0.3, 0.6)))
+    sc = Scene(f"batch{index:02d}", meshes, mats, [light], _default_camera(), res, res, bins, 5.12 / bins, 0.0, 8,
+               sqrt_spp, inc, med, seed + index)
+    sc.flags = FLAG_ORTHONORMAL_FRAME
+    return sc
+
+
+def batch_scenes(seed=1, n=16):
+    """The seeded multi-scene workload (see ``batch_scene``)."""
+    return [batch_scene(i, seed) for i in range(n)]
+
+
 WORKLOADS = {"cornell": cornell, "icosphere": icosphere, "medium": medium, "guided": guided}
 
 
