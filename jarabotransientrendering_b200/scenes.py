@@ -131,6 +131,8 @@ class Scene:
     medium: Optional[Medium] = None
     seed: int = 1
     flags: int = 0            # FLAG_ORTHONORMAL_FRAME: Lambertian sampling in an orthonormal frame
+    camera_unwarp: int = 0    # bin by path time minus the camera-to-first-surface distance
+    bounce_films: int = 0     # N > 0: per-bounce streak films (multibounce streak film)
 
     # ---- flattened arrays (what the C ABI takes) -------------------------
     def flatten(self):

@@ -46,7 +46,8 @@ class CameraS(C.Structure):
 
 class FilmS(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("time_bins", C.c_uint32),
-                ("exposure", C.c_float), ("offset", C.c_float)]
+                ("exposure", C.c_float), ("offset", C.c_float), ("camera_unwarp", C.c_uint32),
+                ("bounce_films", C.c_uint32)]
 
 
 class IntegratorS(C.Structure):
@@ -86,6 +87,9 @@ def lib():
         L.orc_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p,
                                 C.c_void_p]
         L.orc_trace_moller.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_render_bounces.restype = C.c_int
+        L.orc_render_bounces.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                         C.c_uint32, C.c_int] + [C.c_void_p] * 7
         L.orc_render.restype = C.c_int
         L.orc_render.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                  C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -143,7 +147,8 @@ class Oracle:
                    mats, len(scene.materials), lights, len(scene.lights), med)
         pos, nv, uv, vv, fd = scene.camera.basis()
         cam = CameraS(f3(*pos), f3(*nv), f3(*uv), f3(*vv), float(fd))
-        film = FilmS(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset)
+        film = FilmS(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset,
+                     int(getattr(scene, "camera_unwarp", 0)), int(getattr(scene, "bounce_films", 0)))
         integ = IntegratorS(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, scene.flags, scene.seed)
         h = C.c_void_p()
         rc = lib().orc_create(C.byref(s), C.byref(cam), C.byref(film), C.byref(integ), C.byref(h))
@@ -184,25 +189,34 @@ class Oracle:
         return out
 
     def render(self, sample_begin=0, sample_count=None, window=None, nthreads=1,
-               streak=True, steady=True, weight=True):
+               streak=True, steady=True, weight=True, bounces=False):
+        """Adds the camera samples into fresh full-frame films.  With bounces=True (the scene's
+        film has bounce_films = N > 0) also returns the per-bounce films "bstreak"
+        [N][H][W][T][3], "bsteady" [N][H][W][3], "bweight" [N][H][W]."""
         sc = self.scene
         if sample_count is None:
             sample_count = sc.spp
         x0, y0, x1, y1 = window if window is not None else (0, 0, sc.width, sc.height)
         H, W, T = sc.height, sc.width, sc.time_bins
+        NB = int(getattr(sc, "bounce_films", 0)) if bounces else 0
         st = np.zeros((H, W, T, 3), np.float64) if streak else None
         sd = np.zeros((H, W, 3), np.float64) if steady else None
         wt = np.zeros((H, W), np.float64) if weight else None
+        bst = np.zeros((NB, H, W, T, 3), np.float64) if NB else None
+        bsd = np.zeros((NB, H, W, 3), np.float64) if NB else None
+        bwt = np.zeros((NB, H, W), np.float64) if NB else None
         stats = np.zeros(8, np.uint64)
-        rc = lib().orc_render(self.h, x0, y0, x1, y1, sample_begin, sample_count, nthreads,
-                              st.ctypes.data if st is not None else None,
-                              sd.ctypes.data if sd is not None else None,
-                              wt.ctypes.data if wt is not None else None, stats.ctypes.data)
+        ptr = lambda a: a.ctypes.data if a is not None else None
+        rc = lib().orc_render_bounces(self.h, x0, y0, x1, y1, sample_begin, sample_count, nthreads,
+                                      ptr(st), ptr(sd), ptr(wt), ptr(bst), ptr(bsd), ptr(bwt), stats.ctypes.data)
         if rc != 0:
             raise ValueError("orc_render failed")
-        return {"streak": st, "steady": sd, "weight": wt,
-                "stats": dict(zip(["paths", "closest_rays", "shadow_rays", "splats", "closest_nodes",
-                                   "closest_tris", "shadow_nodes", "shadow_tris"], map(int, stats)))}
+        out = {"streak": st, "steady": sd, "weight": wt,
+               "stats": dict(zip(["paths", "closest_rays", "shadow_rays", "splats", "closest_nodes",
+                                  "closest_tris", "shadow_nodes", "shadow_tris"], map(int, stats)))}
+        if NB:
+            out.update(bstreak=bst, bsteady=bsd, bweight=bwt)
+        return out
 
     def path_records(self, x, y, s, j=0, cap=256):
         bins = np.zeros(cap, np.uint32)

@@ -506,7 +506,9 @@ void orc_trace_moller(const orc_ctx* x, const float* rays, uint32_t n, orc_hit* 
 /* ------------------------------------------------------------------------------------------
  * The transient path tracer.
  * ---------------------------------------------------------------------------------------- */
-typedef struct { uint32_t bin; float L[3]; } srec;
+/* bin = BIN_OUTSIDE for a sample outside the time window (kept only for bounce films) */
+#define BIN_OUTSIDE 0xffffffu
+typedef struct { uint32_t bin; uint32_t depth; float L[3]; } srec;
 
 typedef struct {
     uint64_t closest, shadow, splats;
@@ -634,6 +636,11 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
     float g = x->med.g;
     float total_time = (float)F->time_bins * F->exposure + F->offset;
     uint32_t maxb = x->integ.max_bounces;
+    const int unwarp = F->camera_unwarp != 0;
+    const int bounce_films = F->bounce_films != 0;
+    /* World::Li's camera-ray record distance (World.h:749-766): the closest surface along the
+     * camera ray, FLT_MAX when there is none (Ray.h:74-84) */
+    float cam_dist = FLT_MAX;
     int nrec = 0;
 
     v3 f = mk(1.0f, 1.0f, 1.0f);
@@ -643,12 +650,15 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
 
     for (uint32_t depth = 0; depth < maxb; ++depth) {
         wray r;
-        wray_setup(&r, org, dir, SIGMA_VIS, medium ? dsamp : INFINITY);
+        /* with camera unwarp the camera ray is traced to infinity (its surface distance is the
+         * unwarp offset); surface vs medium below is decided by h.t < dsamp either way */
+        wray_setup(&r, org, dir, SIGMA_VIS, (medium && !(unwarp && depth == 0)) ? dsamp : INFINITY);
         orc_hit h;
         st->closest++;
         uint32_t cv = 0, ct = 0;
         int hit = trace1(x, &r, 0, &h, &cv, &ct);
         st->c_nodes += cv; st->c_tris += ct;
+        if (depth == 0 && hit) cam_dist = h.t;
         int surface = hit && (!medium || h.t < dsamp);
         if (!medium && !hit) break;
         float dist, pd;
@@ -724,9 +734,15 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
                                (f.y * (fe.y * (irr.y * att.y))) * scale,
                                (f.z * (fe.z * (irr.z * att.z))) * scale};
                 float tt = time + dl;
-                float ps = (tt - F->offset) / F->exposure;
-                if (ps < (float)F->time_bins && ps >= 0.0f && is_finite3(Lc) &&
-                    (Lc[0] != 0.0f || Lc[1] != 0.0f || Lc[2] != 0.0f)) {
+                float tc = unwarp ? tt - cam_dist : tt;          /* StreakCameraFilm.h:167 */
+                float ps = (tc - F->offset) / F->exposure;
+                int inside = ps < (float)F->time_bins && ps >= 0.0f;
+                int finite = is_finite3(Lc);
+                int useful = inside && finite && (Lc[0] != 0.0f || Lc[1] != 0.0f || Lc[2] != 0.0f);
+                /* bounce films count every visible light connection (the sample exists in the
+                 * reference whatever its time or radiance; non-finite radiance becomes 0,
+                 * TransientRenderer.h:165-169); otherwise only useful samples are traced */
+                if (useful || bounce_films) {
                     wray sr;
                     wray_setup(&sr, lp, ld, SIGMA_VIS, dl - SIGMA_VIS);
                     orc_hit sh;
@@ -735,8 +751,9 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
                     int occluded = trace1(x, &sr, 1, &sh, &sv, &stt2);
                     st->s_nodes += sv; st->s_tris += stt2;
                     if (!occluded) {
-                        rec[nrec].bin = (uint32_t)floorf(ps);
-                        rec[nrec].L[0] = Lc[0]; rec[nrec].L[1] = Lc[1]; rec[nrec].L[2] = Lc[2];
+                        rec[nrec].bin = inside ? (uint32_t)floorf(ps) : BIN_OUTSIDE;
+                        rec[nrec].depth = depth;
+                        for (int c = 0; c < 3; ++c) rec[nrec].L[c] = finite ? Lc[c] : 0.0f;
                         nrec++;
                         st->splats++;
                     }
@@ -857,6 +874,7 @@ int orc_path_records(const orc_ctx* x, uint32_t px, uint32_t py, uint64_t s, uin
 typedef struct {
     const orc_ctx* x; uint32_t x0, x1, y0, y1; uint64_t s0; uint32_t ns;
     double *streak, *steady, *weight;
+    double *bstreak, *bsteady, *bweight;
     uint32_t row_begin, row_step;
     uint64_t paths; pstats st;
 } job;
@@ -866,6 +884,8 @@ static void* render_rows(void* arg) {
     const orc_ctx* x = J->x;
     const orc_film* F = &x->film;
     uint32_t T = F->time_bins, W = F->width;
+    const uint32_t NB = F->bounce_films;
+    const size_t npix = (size_t)F->width * F->height;
     uint32_t ninc = x->integ.incoming_samples;
     float inv_inc = 1.0f / (float)ninc;
     srec rec[256];
@@ -876,18 +896,31 @@ static void* render_rows(void* arg) {
                 v3 o, d;
                 camera_ray(x, px, y, s, &o, &d);
                 if (J->weight) J->weight[pixel] += 1.0;
+                uint64_t present = 0;          /* bounce films with a sample of this camera sample */
                 for (uint32_t j = 0; j < ninc; ++j) {
                     pcg r;
                     path_rng(x, &r, pixel, s, j);
                     int n = trace_path(x, o, d, &r, inv_inc, rec, &J->st);
                     J->paths++;
                     for (int i = 0; i < n; ++i) {
+                        const int inside = rec[i].bin != BIN_OUTSIDE;
                         for (int c = 0; c < 3; ++c) {
-                            if (J->streak) J->streak[((size_t)pixel * T + rec[i].bin) * 3 + c] += (double)rec[i].L[c];
-                            if (J->steady) J->steady[(size_t)pixel * 3 + c] += (double)rec[i].L[c];
+                            if (J->streak && inside) J->streak[((size_t)pixel * T + rec[i].bin) * 3 + c] += (double)rec[i].L[c];
+                            if (J->steady && (inside || NB)) J->steady[(size_t)pixel * 3 + c] += (double)rec[i].L[c];
+                        }
+                        if (NB) {
+                            const uint32_t b = rec[i].depth < NB ? rec[i].depth : NB - 1;
+                            present |= 1ull << b;
+                            for (int c = 0; c < 3 && inside; ++c) {
+                                if (J->bstreak)
+                                    J->bstreak[(((size_t)b * npix + pixel) * T + rec[i].bin) * 3 + c] += (double)rec[i].L[c];
+                                if (J->bsteady) J->bsteady[((size_t)b * npix + pixel) * 3 + c] += (double)rec[i].L[c];
+                            }
                         }
                     }
                 }
+                for (uint32_t b = 0; b < NB && J->bweight; ++b)
+                    if (present >> b & 1ull) J->bweight[(size_t)b * npix + pixel] += 1.0;
             }
         }
     }
@@ -897,6 +930,15 @@ static void* render_rows(void* arg) {
 int orc_render(const orc_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
                uint64_t sample_begin, uint32_t sample_count, int nthreads,
                double* streak, double* steady, double* weight, uint64_t* stats) {
+    return orc_render_bounces(x, x0, y0, x1, y1, sample_begin, sample_count, nthreads, streak, steady, weight,
+                              NULL, NULL, NULL, stats);
+}
+
+int orc_render_bounces(const orc_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                       uint64_t sample_begin, uint32_t sample_count, int nthreads,
+                       double* streak, double* steady, double* weight,
+                       double* bstreak, double* bsteady, double* bweight, uint64_t* stats) {
+    if (x->film.bounce_films > 64) return 1;
     if (x1 > x->film.width || y1 > x->film.height || x0 > x1 || y0 > y1) return 1;
     if (x->integ.max_bounces > 255) return 1;
     if (nthreads < 1) nthreads = 1;
@@ -907,6 +949,7 @@ int orc_render(const orc_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t
         J[i].x = x; J[i].x0 = x0; J[i].x1 = x1; J[i].y0 = y0; J[i].y1 = y1;
         J[i].s0 = sample_begin; J[i].ns = sample_count;
         J[i].streak = streak; J[i].steady = steady; J[i].weight = weight;
+        J[i].bstreak = bstreak; J[i].bsteady = bsteady; J[i].bweight = bweight;
         J[i].row_begin = (uint32_t)i; J[i].row_step = (uint32_t)nthreads;
         J[i].paths = 0; memset(&J[i].st, 0, sizeof(pstats));
     }

@@ -56,7 +56,11 @@ typedef struct orc_scene {
     orc_medium medium;
 } orc_scene;
 typedef struct orc_camera { float position[3]; float nv[3]; float uv[3]; float vv[3]; float focal_distance; } orc_camera;
-typedef struct orc_film { uint32_t width, height, time_bins; float exposure; float offset; } orc_film;
+typedef struct orc_film {
+    uint32_t width, height, time_bins; float exposure; float offset;
+    uint32_t camera_unwarp;   /* bin by path time minus the camera-to-first-surface distance */
+    uint32_t bounce_films;    /* N > 0: per-bounce streak films (MultibounceStreakFilm)       */
+} orc_film;
 typedef struct orc_integrator { uint32_t max_bounces, sqrt_spp, incoming_samples, flags; uint64_t seed; } orc_integrator;
 #define ORC_FLAG_ORTHONORMAL_FRAME 1u
 typedef struct orc_hit { float t; uint32_t prim_id; float u, v; } orc_hit;
@@ -89,6 +93,18 @@ void orc_trace_moller(const orc_ctx* ctx, const float* rays, uint32_t n, orc_hit
 int orc_render(const orc_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
                uint64_t sample_begin, uint32_t sample_count, int nthreads,
                double* streak, double* steady, double* weight, uint64_t* stats);
+
+/* As orc_render, plus the per-bounce films of a film with bounce_films = N > 0 (any may be
+ * NULL): bstreak [N][H][W][T][3], bsteady [N][H][W][3], bweight [N][H][W], following
+ * MultibounceStreakFilm::add_samples (src/Film/MultibounceStreakCameraFilm.h:151-171): a
+ * radiance sample of bounce b goes to film min(b, N-1); bounce film b's weight counts the camera
+ * samples with at least one sample of that film (inside the time window or not).  With N > 0
+ * the main steady image is the base Film's (Film.h:263-284): every sample, also those outside
+ * the time window.                                                                              */
+int orc_render_bounces(const orc_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                       uint64_t sample_begin, uint32_t sample_count, int nthreads,
+                       double* streak, double* steady, double* weight,
+                       double* bstreak, double* bsteady, double* bweight, uint64_t* stats);
 
 /* One path's splat records, for per-path comparisons: returns the number of records
  * (<= cap) of path (pixel x, y, camera sample s, incoming sample j). */
