@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define TR_ABI_VERSION 1
+#define TR_ABI_VERSION 2
 
 typedef enum tr_status {
     TR_OK = 0,
@@ -102,13 +102,22 @@ typedef struct tr_camera {
 } tr_camera;
 
 /* Streak film (src/Film/StreakCameraFilm.h:91-121): width x height pixels, time_bins bins of
- * `exposure` path-length units starting at `offset`. */
+ * `exposure` path-length units starting at `offset`.
+ * camera_unwarp ("-camera-unwarp"): bin every sample by its path time minus the distance from
+ *   the camera to the first surface along its camera ray (StreakCameraFilm.h:167, World.h:749-766).
+ * bounce_films ("-multibounce-streak N"): N > 0 adds N per-bounce streak films as
+ *   MultibounceStreakFilm does (src/Film/MultibounceStreakCameraFilm.h:151-171): a sample of
+ *   bounce b goes to film min(b, N-1); film b's weight counts the camera samples with at least
+ *   one sample of that film (inside the time window or not); the context's steady image is
+ *   then the base Film's, the sum of all samples (Film.h:263-284).  N <= 32.              */
 typedef struct tr_film {
     uint32_t width;
     uint32_t height;
     uint32_t time_bins;
     float exposure;
     float offset;
+    uint32_t camera_unwarp;
+    uint32_t bounce_films;
 } tr_film;
 
 /* Unidirectional path tracing with next-event estimation, the only mode the reference CLI runs
@@ -196,9 +205,14 @@ tr_status tr_get_film(tr_ctx* ctx, double* streak, double* steady, double* weigh
  * caller's own pending work on the destination must be finished first.                      */
 tr_status tr_get_film_device(tr_ctx* ctx, double* d_streak, double* d_steady, double* d_weight);
 
+/* Per-bounce film `bounce` (< bounce_films) of the context, layouts as tr_get_film.           */
+tr_status tr_get_film_bounce(tr_ctx* ctx, uint32_t bounce, double* streak, double* steady, double* weight);
+
 /* Writes the averaged film the way the reference does: one RGBE .hdr streak image per
  * scanline "<name>_%04d.hdr" (time_bins x width) and the steady image "<name>.hdr"
- * (StreakCameraFilm.h:356-437, Film.h:357-471, ImageIO.h:146-193).                           */
+ * (StreakCameraFilm.h:356-437, Film.h:357-471, ImageIO.h:146-193).  With bounce films, the
+ * per-scanline streak images of film b are "<name>_b%02d_%04d.hdr" (b + 1, as
+ * MultibounceStreakFilm names them) and "<name>.hdr" is the base steady image.             */
 tr_status tr_write_film(tr_ctx* ctx, const char* name);
 
 /* Closest-hit (any_hit = 0) or occlusion (any_hit = 1) queries for n host rays.
@@ -216,7 +230,7 @@ tr_status tr_trace_rays_device(tr_ctx* ctx, const float* d_rays, uint32_t n, int
  * cannot afford cudaMalloc's implicit device-wide synchronisation in the middle of a frame.
  * tr_render may grow its path buffers with cudaMalloc; this entry
  * point instead keeps the per-path state of the wavefront in one fixed array compiled into
- * the library (24 MiB per GPU that loads the library, held until the process exits).
+ * the library (24.3 MiB per GPU that loads the library, held until the process exits).
  * It adds camera samples [sample_begin, sample_begin + sample_count) of the pixel window
  * [x0,x1) x [y0,y1) to the context's film, exactly as tr_render_region does, asynchronously
  * on `stream` (cudaStream_t as void*, NULL = the context's stream).
@@ -276,7 +290,8 @@ tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
  * for every batch; the kernels read the batch being rendered from device memory.  Each scene's
  * film receives exactly the samples it would receive from tr_render on its own context (same
  * per-path random streams).  The contexts must live on one device, outlive the batch, and not
- * be rendered through their own calls while a batch call runs. */
+ * be rendered through their own calls while a batch call runs; contexts with bounce films
+ * are rendered with tr_render (TR_ERR_NOT_SUPPORTED here). */
 typedef struct tr_batch tr_batch;
 
 typedef struct tr_batch_config {

@@ -6,11 +6,11 @@ include/transient_b200.h; this package is its host-side binding.
 """
 from . import scenes
 from .renderer import (Context, Batch, Guide, World, Lambertian, GGX, PointLightSource, RectangularAreaLightSource,
-                       HenyeyGreenstein, HomogeneousMedium, PinholeCamera, StreakCameraFilm,
+                       HenyeyGreenstein, HomogeneousMedium, PinholeCamera, StreakCameraFilm, MultibounceStreakFilm,
                        StratifiedSampler, BidirectionalPathTracing, TransientRenderer, HIT_DTYPE, INVALID_ID)
 from ._abi import TransientError, LIB_PATH
 
 __all__ = ["scenes", "Context", "Batch", "Guide", "World", "Lambertian", "GGX", "PointLightSource", "RectangularAreaLightSource",
-           "HenyeyGreenstein", "HomogeneousMedium", "PinholeCamera", "StreakCameraFilm", "StratifiedSampler",
+           "HenyeyGreenstein", "HomogeneousMedium", "PinholeCamera", "StreakCameraFilm", "MultibounceStreakFilm", "StratifiedSampler",
            "BidirectionalPathTracing", "TransientRenderer", "TransientError", "HIT_DTYPE", "INVALID_ID",
            "LIB_PATH"]

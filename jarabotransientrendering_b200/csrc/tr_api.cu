@@ -79,6 +79,8 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     if (!(f->exposure > 0.0f) || !std::isfinite(f->offset))
         return fail(TR_ERR_INVALID_ARGUMENT, "film exposure must be > 0");
     if ((uint64_t)f->width * f->height >= (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "film too large");
+    if (f->camera_unwarp > 1) return fail(TR_ERR_INVALID_ARGUMENT, "camera_unwarp must be 0 or 1");
+    if (f->bounce_films > 32) return fail(TR_ERR_INVALID_ARGUMENT, "at most 32 bounce films");
     if (trk::splat_smem_bytes(f->time_bins, 1) > 220 * 1024)
         return fail(TR_ERR_NOT_SUPPORTED, "time_bins too large for one shared-memory pixel tile");
     if (it->sqrt_spp == 0 || it->incoming_samples == 0)
@@ -121,6 +123,8 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.sh_L = x->alloc<float4>(capacity);
     w.rec = x->alloc<float4>((size_t)capacity * R);
     w.rec_n = x->alloc<uint8_t>(capacity);
+    drop(w.cam_dist);
+    w.cam_dist = x->alloc<float>(capacity);
     if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = x->alloc<unsigned long long>(8);
@@ -158,6 +162,9 @@ trk::Params make_params(tr_ctx* x) {
     }
     p.cam.fd = x->cam.focal_distance;
     p.film.streak = x->d_streak; p.film.steady = x->d_steady; p.film.weight = x->d_weight;
+    p.film.unwarp = x->film.camera_unwarp;
+    p.film.nbounce = x->film.bounce_films;
+    p.film.bstreak = x->d_bstreak; p.film.bsteady = x->d_bsteady; p.film.bweight = x->d_bweight;
     p.film.W = x->film.width; p.film.H = x->film.height; p.film.T = x->film.time_bins;
     p.film.exposure = x->film.exposure; p.film.offset = x->film.offset;
     p.wave = x->wave;
@@ -253,6 +260,12 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 launches += 2;
             }
             timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm); });
+            for (uint32_t b = 0; b < x->film.bounce_films; ++b)
+                timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm, (int)b); });
+            if (x->film.bounce_films) {
+                timed(4, [&] { return trk::launch_bounce_weights(p, strm); });
+                launches += 1ull + x->film.bounce_films;
+            }
             launches += 2 + 3ull * x->integ.max_bounces;
             ext_l += x->integ.max_bounces;
             sh_l += x->integ.max_bounces;
@@ -424,7 +437,8 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         const size_t nstreak = (size_t)f->width * f->height * f->time_bins * 3u;
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        if (nstreak * sizeof(double) + ((size_t)2 << 30) > free_b) {
+        const size_t nb = f->bounce_films;
+        if ((1 + nb) * nstreak * sizeof(double) + ((size_t)2 << 30) > free_b) {
             x->release();
             delete x;
             return fail(TR_ERR_OUT_OF_MEMORY, "streak film of " + std::to_string(nstreak * 8 >> 20) +
@@ -436,6 +450,15 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         TR_CUDA(cudaMemsetAsync(x->d_streak, 0, nstreak * sizeof(double), x->stream));
         TR_CUDA(cudaMemsetAsync(x->d_steady, 0, (size_t)f->width * f->height * 3u * sizeof(double), x->stream));
         TR_CUDA(cudaMemsetAsync(x->d_weight, 0, (size_t)f->width * f->height * sizeof(double), x->stream));
+        if (nb) {
+            const size_t npix = (size_t)f->width * f->height;
+            x->d_bstreak = x->alloc<double>(nb * nstreak);
+            x->d_bsteady = x->alloc<double>(nb * npix * 3u);
+            x->d_bweight = x->alloc<double>(nb * npix);
+            TR_CUDA(cudaMemsetAsync(x->d_bstreak, 0, nb * nstreak * sizeof(double), x->stream));
+            TR_CUDA(cudaMemsetAsync(x->d_bsteady, 0, nb * npix * 3u * sizeof(double), x->stream));
+            TR_CUDA(cudaMemsetAsync(x->d_bweight, 0, nb * npix * sizeof(double), x->stream));
+        }
 
         x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);
         int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
@@ -483,6 +506,11 @@ tr_status tr_clear_film(tr_ctx* x) {
         TR_CUDA(cudaMemsetAsync(x->d_streak, 0, npix * x->film.time_bins * 3u * sizeof(double), x->s()));
         TR_CUDA(cudaMemsetAsync(x->d_steady, 0, npix * 3u * sizeof(double), x->s()));
         TR_CUDA(cudaMemsetAsync(x->d_weight, 0, npix * sizeof(double), x->s()));
+        if (const size_t nb = x->film.bounce_films) {
+            TR_CUDA(cudaMemsetAsync(x->d_bstreak, 0, nb * npix * x->film.time_bins * 3u * sizeof(double), x->s()));
+            TR_CUDA(cudaMemsetAsync(x->d_bsteady, 0, nb * npix * 3u * sizeof(double), x->s()));
+            TR_CUDA(cudaMemsetAsync(x->d_bweight, 0, nb * npix * sizeof(double), x->s()));
+        }
         TR_CUDA(cudaStreamSynchronize(x->s()));
         x->stats.camera_samples = 0;
         x->stats.paths = 0;
@@ -519,21 +547,51 @@ tr_status tr_get_film_device(tr_ctx* x, double* streak, double* steady, double* 
     return copy_film(x, streak, steady, weight, cudaMemcpyDeviceToDevice);
 }
 
+tr_status tr_get_film_bounce(tr_ctx* x, uint32_t b, double* streak, double* steady, double* weight) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    if (b >= x->film.bounce_films) return fail(TR_ERR_INVALID_ARGUMENT, "bounce film index out of range");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        cudaStream_t s = x->s();
+        const size_t npix = (size_t)x->film.width * x->film.height;
+        const size_t ns = npix * x->film.time_bins * 3u;
+        if (streak) TR_CUDA(cudaMemcpyAsync(streak, x->d_bstreak + b * ns, ns * sizeof(double), cudaMemcpyDefault, s));
+        if (steady) TR_CUDA(cudaMemcpyAsync(steady, x->d_bsteady + b * npix * 3u, npix * 3u * sizeof(double), cudaMemcpyDefault, s));
+        if (weight) TR_CUDA(cudaMemcpyAsync(weight, x->d_bweight + b * npix, npix * sizeof(double), cudaMemcpyDefault, s));
+        TR_CUDA(cudaStreamSynchronize(s));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
 tr_status tr_write_film(tr_ctx* x, const char* name) {
     if (!x || !name) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
     const size_t npix = (size_t)x->film.width * x->film.height;
+    const uint32_t nb = x->film.bounce_films;
     std::vector<double> streak, steady(npix * 3), weight(npix);
     try {
         streak.resize(npix * x->film.time_bins * 3u);
     } catch (const std::bad_alloc&) {
         return fail(TR_ERR_OUT_OF_MEMORY, "host film buffer");
     }
-    tr_status st = tr_get_film(x, streak.data(), steady.data(), weight.data());
-    if (st != TR_OK) return st;
     std::string err;
-    if (!trio::write_streak_film(name, x->film.width, x->film.height, x->film.time_bins, streak.data(),
+    // with bounce films: the base steady image (Film::write) and the per-bounce streak images
+    // named as MultibounceStreakFilm::set_name does (MultibounceStreakCameraFilm.h:130-141)
+    tr_status st = tr_get_film(x, nb ? nullptr : streak.data(), steady.data(), weight.data());
+    if (st != TR_OK) return st;
+    if (!trio::write_streak_film(name, x->film.width, x->film.height, x->film.time_bins, nb ? nullptr : streak.data(),
                                  steady.data(), weight.data(), &err))
         return fail(TR_ERR_IO, err);
+    for (uint32_t b = 0; b < nb; ++b) {
+        st = tr_get_film_bounce(x, b, streak.data(), nullptr, weight.data());
+        if (st != TR_OK) return st;
+        char bname[4096];
+        std::snprintf(bname, sizeof(bname), "%s_b%02u", name, b + 1);
+        if (!trio::write_streak_film(bname, x->film.width, x->film.height, x->film.time_bins, streak.data(), nullptr,
+                                     weight.data(), &err))
+            return fail(TR_ERR_IO, err);
+    }
     return TR_OK;
 }
 
@@ -604,7 +662,8 @@ constexpr size_t kNaBytes = 7 * kNaF4                                           
                           + na_align(sizeof(float4) * kNaSlots * TR_NOALLOC_MAX_BOUNCES)  // records
                           + na_align(kNaSlots)                                    // records per slot
                           + na_align(sizeof(uint32_t) * trk::kCounters)           // queue counters
-                          + na_align(sizeof(unsigned long long) * 8);             // ray / splat counts
+                          + na_align(sizeof(unsigned long long) * 8)              // ray / splat counts
+                          + na_align(sizeof(float) * kNaSlots);                   // camera distances
 
 // The scratch itself.  Its name is only a host-side handle: host code must use the device
 // address from cudaGetSymbolAddress, never &g_noalloc_scratch.
@@ -672,6 +731,7 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
         w.rec_n = take(kNaSlots);
         w.counters = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * trk::kCounters));
         w.stats = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 8));
+        w.cam_dist = reinterpret_cast<float*>(take(sizeof(float) * kNaSlots));
         w.capacity = (uint32_t)kNaSlots;
         // what the kernels expect to start at zero: queue counters / fetch cursors and the
         // ray counters (records-per-slot are reset by the ray generation kernel)
@@ -688,6 +748,8 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
             TR_CUDA(trk::launch_shadow(p, (int)d, x->trace_grid, strm));
         }
         TR_CUDA(trk::launch_splat(p, x->splat_g, strm));
+        for (uint32_t b = 0; b < x->film.bounce_films; ++b) TR_CUDA(trk::launch_splat(p, x->splat_g, strm, (int)b));
+        if (x->film.bounce_films) TR_CUDA(trk::launch_bounce_weights(p, strm));
         x->stats.paths += paths;
         x->stats.camera_samples += npix * ns;
     } catch (const CudaError& e) {

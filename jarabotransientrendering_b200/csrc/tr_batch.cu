@@ -168,6 +168,8 @@ void ensure_batch_wave(tr_batch* b, uint32_t capacity) {
     w.sh_L = b->alloc<float4>(capacity);
     w.rec = b->alloc<float4>((size_t)capacity * std::max<uint32_t>(1u, b->max_bounces));
     w.rec_n = b->alloc<uint8_t>(capacity);
+    b->drop(w.cam_dist);
+    w.cam_dist = b->alloc<float>(capacity);
     if (!w.counters) w.counters = b->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = b->alloc<unsigned long long>(8);
@@ -343,6 +345,8 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         if (!contexts[i]) return fail(TR_ERR_INVALID_ARGUMENT, "context " + std::to_string(i) + " is null");
         if (contexts[i]->device != contexts[0]->device)
             return fail(TR_ERR_INVALID_ARGUMENT, "all contexts of a batch must be on one device");
+        if (contexts[i]->film.bounce_films)
+            return fail(TR_ERR_NOT_SUPPORTED, "contexts with bounce films render through tr_render, not in a batch");
     }
     tr_batch* b = new (std::nothrow) tr_batch();
     if (!b) return fail(TR_ERR_OUT_OF_MEMORY, "host allocation");

@@ -49,7 +49,7 @@ bool write_streak_film(const char* name, uint32_t W, uint32_t H, uint32_t T, con
     std::vector<float> img((size_t)W * T * 3);
     std::vector<float> tr;
     char buf[4096];
-    for (uint32_t y = 0; y < H; ++y) {
+    for (uint32_t y = 0; streak && y < H; ++y) {
         for (uint32_t x = 0; x < W; ++x) {
             const double w = weight[(size_t)y * W + x];
             const double* src = streak + (((size_t)y * W + x) * T) * 3;
@@ -69,6 +69,7 @@ bool write_streak_film(const char* name, uint32_t W, uint32_t H, uint32_t T, con
         }
         if (!ok) return false;
     }
+    if (!steady) return true;
     std::vector<float> st((size_t)W * H * 3);
     for (size_t i = 0; i < (size_t)W * H; ++i)
         for (int c = 0; c < 3; ++c) st[i * 3 + c] = avg_nan0(steady[i * 3 + c], weight[i]);

@@ -14,7 +14,8 @@ bool write_hdr(const std::string& path, uint32_t width, uint32_t height, const f
 // Writes what StreakCameraFilm::write produces (src/Film/StreakCameraFilm.h:233-242,356-437 and
 // Film::average_and_write, src/Film/Film.h:357-471): for each scanline y an image
 // "<name>_%04d.hdr" of width T (time) and height W (x), each row divided by that pixel's weight
-// (NaN -> 0), transposed when T < 8; and the steady image "<name>.hdr" (W x H).
+// (NaN -> 0), transposed when T < 8; and the steady image "<name>.hdr" (W x H).  A null
+// streak or steady skips that part.
 bool write_streak_film(const char* name, uint32_t W, uint32_t H, uint32_t T, const double* streak,
                        const double* steady, const double* weight, std::string* err);
 

@@ -120,6 +120,9 @@ struct tr_ctx {
     double* d_streak = nullptr;
     double* d_steady = nullptr;
     double* d_weight = nullptr;
+    double* d_bstreak = nullptr;            // per-bounce films (tr_film.bounce_films > 0)
+    double* d_bsteady = nullptr;
+    double* d_bweight = nullptr;
 
     // wavefront state
     trk::Wave wave{};

@@ -15,6 +15,8 @@
 #include "tr_device.cuh"
 #include "tr_kernels.cuh"
 
+#include <algorithm>
+
 namespace trk {
 using namespace trd;
 
@@ -184,13 +186,21 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(const _
         if (idx < n) {
             const uint32_t slot = depth == 0 ? idx : q[idx];
             const SceneDev* sc = &p.scene;
-            if constexpr (kMulti) sc = &p.multi.scenes[seg_of_slot(cur_batch(p), slot).scene].scene;
+            const FilmDev* film = &p.film;
+            if constexpr (kMulti) {
+                const SceneSlot& S = p.multi.scenes[seg_of_slot(cur_batch(p), slot).scene];
+                sc = &S.scene;
+                film = &S.film;
+            }
             const float4 o = p.wave.ray_o[slot];
             const float4 d = p.wave.ray_d[slot];
             WRay r;
             wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
             float t, u, v;
-            const uint32_t id = traverse<false>(*sc, r, o.w, t, u, v, stack + threadIdx.x, kTraceBlock);
+            // camera unwarp needs the camera ray's closest surface at any distance; shade still
+            // decides surface vs medium event by comparing with the sampled distance (o.w)
+            const float tfar = depth == 0 && film->unwarp ? __int_as_float(0x7f800000) : o.w;
+            const uint32_t id = traverse<false>(*sc, r, tfar, t, u, v, stack + threadIdx.x, kTraceBlock);
             p.wave.hit[slot] = make_float4(t, __uint_as_float(id), u, v);
         }
     }
@@ -319,6 +329,17 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
                     f = mk(th.x / ptot, th.y / ptot, th.z / ptot);
                 }
                 const float time = rd.w + dist;
+                // camera unwarp: World::Li's record distance = closest surface along the camera
+                // ray, FLT_MAX when there is none (World.h:749-766, Ray.h:74-84)
+                float cam_d = 0.0f;
+                if (film.unwarp) {
+                    if (depth == 0) {
+                        cam_d = hit ? h.x : 3.40282347e+38f;
+                        p.wave.cam_dist[slot] = cam_d;
+                    } else {
+                        cam_d = p.wave.cam_dist[slot];
+                    }
+                }
                 const f3 org = mk(ro.x, ro.y, ro.z), dir = mk(rd.x, rd.y, rd.z);
                 const f3 pos = org + dir * dist;
                 if (!(time > total_time)) {
@@ -387,14 +408,20 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
                             const float Lg = (f.y * (fe.y * (irr.y * att.y))) * scale;
                             const float Lb = (f.z * (fe.z * (irr.z * att.z))) * scale;
                             const float tt = time + dl;
-                            const float ps = (tt - film.offset) / film.exposure;
-                            if (ps < (float)film.T && ps >= 0.0f && finite3(Lr, Lg, Lb) &&
-                                (Lr != 0.0f || Lg != 0.0f || Lb != 0.0f)) {
+                            const float tc = film.unwarp ? tt - cam_d : tt;      // StreakCameraFilm.h:167
+                            const float ps = (tc - film.offset) / film.exposure;
+                            const bool inside = ps < (float)film.T && ps >= 0.0f;
+                            const bool fin = finite3(Lr, Lg, Lb);
+                            // with bounce films every visible light connection is a sample (its
+                            // time and radiance aside; non-finite radiance becomes 0 as in
+                            // TransientRenderer.h:165-169); otherwise only useful ones are traced
+                            if ((inside && fin && (Lr != 0.0f || Lg != 0.0f || Lb != 0.0f)) || film.nbounce) {
                                 want_shadow = true;
+                                const uint32_t bin = inside ? (uint32_t)floorf(ps) : kBinOutside;
                                 sh_o = make_float4(lp.x, lp.y, lp.z, dl - kSigmaVis);
-                                sh_d = make_float4(ld.x, ld.y, ld.z,
-                                                   __uint_as_float((uint32_t)floorf(ps) | ((uint32_t)depth << 24)));
-                                sh_L = make_float4(Lr, Lg, Lb, __uint_as_float(slot));
+                                sh_d = make_float4(ld.x, ld.y, ld.z, __uint_as_float(bin | ((uint32_t)depth << 24)));
+                                sh_L = fin ? make_float4(Lr, Lg, Lb, __uint_as_float(slot))
+                                           : make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(slot));
                             }
                         }
                     }
@@ -524,7 +551,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
 // tile (warp-aggregated atomics on equal (pixel, bin) keys) and adds the tile to the FP64 film.
 // -----------------------------------------------------------------------------------------
 template <bool kMulti>
-__global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ Params p, int G_launch) {
+__global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ Params p, int G_launch, int bsel) {
     extern __shared__ __align__(16) float tile[];
     // the block's segment and film: the launch's own in single-scene mode; in multi-scene mode
     // from the current batch's block table, each segment with its own film-tile width
@@ -545,7 +572,15 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
     const uint32_t TT = T * 3u;
     const uint32_t pix0 = blk * G;
     if (pix0 >= B.npix) return;
+    if (bsel >= (int)film.nbounce) return;                // this scene has no such bounce film
     const uint32_t gp = min((uint32_t)G, B.npix - pix0);
+    // bsel < 0: the film; with bounce films its steady image is the base Film's (all samples).
+    // bsel = b: bounce film b, fed by the records of bounce min(depth, N-1) == b.
+    const size_t npix_film = (size_t)film.W * film.H;
+    double* out_streak = bsel < 0 ? film.streak : film.bstreak + (size_t)bsel * npix_film * TT;
+    double* out_steady = bsel < 0 ? film.steady : film.bsteady + (size_t)bsel * npix_film * 3u;
+    const bool steady_all = bsel < 0 && film.nbounce > 0;
+    const uint32_t nb_last = film.nbounce ? film.nbounce - 1u : 0u;
     float* steady = tile + (size_t)G * TT;
     {
         float4* t4 = reinterpret_cast<float4*>(tile);
@@ -580,14 +615,18 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
             const bool valid = k < cnt;
             float4 rc = make_float4(0.f, 0.f, 0.f, 0.f);
             if (valid) rc = __ldcs(&p.wave.rec[(size_t)k * rs + slot]);     // streamed, read once
-            const uint32_t key = valid ? pl * T + (__float_as_uint(rc.w) & 0x00ffffffu) : 0xffffffffu;
+            const uint32_t bin = __float_as_uint(rc.w) & 0x00ffffffu;
+            const uint32_t rdepth = __float_as_uint(rc.w) >> 24;
+            const bool mine = valid && (bsel < 0 || min(rdepth, nb_last) == (uint32_t)bsel);
+            const bool inwin = mine && bin != kBinOutside;
+            const uint32_t key = inwin ? pl * T + bin : 0xffffffffu;
             // lanes holding the same (pixel, bin) are summed with shuffles; the group's
             // lowest lane issues one shared-memory atomic per channel
             const unsigned peers = __match_any_sync(kFull, key);
             const int rank = __popc(peers & lt);
             const int gsize = __popc(peers);
             float vx = rc.x, vy = rc.y, vz = rc.z;
-            const uint32_t maxg = __reduce_max_sync(kFull, valid ? (uint32_t)gsize : 1u);
+            const uint32_t maxg = __reduce_max_sync(kFull, inwin ? (uint32_t)gsize : 1u);
             for (int step = 1; step < (int)maxg; step <<= 1) {
                 const int src_rank = rank + step;
                 const int src = src_rank < gsize ? (int)__fns(peers, 0, src_rank + 1) : (int)lane;
@@ -596,11 +635,11 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
                 const float oz = __shfl_sync(kFull, vz, src);
                 if ((rank & (2 * step - 1)) == 0 && src_rank < gsize) { vx += ox; vy += oy; vz += oz; }
             }
-            if (valid && rank == 0) {
+            if (inwin && rank == 0) {
                 float* cell = tile + (size_t)key * 3u;
                 atomicAdd(cell, vx); atomicAdd(cell + 1, vy); atomicAdd(cell + 2, vz);
             }
-            if (valid) { ax += rc.x; ay += rc.y; az += rc.z; }
+            if (inwin || (steady_all && valid)) { ax += rc.x; ay += rc.y; az += rc.z; }
         }
     }
     if (acc_pl != 0xffffffffu) {
@@ -613,7 +652,7 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
     for (uint32_t pl = 0; pl < gp; ++pl) {
         const uint32_t wpix = B.pix_begin + pix0 + pl;
         const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
-        double* dst = film.streak + pixel * TT;
+        double* dst = out_streak + pixel * TT;
         const float* src = tile + (size_t)pl * TT;
         for (uint32_t e0 = threadIdx.x; e0 < TT; e0 += 4u * blockDim.x) {
             float v[4];
@@ -631,9 +670,39 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
             }
         }
         if (threadIdx.x == 0) {
-            film.weight[pixel] += (double)B.ns;
-            for (int c = 0; c < 3; ++c) film.steady[pixel * 3 + c] += (double)steady[pl * 3 + c];
+            if (bsel < 0) film.weight[pixel] += (double)B.ns;
+            for (int c = 0; c < 3; ++c) out_steady[pixel * 3 + c] += (double)steady[pl * 3 + c];
         }
+    }
+}
+
+// Per-bounce film weights (MultibounceStreakCameraFilm.h:151-171 with StreakCameraFilm.h:139-160):
+// bounce film b's weight grows by one per camera sample (all its incoming paths together) that
+// has at least one radiance sample of bounce min(depth, N-1) == b, inside the time window or not.
+__global__ void __launch_bounds__(256) k_bounce_weights(const __grid_constant__ Params p) {
+    const Batch& B = p.batch;
+    const FilmDev& film = p.film;
+    const uint32_t ncs = B.npix * B.ns;
+    const size_t rs = p.wave.capacity;
+    const size_t npix_film = (size_t)film.W * film.H;
+    const uint32_t nb_last = film.nbounce - 1u;
+    for (uint32_t cs = blockIdx.x * blockDim.x + threadIdx.x; cs < ncs; cs += gridDim.x * blockDim.x) {
+        const uint32_t pl = cs / B.ns;
+        const uint32_t slot0 = cs * B.ninc;              // ((pl * ns) + s) * ninc
+        uint32_t mask = 0;
+        for (uint32_t j = 0; j < B.ninc; ++j) {
+            const uint32_t slot = slot0 + j;
+            const uint32_t cnt = p.wave.rec_n[slot];
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t d = __float_as_uint(p.wave.rec[(size_t)k * rs + slot].w) >> 24;
+                mask |= 1u << min(d, nb_last);
+            }
+        }
+        if (!mask) continue;
+        const uint32_t wpix = B.pix_begin + pl;
+        const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
+        for (uint32_t b = 0; b <= nb_last; ++b)
+            if (mask >> b & 1u) atomicAdd(&film.bweight[(size_t)b * npix_film + pixel], 1.0);
     }
 }
 
@@ -732,7 +801,7 @@ cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s) 
     else k_shadow<false><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
 }
-cudaError_t launch_splat(const Params& p, int G, cudaStream_t s) {
+cudaError_t launch_splat(const Params& p, int G, cudaStream_t s, int bsel) {
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_splat<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -740,14 +809,20 @@ cudaError_t launch_splat(const Params& p, int G, cudaStream_t s) {
         attr_set = true;
     }
     if (p.multi.scenes) {
-        k_splat<true><<<p.multi.max_splat_blocks, kSplatBlock, p.multi.splat_smem, s>>>(p, 0);
+        k_splat<true><<<p.multi.max_splat_blocks, kSplatBlock, p.multi.splat_smem, s>>>(p, 0, bsel);
     } else {
         const size_t smem = splat_smem_bytes(p.film.T, G);
         const uint32_t blocks = (p.batch.npix + (uint32_t)G - 1) / (uint32_t)G;
-        k_splat<false><<<blocks, kSplatBlock, smem, s>>>(p, G);
+        k_splat<false><<<blocks, kSplatBlock, smem, s>>>(p, G, bsel);
     }
     return cudaGetLastError();
 }
+cudaError_t launch_bounce_weights(const Params& p, cudaStream_t s) {
+    const uint32_t ncs = p.batch.npix * p.batch.ns;
+    k_bounce_weights<<<std::max(1u, std::min(4096u, (ncs + 255) / 256)), 256, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
 // last node of a multi-scene batch: the next replay renders the next batch descriptor
 __global__ void k_advance(uint32_t* cur) { *cur += 1u; }
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s) {

@@ -89,7 +89,8 @@ struct Wave {
     float4* sh_o;             // shadow: origin, tfar
     float4* sh_d;             // shadow: direction, time bin (bits)
     float4* sh_L;             // shadow: contribution rgb, slot (bits)
-    float4* rec;              // splat records [bounce][capacity]: rgb, bin (bits)
+    float4* rec;              // splat records [bounce][capacity]: rgb, bin | depth << 24 (bits)
+    float* cam_dist;          // camera-to-first-surface distance per slot (camera unwarp)
     uint8_t* rec_n;           // records per slot
     uint32_t* counters;       // see counter_* helpers below
     unsigned long long* stats;// closest, shadow, splats, paths (accumulated)
@@ -102,7 +103,16 @@ struct FilmDev {
     double* weight;           // [H][W]
     uint32_t W, H, T;
     float exposure, offset;
+    uint32_t unwarp;          // bin by path time minus the camera-to-first-surface distance
+    uint32_t nbounce;         // per-bounce films (0 = none)
+    double* bstreak;          // [nbounce][H][W][T][3]
+    double* bsteady;          // [nbounce][H][W][3]
+    double* bweight;          // [nbounce][H][W]
 };
+
+// bin of a radiance sample outside the time window: kept (with bounce films only) because the
+// sample still counts for its bounce film's weight and for the base steady image
+constexpr uint32_t kBinOutside = 0xffffffu;
 
 struct SceneSlot {            // one scene of a multi-scene batch
     SceneDev scene;
@@ -177,7 +187,10 @@ cudaError_t launch_raygen(const Params& p, cudaStream_t s);
 cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s);
 cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
-cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s);
+// bsel < 0: the film itself; bsel = b: per-bounce film b (records of bounce min(depth, N-1) == b)
+cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s, int bsel = -1);
+// per-bounce film weights: +1 per camera sample with a record of that bounce film
+cudaError_t launch_bounce_weights(const Params& p, cudaStream_t s);
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);

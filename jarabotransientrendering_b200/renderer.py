@@ -67,7 +67,8 @@ class Context:
                         mats, len(scene.materials), lights, len(scene.lights), med)
         pos, nv, uv, vv, fd = scene.camera.basis()
         cam = _abi.Camera(_abi.f3(*pos), _abi.f3(*nv), _abi.f3(*uv), _abi.f3(*vv), float(fd))
-        film = _abi.Film(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset)
+        film = _abi.Film(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset,
+                         int(scene.camera_unwarp), int(scene.bounce_films))
         integ = _abi.Integrator(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, scene.flags, scene.seed)
         h = C.c_void_p()
         _abi.check(L.tr_create(C.byref(sc), C.byref(cam), C.byref(film), C.byref(integ), device, C.byref(h)))
@@ -99,6 +100,18 @@ class Context:
         _abi.check(_abi.lib().tr_get_film(self.h, st.ctypes.data if st is not None else None,
                                           sd.ctypes.data if sd is not None else None,
                                           wt.ctypes.data if wt is not None else None))
+        return {"streak": st, "steady": sd, "weight": wt}
+
+    def bounce_film(self, bounce, streak=True, steady=True, weight=True):
+        """Per-bounce film ``bounce`` (scenes with bounce_films > 0), as ``film``."""
+        sc = self.scene
+        H, W, T = sc.height, sc.width, sc.time_bins
+        st = np.empty((H, W, T, 3), np.float64) if streak else None
+        sd = np.empty((H, W, 3), np.float64) if steady else None
+        wt = np.empty((H, W), np.float64) if weight else None
+        _abi.check(_abi.lib().tr_get_film_bounce(self.h, bounce, st.ctypes.data if st is not None else None,
+                                                 sd.ctypes.data if sd is not None else None,
+                                                 wt.ctypes.data if wt is not None else None))
         return {"streak": st, "steady": sd, "weight": wt}
 
     def film_into(self, streak=None, steady=None, weight=None):
@@ -414,11 +427,12 @@ class StreakCameraFilm:
     """Streak film of ``time_resolution`` bins of ``exposure`` (StreakCameraFilm.h:91-121).
     After a render it holds the accumulated sums (``streak``, ``steady``, ``weight``)."""
 
+    bounce_films = 0
+
     def __init__(self, w, h, t, exposure, camera_unwarp=False, filter=None):
-        if camera_unwarp:
-            raise NotImplementedError("-camera-unwarp is not supported by the GPU path")
         self.width, self.height, self.time_resolution = int(w), int(h), int(t)
         self.exposure = float(exposure)
+        self.camera_unwarp = bool(camera_unwarp)
         self.offset = 0.0
         self.streak = self.steady = self.weight = None
         self._ctx = None
@@ -443,6 +457,26 @@ class StreakCameraFilm:
         if self._ctx is None:
             raise RuntimeError("film has not been rendered")
         self._ctx.write(name)
+
+
+class MultibounceStreakFilm(StreakCameraFilm):
+    """``nb_bounces`` per-bounce streak films (MultibounceStreakCameraFilm.h:63-83,151-171):
+    a radiance sample of bounce b goes to film min(b, nb_bounces - 1).  After a render
+    ``bounce_streak``/``bounce_steady``/``bounce_weight`` hold the per-bounce sums and
+    ``steady`` the base film's image of all samples."""
+
+    def __init__(self, w, h, t, exposure, nb_bounces, filter=None, camera_unwarp=False):
+        super().__init__(w, h, t, exposure, camera_unwarp, filter)
+        if not 1 <= int(nb_bounces) <= 32:
+            raise ValueError("nb_bounces must be in [1, 32]")
+        self.bounce_films = int(nb_bounces)
+        self.bounce_streak = self.bounce_steady = self.bounce_weight = None
+
+    def bounce_streak_image(self, b=0, y=0):
+        """Averaged streak image (time x width) of scanline y of bounce film b."""
+        with np.errstate(invalid="ignore", divide="ignore"):
+            img = self.bounce_streak[b, y] / self.bounce_weight[b, y][:, None, None]
+        return np.nan_to_num(img, nan=0.0).transpose(1, 0, 2)
 
 
 class StratifiedSampler:
@@ -494,10 +528,17 @@ class TransientRenderer:
                         film.width, film.height, film.time_resolution, film.exposure, film.offset,
                         integrator.max_path_size, sampler.sqrt_spp, integrator.incoming_samples,
                         world._medium, integrator.seed)
+        scene.camera_unwarp = int(film.camera_unwarp)
+        scene.bounce_films = int(film.bounce_films)
         ctx = Context(scene, self.device)
         ctx.render(0, scene.spp)
         f = ctx.film()
         film.streak, film.steady, film.weight = f["streak"], f["steady"], f["weight"]
+        if film.bounce_films:
+            b = [ctx.bounce_film(k) for k in range(film.bounce_films)]
+            film.bounce_streak = np.stack([x["streak"] for x in b])
+            film.bounce_steady = np.stack([x["steady"] for x in b])
+            film.bounce_weight = np.stack([x["weight"] for x in b])
         film._ctx = ctx
         if name:
             ctx.write(name)

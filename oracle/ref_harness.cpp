@@ -17,11 +17,16 @@
  *     CMake-generated headers;
  *   - the film is a StreakCameraFilm whose add_samples (StreakCameraFilm.h:139-192) is
  *     overridden to accumulate the same (pixel, bin) sums in double precision into one
- *     buffer instead of averaging and writing RGBE scanlines.
+ *     buffer instead of averaging and writing RGBE scanlines; with `filmopts U N` it also
+ *     applies the camera unwarp of StreakCameraFilm.h:167 (sample time minus the record's
+ *     camera distance) and, for N > 0, routes the samples to N per-bounce films with the
+ *     weights of MultibounceStreakFilm::add_samples (MultibounceStreakCameraFilm.h:151-171),
+ *     the main steady image then being the base Film's (all samples, Film.h:263-284).
  *
  * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
  *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
- *   streak [H][W][T][3] (unless --no-streak), steady [H][W][3], weight [H][W].
+ *   streak [H][W][T][3] (unless --no-streak), steady [H][W][3], weight [H][W], then with N
+ *   bounce films bstreak [N][H][W][T][3], bsteady [N][H][W][3], bweight [N][H][W].
  *   Prints one JSON line with paths, seconds and paths/s on stdout.
  */
 #include <chrono>
@@ -62,29 +67,50 @@ public:
     Real exposure, offset;
     std::vector<double> streak, steady, weight;
     bool keep_streak;
-    AccumStreakFilm(unsigned w, unsigned h, unsigned t, Real exp_, Real off, bool ks)
-        : Base(w, h, t, exp_, false, nullptr), W(w), H(h), T(t), exposure(exp_), offset(off),
-          keep_streak(ks) {
+    bool unwarp;
+    unsigned NB;
+    std::vector<double> bstreak, bsteady, bweight;
+    AccumStreakFilm(unsigned w, unsigned h, unsigned t, Real exp_, Real off, bool ks, bool uw, unsigned nb)
+        : Base(w, h, t, exp_, uw, nullptr), W(w), H(h), T(t), exposure(exp_), offset(off),
+          keep_streak(ks), unwarp(uw), NB(nb) {
         if (off > 0) this->set_offset(off);
         if (ks) streak.assign((size_t)h * w * t * 3, 0.0);
         steady.assign((size_t)h * w * 3, 0.0);
         weight.assign((size_t)h * w, 0.0);
+        if (nb) {
+            bstreak.assign((size_t)nb * h * w * t * 3, 0.0);
+            bsteady.assign((size_t)nb * h * w * 3, 0.0);
+            bweight.assign((size_t)nb * h * w, 0.0);
+        }
     }
     /* StreakCameraFilm::add_samples with the box filter of size 1 (weight 1, one pixel): */
     void add_samples(const Sample& sample, const RadianceSampleRecordVector<3, Radiance>& rec) override {
         unsigned x = (unsigned)std::floor(sample.position[0]);
         unsigned y = (unsigned)std::floor(sample.position[1]);
         size_t pix = (size_t)y * W + x;
+        const size_t npix = (size_t)W * H;
         weight[pix] += sample.weight;
+        std::vector<char> present(NB, 0);
         for (const RadianceSample<3, Radiance>& r : rec.samples) {
-            Real pos_sensor = (r.time - offset) / exposure;
-            if (!(pos_sensor < T && pos_sensor >= 0.0)) continue;
+            const unsigned b = NB ? (r.bounce < NB ? r.bounce : NB - 1) : 0;
+            if (NB) present[b] = 1;
+            Real cam_time = unwarp ? (r.time - rec.distance) : r.time;
+            Real pos_sensor = (cam_time - offset) / exposure;
+            const bool inside = pos_sensor < T && pos_sensor >= 0.0;
+            for (int c = 0; c < 3; ++c)
+                if (inside || NB) steady[pix * 3 + c] += (double)r.radiance[c];
+            if (!inside) continue;
             size_t t = (size_t)std::floor(pos_sensor);
             for (int c = 0; c < 3; ++c) {
                 if (keep_streak) streak[(pix * T + t) * 3 + c] += (double)r.radiance[c];
-                steady[pix * 3 + c] += (double)r.radiance[c];
+                if (NB) {
+                    bstreak[(((size_t)b * npix + pix) * T + t) * 3 + c] += (double)r.radiance[c];
+                    bsteady[((size_t)b * npix + pix) * 3 + c] += (double)r.radiance[c];
+                }
             }
         }
+        for (unsigned b = 0; b < NB; ++b)
+            if (present[b]) bweight[(size_t)b * npix + pix] += sample.weight;
     }
     void write(const char*) override {}
 };
@@ -105,7 +131,7 @@ int main(int argc, char** argv) {
     std::ifstream in(argv[1]);
     if (!in) fail("cannot open scene");
     std::string tag;
-    unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1;
+    unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1, unwarp = 0, nbounce = 0;
     Real exposure = 0, offset = 0, fov = 40;
     unsigned long long seed = 1;
     Vector3 cpos, cfoc, cup;
@@ -116,6 +142,7 @@ int main(int argc, char** argv) {
     std::vector<std::string> light_lines;
     while (in >> tag) {
         if (tag == "film") { in >> W >> H >> T >> exposure >> offset; }
+        else if (tag == "filmopts") { in >> unwarp >> nbounce; }
         else if (tag == "camera") {
             float a[9]; for (float& v : a) in >> v; in >> fov;
             cpos = Vector3(a[0], a[1], a[2]); cfoc = Vector3(a[3], a[4], a[5]); cup = Vector3(a[6], a[7], a[8]);
@@ -176,7 +203,7 @@ int main(int argc, char** argv) {
     Real fovr = M_PI / 180. * fov / 2;                                   /* bunnykiller.cpp:1156-1161 */
     Real fd = 1. / tan(fovr);
     PinholeCamera camera(cpos, cfoc, cup, fd);
-    AccumStreakFilm film(W, H, T, exposure, offset, keep_streak);
+    AccumStreakFilm film(W, H, T, exposure, offset, keep_streak, unwarp != 0, nbounce);
     StratifiedSampler sampler(W, H, sqrt_spp, true);
     TransientRenderer<3, Radiance, RadianceAttenuation> engine(nullptr, false);
     Random::StdRNG.seed(seed);                                           /* bunnykiller.cpp:1794 */
@@ -207,6 +234,11 @@ int main(int argc, char** argv) {
     if (keep_streak) fwrite(film.streak.data(), sizeof(double), film.streak.size(), out);
     fwrite(film.steady.data(), sizeof(double), film.steady.size(), out);
     fwrite(film.weight.data(), sizeof(double), film.weight.size(), out);
+    if (nbounce) {
+        fwrite(film.bstreak.data(), sizeof(double), film.bstreak.size(), out);
+        fwrite(film.bsteady.data(), sizeof(double), film.bsteady.size(), out);
+        fwrite(film.bweight.data(), sizeof(double), film.bweight.size(), out);
+    }
     fclose(out);
     FILE* tty = fopen("/dev/stderr", "w");
     fprintf(tty, "{\"paths\": %llu, \"seconds\": %.6f, \"paths_per_s\": %.3f}\n", paths, secs, paths / secs);

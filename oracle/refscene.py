@@ -20,7 +20,14 @@ def ref_available():
     return os.path.exists(REF_BIN)
 
 
-def build_ref(ref_src="/root/reference/src"):
+REF_SRC = "/root/reference/src"     # where the reference sources lie in the build container
+
+
+def sources_available(ref_src=REF_SRC):
+    return os.path.isdir(ref_src)
+
+
+def build_ref(ref_src=REF_SRC):
     """Compile the harness from the reference sources (only where those sources exist)."""
     if os.path.isdir(ref_src):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_SRC={ref_src}"])
@@ -30,6 +37,9 @@ def build_ref(ref_src="/root/reference/src"):
 def write_scene(scene, path, seed=None):
     lines = []
     lines.append(f"film {scene.width} {scene.height} {scene.time_bins} {scene.exposure!r} {scene.offset!r}")
+    uw, nb = int(getattr(scene, "camera_unwarp", 0)), int(getattr(scene, "bounce_films", 0))
+    if uw or nb:
+        lines.append(f"filmopts {uw} {nb}")
     c = scene.camera
     lines.append("camera " + " ".join(repr(float(v)) for v in (*c.position, *c.focus, *c.up)) + f" {c.fov_deg!r}")
     lines.append(f"integrator {scene.max_bounces} {scene.sqrt_spp} {scene.incoming_samples} "
@@ -77,9 +87,20 @@ def render(scene, seed=None, rows=None, keep_streak=True, workdir=None):
         streak = raw[:H * W * T * 3].reshape(H, W, T, 3)
         off = H * W * T * 3
     steady = raw[off:off + H * W * 3].reshape(H, W, 3)
-    weight = raw[off + H * W * 3:].reshape(H, W)
+    off += H * W * 3
+    weight = raw[off:off + H * W].reshape(H, W)
+    off += H * W
+    extra = {}
+    NB = int(getattr(scene, "bounce_films", 0))
+    if NB:
+        n = NB * H * W * T * 3
+        extra["bstreak"] = raw[off:off + n].reshape(NB, H, W, T, 3)
+        off += n
+        extra["bsteady"] = raw[off:off + NB * H * W * 3].reshape(NB, H, W, 3)
+        off += NB * H * W * 3
+        extra["bweight"] = raw[off:off + NB * H * W].reshape(NB, H, W)
     if workdir is None:
         for p in (sp, op):
             os.remove(p)
         os.rmdir(wd)
-    return {"streak": streak, "steady": steady, "weight": weight, **info}
+    return {"streak": streak, "steady": steady, "weight": weight, **extra, **info}

@@ -6,7 +6,11 @@ scenes with K independent seeds and stores per-bin mean and standard error of th
 film, plus per-seed total energy.  Needs the reference sources (only in the build
 container); the committed .npz files are what the tests read.
 
-    python tests/golden/make_golden.py            # writes tests/golden/ref_*.npz
+    python tests/golden/make_golden.py [names]    # writes tests/golden/ref_*.npz
+
+`unwarp` and `bounces` exercise the film options: the camera unwarp of StreakCameraFilm and
+three per-bounce films of MultibounceStreakFilm (their per-bounce streaks are stored as one
+film of 3H rows, their weights and the base steady image beside them).
 """
 import os
 import sys
@@ -33,21 +37,39 @@ def golden_scenes():
     a = S.guided(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6,
                  lambertian_floor=True)
     a.lights = [S.rect_light((0.6, 0.8, 0.6), (0.6, 0.0, 0.6), (0.2, 0.2), 4.0)]
-    return {"cornell": c, "medium": m, "arealight": a}
+    u = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
+    u.lights[0].position = (0.5, 0.8, 0.5)
+    u.camera_unwarp = 1
+    b = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
+    b.lights[0].position = (0.5, 0.8, 0.5)
+    b.bounce_films = 3
+    return {"cornell": c, "medium": m, "arealight": a, "unwarp": u, "bounces": b}
 
 
-def main():
+def main(names=None):
     if not refscene.build_ref():
         raise SystemExit("reference sources not available: cannot build oracle/_ref/ref_render")
     for name, sc in golden_scenes().items():
-        films = np.array([refscene.render(sc, seed=s)["streak"] for s in range(1, K + 1)])
+        if names and name not in names:
+            continue
+        runs = [refscene.render(sc, seed=s) for s in range(1, K + 1)]
+        films = np.array([r["streak"] for r in runs])
+        if sc.bounce_films:
+            nb, H = sc.bounce_films, sc.height
+            films = np.array([r["bstreak"].reshape(nb * H, *r["bstreak"].shape[2:]) for r in runs])
         mean = films.mean(0)
         se = films.std(0, ddof=1) / np.sqrt(K)
         energy = films.sum(axis=(1, 2, 3, 4))
+        extra = {}
+        if sc.bounce_films:
+            bw = np.array([r["bweight"] for r in runs])
+            sd = np.array([r["steady"] for r in runs])
+            extra = dict(bweight_mean=bw.mean(0), bweight_se=bw.std(0, ddof=1) / np.sqrt(K),
+                         steady_mean=sd.mean(0), steady_se=sd.std(0, ddof=1) / np.sqrt(K))
         out = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}.npz")
-        np.savez_compressed(out, mean=mean.astype(np.float32), se=se.astype(np.float32), energy=energy, k=K)
+        np.savez_compressed(out, mean=mean.astype(np.float32), se=se.astype(np.float32), energy=energy, k=K, **extra)
         print(name, out, "energy %.4f +- %.4f" % (energy.mean(), energy.std(ddof=1) / np.sqrt(K)))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -116,11 +116,47 @@ def test_oracle_matches_reference_statistics(oracle_lib, name):
     assert r["one_sided_bins"] == 0, r
 
 
+def test_oracle_camera_unwarp_matches_reference(oracle_lib):
+    """Camera unwarp (StreakCameraFilm.h:167): bins by path time minus the camera-to-first-surface
+    distance; the oracle agrees with the reference's own integrator and record distance."""
+    sc = _golden_scene("unwarp")
+    g = _golden("unwarp")
+    o = oracle_lib.Oracle(sc)
+    K = len(g["energy"])
+    films = np.array([o.render(sample_begin=64 * k, sample_count=64, nthreads=4)["streak"] for k in range(K)])
+    r = compare_to_golden(films, g)
+    assert r["frac_z3"] < 0.02 and abs(r["mean_z"]) < 0.1 and r["max_z"] < 7.0, r
+    assert abs(r["energy_z"]) < 4.0 and r["one_sided_bins"] == 0, r
+
+
+def test_oracle_bounce_films_match_reference(oracle_lib):
+    """Per-bounce films (MultibounceStreakCameraFilm.h:151-171): the streak of each bounce film,
+    each film's weight (camera samples with a sample of that bounce, inside the time window or
+    not) and the base film's steady image (all samples) agree with the reference."""
+    sc = _golden_scene("bounces")
+    g = _golden("bounces")
+    o = oracle_lib.Oracle(sc)
+    K = len(g["energy"])
+    nb, H = sc.bounce_films, sc.height
+    runs = [o.render(sample_begin=64 * k, sample_count=64, nthreads=4, bounces=True) for k in range(K)]
+    films = np.array([r["bstreak"].reshape(nb * H, *r["bstreak"].shape[2:]) for r in runs])
+    r = compare_to_golden(films, g)
+    assert r["frac_z3"] < 0.02 and abs(r["mean_z"]) < 0.1 and r["max_z"] < 7.0, r
+    assert abs(r["energy_z"]) < 4.0 and r["one_sided_bins"] == 0, r
+    for key, arr in (("bweight", np.array([r["bweight"] for r in runs])), ("steady", np.array([r["steady"] for r in runs]))):
+        se = np.sqrt((arr.std(0, ddof=1) / np.sqrt(K)) ** 2 + g[key + "_se"] ** 2)
+        m = se > 0
+        z = (arr.mean(0) - g[key + "_mean"])[m] / se[m]
+        assert (np.abs(z) > 3).mean() < 0.03 and abs(z.mean()) < 0.2, (key, (np.abs(z) > 3).mean(), z.mean())
+    # the weights count camera samples: at most the samples per pixel
+    assert (g["bweight_mean"] <= 64 + 1e-9).all()
+
+
 def test_oracle_reference_harness_live(oracle_lib):
     """When the reference sources are present, rebuild and rerun the reference harness and
     check it still reproduces the committed golden statistics."""
     from oracle import refscene
-    if not os.path.isdir("/root/reference/src"):
+    if not refscene.sources_available():
         pytest.skip("reference sources not present on this machine")
     assert refscene.build_ref()
     sc = _golden_scene("cornell")
