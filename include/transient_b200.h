@@ -118,7 +118,17 @@ typedef struct tr_film {
     float offset;
     uint32_t camera_unwarp;
     uint32_t bounce_films;
+    uint32_t components;       /* TR_COMP_* bits ("-film-depth", "-film-positions", "-film-normals") */
 } tr_film;
+
+/* Film components (FilmComponents.h; Film::add_components, Film.h:127-145): per pixel, the
+ * sum over camera samples of World::Li's camera-ray record (World.h:749-766) -- the distance
+ * to the closest surface at any distance (FLT_MAX when there is none), and that point's
+ * position and normal (zero when none).  tr_write_film writes them averaged as
+ * "<name>_depth.hdr", "<name>_positions.raw" and "<name>_normals.raw" (Film.h:357-471).    */
+#define TR_COMP_DEPTH 2u
+#define TR_COMP_POSITIONS 8u
+#define TR_COMP_NORMALS 16u
 
 /* Unidirectional path tracing with next-event estimation, the only mode the reference CLI runs
  * (src/Integrator/BidirectionalPathTracing.h:122-137,1099-1140; ProgramParams.h:162-164).
@@ -204,6 +214,10 @@ tr_status tr_get_film(tr_ctx* ctx, double* streak, double* steady, double* weigh
  * the context's stream after its pending renders and return when the copy is complete; the
  * caller's own pending work on the destination must be finished first.                      */
 tr_status tr_get_film_device(tr_ctx* ctx, double* d_streak, double* d_steady, double* d_weight);
+
+/* Component sums (any may be NULL; the film must have the component): depth [H][W],
+ * positions [H][W][3], normals [H][W][3] (double, divide by weight to average).               */
+tr_status tr_get_film_components(tr_ctx* ctx, double* depth, double* positions, double* normals);
 
 /* Per-bounce film `bounce` (< bounce_films) of the context, layouts as tr_get_film.           */
 tr_status tr_get_film_bounce(tr_ctx* ctx, uint32_t bounce, double* streak, double* steady, double* weight);

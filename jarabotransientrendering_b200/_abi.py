@@ -43,7 +43,7 @@ class Camera(C.Structure):
 class Film(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("time_bins", C.c_uint32),
                 ("exposure", C.c_float), ("offset", C.c_float), ("camera_unwarp", C.c_uint32),
-                ("bounce_films", C.c_uint32)]
+                ("bounce_films", C.c_uint32), ("components", C.c_uint32)]
 
 
 class Integrator(C.Structure):
@@ -86,6 +86,7 @@ PROTOTYPES = {
     "tr_get_film": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_bounce": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tr_get_film_components": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_write_film": (C.c_int, [C.c_void_p, C.c_char_p]),
     "tr_trace_rays": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]),
     "tr_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),

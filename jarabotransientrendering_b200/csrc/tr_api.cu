@@ -81,6 +81,8 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     if ((uint64_t)f->width * f->height >= (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "film too large");
     if (f->camera_unwarp > 1) return fail(TR_ERR_INVALID_ARGUMENT, "camera_unwarp must be 0 or 1");
     if (f->bounce_films > 32) return fail(TR_ERR_INVALID_ARGUMENT, "at most 32 bounce films");
+    if (f->components & ~(TR_COMP_DEPTH | TR_COMP_POSITIONS | TR_COMP_NORMALS))
+        return fail(TR_ERR_INVALID_ARGUMENT, "unknown film component bits");
     if (trk::splat_smem_bytes(f->time_bins, 1) > 220 * 1024)
         return fail(TR_ERR_NOT_SUPPORTED, "time_bins too large for one shared-memory pixel tile");
     if (it->sqrt_spp == 0 || it->incoming_samples == 0)
@@ -165,6 +167,8 @@ trk::Params make_params(tr_ctx* x) {
     p.film.unwarp = x->film.camera_unwarp;
     p.film.nbounce = x->film.bounce_films;
     p.film.bstreak = x->d_bstreak; p.film.bsteady = x->d_bsteady; p.film.bweight = x->d_bweight;
+    p.film.comps = x->film.components;
+    p.film.cdepth = x->d_cdepth; p.film.cpos = x->d_cpos; p.film.cnorm = x->d_cnorm;
     p.film.W = x->film.width; p.film.H = x->film.height; p.film.T = x->film.time_bins;
     p.film.exposure = x->film.exposure; p.film.offset = x->film.offset;
     p.wave = x->wave;
@@ -459,6 +463,15 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             TR_CUDA(cudaMemsetAsync(x->d_bsteady, 0, nb * npix * 3u * sizeof(double), x->stream));
             TR_CUDA(cudaMemsetAsync(x->d_bweight, 0, nb * npix * sizeof(double), x->stream));
         }
+        {
+            const size_t npix = (size_t)f->width * f->height;
+            if (f->components & TR_COMP_DEPTH) x->d_cdepth = x->alloc<double>(npix);
+            if (f->components & TR_COMP_POSITIONS) x->d_cpos = x->alloc<double>(npix * 3u);
+            if (f->components & TR_COMP_NORMALS) x->d_cnorm = x->alloc<double>(npix * 3u);
+            if (x->d_cdepth) TR_CUDA(cudaMemsetAsync(x->d_cdepth, 0, npix * sizeof(double), x->stream));
+            if (x->d_cpos) TR_CUDA(cudaMemsetAsync(x->d_cpos, 0, npix * 3u * sizeof(double), x->stream));
+            if (x->d_cnorm) TR_CUDA(cudaMemsetAsync(x->d_cnorm, 0, npix * 3u * sizeof(double), x->stream));
+        }
 
         x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);
         int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
@@ -511,6 +524,9 @@ tr_status tr_clear_film(tr_ctx* x) {
             TR_CUDA(cudaMemsetAsync(x->d_bsteady, 0, nb * npix * 3u * sizeof(double), x->s()));
             TR_CUDA(cudaMemsetAsync(x->d_bweight, 0, nb * npix * sizeof(double), x->s()));
         }
+        if (x->d_cdepth) TR_CUDA(cudaMemsetAsync(x->d_cdepth, 0, npix * sizeof(double), x->s()));
+        if (x->d_cpos) TR_CUDA(cudaMemsetAsync(x->d_cpos, 0, npix * 3u * sizeof(double), x->s()));
+        if (x->d_cnorm) TR_CUDA(cudaMemsetAsync(x->d_cnorm, 0, npix * 3u * sizeof(double), x->s()));
         TR_CUDA(cudaStreamSynchronize(x->s()));
         x->stats.camera_samples = 0;
         x->stats.paths = 0;
@@ -545,6 +561,24 @@ tr_status tr_get_film(tr_ctx* x, double* streak, double* steady, double* weight)
 
 tr_status tr_get_film_device(tr_ctx* x, double* streak, double* steady, double* weight) {
     return copy_film(x, streak, steady, weight, cudaMemcpyDeviceToDevice);
+}
+
+tr_status tr_get_film_components(tr_ctx* x, double* depth, double* positions, double* normals) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    if ((depth && !x->d_cdepth) || (positions && !x->d_cpos) || (normals && !x->d_cnorm))
+        return fail(TR_ERR_INVALID_ARGUMENT, "the film does not have that component");
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        cudaStream_t s = x->s();
+        const size_t npix = (size_t)x->film.width * x->film.height;
+        if (depth) TR_CUDA(cudaMemcpyAsync(depth, x->d_cdepth, npix * sizeof(double), cudaMemcpyDefault, s));
+        if (positions) TR_CUDA(cudaMemcpyAsync(positions, x->d_cpos, npix * 3u * sizeof(double), cudaMemcpyDefault, s));
+        if (normals) TR_CUDA(cudaMemcpyAsync(normals, x->d_cnorm, npix * 3u * sizeof(double), cudaMemcpyDefault, s));
+        TR_CUDA(cudaStreamSynchronize(s));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
 }
 
 tr_status tr_get_film_bounce(tr_ctx* x, uint32_t b, double* streak, double* steady, double* weight) {
@@ -583,6 +617,23 @@ tr_status tr_write_film(tr_ctx* x, const char* name) {
     if (!trio::write_streak_film(name, x->film.width, x->film.height, x->film.time_bins, nb ? nullptr : streak.data(),
                                  steady.data(), weight.data(), &err))
         return fail(TR_ERR_IO, err);
+    // film components, averaged by the film weight (Film::average_and_write, Film.h:357-471)
+    if (x->film.components) {
+        std::vector<double> cd(npix), cp(npix * 3), cn(npix * 3);
+        st = tr_get_film_components(x, x->d_cdepth ? cd.data() : nullptr, x->d_cpos ? cp.data() : nullptr,
+                                    x->d_cnorm ? cn.data() : nullptr);
+        if (st != TR_OK) return st;
+        const std::string base(name);
+        if (x->d_cdepth && !trio::write_component(base + "_depth.hdr", x->film.width, x->film.height, 1, cd.data(),
+                                                  weight.data(), &err))
+            return fail(TR_ERR_IO, err);
+        if (x->d_cpos && !trio::write_component(base + "_positions.raw", x->film.width, x->film.height, 3, cp.data(),
+                                                weight.data(), &err))
+            return fail(TR_ERR_IO, err);
+        if (x->d_cnorm && !trio::write_component(base + "_normals.raw", x->film.width, x->film.height, 3, cn.data(),
+                                                 weight.data(), &err))
+            return fail(TR_ERR_IO, err);
+    }
     for (uint32_t b = 0; b < nb; ++b) {
         st = tr_get_film_bounce(x, b, streak.data(), nullptr, weight.data());
         if (st != TR_OK) return st;

@@ -77,4 +77,24 @@ bool write_streak_film(const char* name, uint32_t W, uint32_t H, uint32_t T, con
     return write_hdr(buf, W, H, st.data(), err);
 }
 
+bool write_component(const std::string& path, uint32_t W, uint32_t H, uint32_t channels, const double* sums,
+                     const double* weight, std::string* err) {
+    const size_t npix = (size_t)W * H;
+    std::vector<float> avg(npix * channels);
+    for (size_t i = 0; i < npix; ++i)
+        for (uint32_t c = 0; c < channels; ++c) avg[i * channels + c] = avg_nan0(sums[i * channels + c], weight[i]);
+    if (path.size() >= 4 && path.compare(path.size() - 4, 4, ".raw") == 0) {
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) { if (err) *err = "cannot open " + path; return false; }
+        const bool ok = std::fwrite(avg.data(), sizeof(float), avg.size(), f) == avg.size();
+        std::fclose(f);
+        if (!ok && err) *err = "short write to " + path;
+        return ok;
+    }
+    std::vector<float> rgb(npix * 3);
+    for (size_t i = 0; i < npix; ++i)
+        for (int c = 0; c < 3; ++c) rgb[i * 3 + c] = avg[i * channels + (channels == 1 ? 0 : c)];
+    return write_hdr(path, W, H, rgb.data(), err);
+}
+
 }  // namespace trio

@@ -19,4 +19,10 @@ bool write_hdr(const std::string& path, uint32_t width, uint32_t height, const f
 bool write_streak_film(const char* name, uint32_t W, uint32_t H, uint32_t T, const double* streak,
                        const double* steady, const double* weight, std::string* err);
 
+// Writes a film component averaged by the pixel weight (NaN -> 0) the way Film::average_and_write
+// does (src/Film/Film.h:357-471, src/Image/ImageIO.h:146-193): ".hdr" as RGBE (one channel
+// replicated to RGB, as stb's writer does), ".raw" as the float32 [H][W][channels] dump.
+bool write_component(const std::string& path, uint32_t W, uint32_t H, uint32_t channels, const double* sums,
+                     const double* weight, std::string* err);
+
 }  // namespace trio

@@ -123,6 +123,9 @@ struct tr_ctx {
     double* d_bstreak = nullptr;            // per-bounce films (tr_film.bounce_films > 0)
     double* d_bsteady = nullptr;
     double* d_bweight = nullptr;
+    double* d_cdepth = nullptr;             // film components (tr_film.components)
+    double* d_cpos = nullptr;
+    double* d_cnorm = nullptr;
 
     // wavefront state
     trk::Wave wave{};

@@ -197,9 +197,10 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(const _
             WRay r;
             wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
             float t, u, v;
-            // camera unwarp needs the camera ray's closest surface at any distance; shade still
+            // camera unwarp and the film components need the camera ray's closest surface at any
+            // distance (World::Li's record, World.h:749-766); shade still
             // decides surface vs medium event by comparing with the sampled distance (o.w)
-            const float tfar = depth == 0 && film->unwarp ? __int_as_float(0x7f800000) : o.w;
+            const float tfar = depth == 0 && (film->unwarp || film->comps) ? __int_as_float(0x7f800000) : o.w;
             const uint32_t id = traverse<false>(*sc, r, tfar, t, u, v, stack + threadIdx.x, kTraceBlock);
             p.wave.hit[slot] = make_float4(t, __uint_as_float(id), u, v);
         }
@@ -307,6 +308,29 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
             const bool hit = id != kInvalid;
             const float dsamp = ro.w;
             const bool surface = hit && (!medium || h.x < dsamp);
+            if (depth == 0 && film.comps && lslot % B.ninc == 0) {
+                // film components: one camera-ray record per camera sample (Film.h:127-145)
+                const uint32_t pl = lslot / per_pix;
+                const uint32_t wpix = B.pix_begin + pl;
+                const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
+                f3 cp = mk(0.f, 0.f, 0.f), cn = cp;
+                if (hit) {
+                    cp = mk(ro.x, ro.y, ro.z) + mk(rd.x, rd.y, rd.z) * h.x;
+                    const float4 ng = __ldg(&sc.tri_ng[id]);
+                    cn = mk(ng.x, ng.y, ng.z);
+                }
+                if (film.comps & 2u) atomicAdd(&film.cdepth[pixel], (double)(hit ? h.x : 3.40282347e+38f));
+                if (film.comps & 8u) {
+                    atomicAdd(&film.cpos[pixel * 3], (double)cp.x);
+                    atomicAdd(&film.cpos[pixel * 3 + 1], (double)cp.y);
+                    atomicAdd(&film.cpos[pixel * 3 + 2], (double)cp.z);
+                }
+                if (film.comps & 16u) {
+                    atomicAdd(&film.cnorm[pixel * 3], (double)cn.x);
+                    atomicAdd(&film.cnorm[pixel * 3 + 1], (double)cn.y);
+                    atomicAdd(&film.cnorm[pixel * 3 + 2], (double)cn.z);
+                }
+            }
             if (medium || hit) {
                 // per-path RNG: state in memory, increment from the camera sample
                 const uint32_t pl = lslot / per_pix;

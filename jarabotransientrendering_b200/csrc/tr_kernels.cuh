@@ -108,6 +108,10 @@ struct FilmDev {
     double* bstreak;          // [nbounce][H][W][T][3]
     double* bsteady;          // [nbounce][H][W][3]
     double* bweight;          // [nbounce][H][W]
+    uint32_t comps;           // film components (TR_COMP_* bits)
+    double* cdepth;           // [H][W] camera-ray record sums
+    double* cpos;             // [H][W][3]
+    double* cnorm;            // [H][W][3]
 };
 
 // bin of a radiance sample outside the time window: kept (with bounce films only) because the

@@ -68,7 +68,7 @@ class Context:
         pos, nv, uv, vv, fd = scene.camera.basis()
         cam = _abi.Camera(_abi.f3(*pos), _abi.f3(*nv), _abi.f3(*uv), _abi.f3(*vv), float(fd))
         film = _abi.Film(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset,
-                         int(scene.camera_unwarp), int(scene.bounce_films))
+                         int(scene.camera_unwarp), int(scene.bounce_films), int(scene.components))
         integ = _abi.Integrator(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, scene.flags, scene.seed)
         h = C.c_void_p()
         _abi.check(L.tr_create(C.byref(sc), C.byref(cam), C.byref(film), C.byref(integ), device, C.byref(h)))
@@ -113,6 +113,19 @@ class Context:
                                                  sd.ctypes.data if sd is not None else None,
                                                  wt.ctypes.data if wt is not None else None))
         return {"streak": st, "steady": sd, "weight": wt}
+
+    def components(self):
+        """Per-pixel sums of the enabled film components: {"depth": [H][W], "positions",
+        "normals": [H][W][3]} (None for a component the film does not have)."""
+        sc = self.scene
+        H, W = sc.height, sc.width
+        c = sc.components
+        d = np.empty((H, W), np.float64) if c & S.COMP_DEPTH else None
+        p = np.empty((H, W, 3), np.float64) if c & S.COMP_POSITIONS else None
+        n = np.empty((H, W, 3), np.float64) if c & S.COMP_NORMALS else None
+        ptr = lambda a: a.ctypes.data if a is not None else None
+        _abi.check(_abi.lib().tr_get_film_components(self.h, ptr(d), ptr(p), ptr(n)))
+        return {"depth": d, "positions": p, "normals": n}
 
     def film_into(self, streak=None, steady=None, weight=None):
         """tr_get_film into caller-provided (e.g. pinned) float64 host arrays."""
@@ -429,10 +442,13 @@ class StreakCameraFilm:
 
     bounce_films = 0
 
-    def __init__(self, w, h, t, exposure, camera_unwarp=False, filter=None):
+    def __init__(self, w, h, t, exposure, camera_unwarp=False, filter=None, comp=1):
+        """comp: FilmComponents bits (1 radiance | 2 depth | 8 positions | 16 normals); the
+        variance bit (4) is ignored, as the reference's Film keeps no variance image."""
         self.width, self.height, self.time_resolution = int(w), int(h), int(t)
         self.exposure = float(exposure)
         self.camera_unwarp = bool(camera_unwarp)
+        self.components = int(comp) & (S.COMP_DEPTH | S.COMP_POSITIONS | S.COMP_NORMALS)
         self.offset = 0.0
         self.streak = self.steady = self.weight = None
         self._ctx = None
@@ -465,8 +481,8 @@ class MultibounceStreakFilm(StreakCameraFilm):
     ``bounce_streak``/``bounce_steady``/``bounce_weight`` hold the per-bounce sums and
     ``steady`` the base film's image of all samples."""
 
-    def __init__(self, w, h, t, exposure, nb_bounces, filter=None, camera_unwarp=False):
-        super().__init__(w, h, t, exposure, camera_unwarp, filter)
+    def __init__(self, w, h, t, exposure, nb_bounces, filter=None, camera_unwarp=False, comp=1):
+        super().__init__(w, h, t, exposure, camera_unwarp, filter, comp)
         if not 1 <= int(nb_bounces) <= 32:
             raise ValueError("nb_bounces must be in [1, 32]")
         self.bounce_films = int(nb_bounces)
@@ -530,6 +546,7 @@ class TransientRenderer:
                         world._medium, integrator.seed)
         scene.camera_unwarp = int(film.camera_unwarp)
         scene.bounce_films = int(film.bounce_films)
+        scene.components = int(film.components)
         ctx = Context(scene, self.device)
         ctx.render(0, scene.spp)
         f = ctx.film()
@@ -539,6 +556,8 @@ class TransientRenderer:
             film.bounce_streak = np.stack([x["streak"] for x in b])
             film.bounce_steady = np.stack([x["steady"] for x in b])
             film.bounce_weight = np.stack([x["weight"] for x in b])
+        if film.components:
+            film.component_sums = ctx.components()
         film._ctx = ctx
         if name:
             ctx.write(name)

@@ -46,6 +46,7 @@ LIGHT_POINT = 0
 LIGHT_RECT = 1
 
 FLAG_ORTHONORMAL_FRAME = 1
+COMP_DEPTH, COMP_POSITIONS, COMP_NORMALS = 2, 8, 16     # FilmComponents bits (FilmComponents.h)
 
 
 @dataclasses.dataclass
@@ -133,6 +134,7 @@ class Scene:
     flags: int = 0            # FLAG_ORTHONORMAL_FRAME: Lambertian sampling in an orthonormal frame
     camera_unwarp: int = 0    # bin by path time minus the camera-to-first-surface distance
     bounce_films: int = 0     # N > 0: per-bounce streak films (multibounce streak film)
+    components: int = 0       # film components: COMP_DEPTH | COMP_POSITIONS | COMP_NORMALS
 
     # ---- flattened arrays (what the C ABI takes) -------------------------
     def flatten(self):

@@ -47,7 +47,7 @@ class CameraS(C.Structure):
 class FilmS(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("time_bins", C.c_uint32),
                 ("exposure", C.c_float), ("offset", C.c_float), ("camera_unwarp", C.c_uint32),
-                ("bounce_films", C.c_uint32)]
+                ("bounce_films", C.c_uint32), ("components", C.c_uint32)]
 
 
 class IntegratorS(C.Structure):
@@ -87,9 +87,9 @@ def lib():
         L.orc_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p,
                                 C.c_void_p]
         L.orc_trace_moller.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
-        L.orc_render_bounces.restype = C.c_int
-        L.orc_render_bounces.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
-                                         C.c_uint32, C.c_int] + [C.c_void_p] * 7
+        L.orc_render_ex.restype = C.c_int
+        L.orc_render_ex.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                    C.c_uint32, C.c_int] + [C.c_void_p] * 10
         L.orc_render.restype = C.c_int
         L.orc_render.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                  C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -148,7 +148,8 @@ class Oracle:
         pos, nv, uv, vv, fd = scene.camera.basis()
         cam = CameraS(f3(*pos), f3(*nv), f3(*uv), f3(*vv), float(fd))
         film = FilmS(scene.width, scene.height, scene.time_bins, scene.exposure, scene.offset,
-                     int(getattr(scene, "camera_unwarp", 0)), int(getattr(scene, "bounce_films", 0)))
+                     int(getattr(scene, "camera_unwarp", 0)), int(getattr(scene, "bounce_films", 0)),
+                     int(getattr(scene, "components", 0)))
         integ = IntegratorS(scene.max_bounces, scene.sqrt_spp, scene.incoming_samples, scene.flags, scene.seed)
         h = C.c_void_p()
         rc = lib().orc_create(C.byref(s), C.byref(cam), C.byref(film), C.byref(integ), C.byref(h))
@@ -189,10 +190,11 @@ class Oracle:
         return out
 
     def render(self, sample_begin=0, sample_count=None, window=None, nthreads=1,
-               streak=True, steady=True, weight=True, bounces=False):
+               streak=True, steady=True, weight=True, bounces=False, components=False):
         """Adds the camera samples into fresh full-frame films.  With bounces=True (the scene's
         film has bounce_films = N > 0) also returns the per-bounce films "bstreak"
-        [N][H][W][T][3], "bsteady" [N][H][W][3], "bweight" [N][H][W]."""
+        [N][H][W][T][3], "bsteady" [N][H][W][3], "bweight" [N][H][W]; with components=True the
+        per-pixel sums "depth" [H][W], "positions" and "normals" [H][W][3]."""
         sc = self.scene
         if sample_count is None:
             sample_count = sc.spp
@@ -205,10 +207,14 @@ class Oracle:
         bst = np.zeros((NB, H, W, T, 3), np.float64) if NB else None
         bsd = np.zeros((NB, H, W, 3), np.float64) if NB else None
         bwt = np.zeros((NB, H, W), np.float64) if NB else None
+        cd = np.zeros((H, W), np.float64) if components else None
+        cp = np.zeros((H, W, 3), np.float64) if components else None
+        cn = np.zeros((H, W, 3), np.float64) if components else None
         stats = np.zeros(8, np.uint64)
         ptr = lambda a: a.ctypes.data if a is not None else None
-        rc = lib().orc_render_bounces(self.h, x0, y0, x1, y1, sample_begin, sample_count, nthreads,
-                                      ptr(st), ptr(sd), ptr(wt), ptr(bst), ptr(bsd), ptr(bwt), stats.ctypes.data)
+        rc = lib().orc_render_ex(self.h, x0, y0, x1, y1, sample_begin, sample_count, nthreads,
+                                 ptr(st), ptr(sd), ptr(wt), ptr(bst), ptr(bsd), ptr(bwt), ptr(cd), ptr(cp), ptr(cn),
+                                 stats.ctypes.data)
         if rc != 0:
             raise ValueError("orc_render failed")
         out = {"streak": st, "steady": sd, "weight": wt,
@@ -216,6 +222,8 @@ class Oracle:
                                   "closest_tris", "shadow_nodes", "shadow_tris"], map(int, stats)))}
         if NB:
             out.update(bstreak=bst, bsteady=bsd, bweight=bwt)
+        if components:
+            out.update(depth=cd, positions=cp, normals=cn)
         return out
 
     def path_records(self, x, y, s, j=0, cap=256):

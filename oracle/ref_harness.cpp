@@ -26,7 +26,9 @@
  * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
  *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
  *   streak [H][W][T][3] (unless --no-streak), steady [H][W][3], weight [H][W], then with N
- *   bounce films bstreak [N][H][W][T][3], bsteady [N][H][W][3], bweight [N][H][W].
+ *   bounce films bstreak [N][H][W][T][3], bsteady [N][H][W][3], bweight [N][H][W], then with
+ *   components (`filmopts U N C`, C != 0) depth [H][W], positions [H][W][3], normals [H][W][3]
+ *   summed from each camera sample's record (Film::add_components, Film.h:127-145).
  *   Prints one JSON line with paths, seconds and paths/s on stdout.
  */
 #include <chrono>
@@ -69,10 +71,17 @@ public:
     bool keep_streak;
     bool unwarp;
     unsigned NB;
+    unsigned comps;
     std::vector<double> bstreak, bsteady, bweight;
-    AccumStreakFilm(unsigned w, unsigned h, unsigned t, Real exp_, Real off, bool ks, bool uw, unsigned nb)
+    std::vector<double> cdepth, cpos, cnorm;
+    AccumStreakFilm(unsigned w, unsigned h, unsigned t, Real exp_, Real off, bool ks, bool uw, unsigned nb, unsigned cm)
         : Base(w, h, t, exp_, uw, nullptr), W(w), H(h), T(t), exposure(exp_), offset(off),
-          keep_streak(ks), unwarp(uw), NB(nb) {
+          keep_streak(ks), unwarp(uw), NB(nb), comps(cm) {
+        if (cm) {
+            cdepth.assign((size_t)h * w, 0.0);
+            cpos.assign((size_t)h * w * 3, 0.0);
+            cnorm.assign((size_t)h * w * 3, 0.0);
+        }
         if (off > 0) this->set_offset(off);
         if (ks) streak.assign((size_t)h * w * t * 3, 0.0);
         steady.assign((size_t)h * w * 3, 0.0);
@@ -111,6 +120,13 @@ public:
         }
         for (unsigned b = 0; b < NB; ++b)
             if (present[b]) bweight[(size_t)b * npix + pix] += sample.weight;
+        if (comps) {                                     /* Film::add_components, Film.h:127-145 */
+            cdepth[pix] += (double)(rec.distance * sample.weight);
+            for (int c = 0; c < 3; ++c) {
+                cpos[pix * 3 + c] += (double)(rec.pos[c] * sample.weight);
+                cnorm[pix * 3 + c] += (double)(rec.normal[c] * sample.weight);
+            }
+        }
     }
     void write(const char*) override {}
 };
@@ -131,7 +147,7 @@ int main(int argc, char** argv) {
     std::ifstream in(argv[1]);
     if (!in) fail("cannot open scene");
     std::string tag;
-    unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1, unwarp = 0, nbounce = 0;
+    unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1, unwarp = 0, nbounce = 0, comps = 0;
     Real exposure = 0, offset = 0, fov = 40;
     unsigned long long seed = 1;
     Vector3 cpos, cfoc, cup;
@@ -142,7 +158,7 @@ int main(int argc, char** argv) {
     std::vector<std::string> light_lines;
     while (in >> tag) {
         if (tag == "film") { in >> W >> H >> T >> exposure >> offset; }
-        else if (tag == "filmopts") { in >> unwarp >> nbounce; }
+        else if (tag == "filmopts") { in >> unwarp >> nbounce >> comps; }
         else if (tag == "camera") {
             float a[9]; for (float& v : a) in >> v; in >> fov;
             cpos = Vector3(a[0], a[1], a[2]); cfoc = Vector3(a[3], a[4], a[5]); cup = Vector3(a[6], a[7], a[8]);
@@ -203,7 +219,7 @@ int main(int argc, char** argv) {
     Real fovr = M_PI / 180. * fov / 2;                                   /* bunnykiller.cpp:1156-1161 */
     Real fd = 1. / tan(fovr);
     PinholeCamera camera(cpos, cfoc, cup, fd);
-    AccumStreakFilm film(W, H, T, exposure, offset, keep_streak, unwarp != 0, nbounce);
+    AccumStreakFilm film(W, H, T, exposure, offset, keep_streak, unwarp != 0, nbounce, comps);
     StratifiedSampler sampler(W, H, sqrt_spp, true);
     TransientRenderer<3, Radiance, RadianceAttenuation> engine(nullptr, false);
     Random::StdRNG.seed(seed);                                           /* bunnykiller.cpp:1794 */
@@ -238,6 +254,11 @@ int main(int argc, char** argv) {
         fwrite(film.bstreak.data(), sizeof(double), film.bstreak.size(), out);
         fwrite(film.bsteady.data(), sizeof(double), film.bsteady.size(), out);
         fwrite(film.bweight.data(), sizeof(double), film.bweight.size(), out);
+    }
+    if (comps) {
+        fwrite(film.cdepth.data(), sizeof(double), film.cdepth.size(), out);
+        fwrite(film.cpos.data(), sizeof(double), film.cpos.size(), out);
+        fwrite(film.cnorm.data(), sizeof(double), film.cnorm.size(), out);
     }
     fclose(out);
     FILE* tty = fopen("/dev/stderr", "w");

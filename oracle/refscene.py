@@ -38,8 +38,9 @@ def write_scene(scene, path, seed=None):
     lines = []
     lines.append(f"film {scene.width} {scene.height} {scene.time_bins} {scene.exposure!r} {scene.offset!r}")
     uw, nb = int(getattr(scene, "camera_unwarp", 0)), int(getattr(scene, "bounce_films", 0))
-    if uw or nb:
-        lines.append(f"filmopts {uw} {nb}")
+    cm = int(getattr(scene, "components", 0))
+    if uw or nb or cm:
+        lines.append(f"filmopts {uw} {nb} {cm}")
     c = scene.camera
     lines.append("camera " + " ".join(repr(float(v)) for v in (*c.position, *c.focus, *c.up)) + f" {c.fov_deg!r}")
     lines.append(f"integrator {scene.max_bounces} {scene.sqrt_spp} {scene.incoming_samples} "
@@ -99,6 +100,12 @@ def render(scene, seed=None, rows=None, keep_streak=True, workdir=None):
         extra["bsteady"] = raw[off:off + NB * H * W * 3].reshape(NB, H, W, 3)
         off += NB * H * W * 3
         extra["bweight"] = raw[off:off + NB * H * W].reshape(NB, H, W)
+    if int(getattr(scene, "components", 0)):
+        extra["depth"] = raw[off:off + H * W].reshape(H, W)
+        off += H * W
+        extra["positions"] = raw[off:off + H * W * 3].reshape(H, W, 3)
+        off += H * W * 3
+        extra["normals"] = raw[off:off + H * W * 3].reshape(H, W, 3)
     if workdir is None:
         for p in (sp, op):
             os.remove(p)

@@ -627,8 +627,14 @@ void orc_ggx_eval_cos(const float* kd, float alpha, const float* n, const float*
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
 }
 
-/* One random walk; appends its splat records (at most max_bounces) to rec. */
-static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc, srec* rec, pstats* st) {
+/* World::Li's record of a camera ray: closest surface distance (FLT_MAX when none), position
+ * and normal of that point (zero when none). */
+typedef struct { float t; v3 pos, n; } camrec;
+
+/* One random walk; appends its splat records (at most max_bounces) to rec; fills cr (if not
+ * NULL) with the camera ray's record. */
+static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc, srec* rec, pstats* st,
+                      camrec* cr) {
     const orc_film* F = &x->film;
     const int medium = x->med.enabled != 0;
     v3 sig_s = ld3(x->med.sigma_s), sig_t = add(ld3(x->med.sigma_a), ld3(x->med.sigma_s));
@@ -637,6 +643,7 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
     float total_time = (float)F->time_bins * F->exposure + F->offset;
     uint32_t maxb = x->integ.max_bounces;
     const int unwarp = F->camera_unwarp != 0;
+    const int need_cam = unwarp || F->components != 0;   /* camera ray traced to any distance */
     const int bounce_films = F->bounce_films != 0;
     /* World::Li's camera-ray record distance (World.h:749-766): the closest surface along the
      * camera ray, FLT_MAX when there is none (Ray.h:74-84) */
@@ -652,13 +659,18 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
         wray r;
         /* with camera unwarp the camera ray is traced to infinity (its surface distance is the
          * unwarp offset); surface vs medium below is decided by h.t < dsamp either way */
-        wray_setup(&r, org, dir, SIGMA_VIS, (medium && !(unwarp && depth == 0)) ? dsamp : INFINITY);
+        wray_setup(&r, org, dir, SIGMA_VIS, (medium && !(need_cam && depth == 0)) ? dsamp : INFINITY);
         orc_hit h;
         st->closest++;
         uint32_t cv = 0, ct = 0;
         int hit = trace1(x, &r, 0, &h, &cv, &ct);
         st->c_nodes += cv; st->c_tris += ct;
         if (depth == 0 && hit) cam_dist = h.t;
+        if (depth == 0 && cr) {
+            cr->t = hit ? h.t : FLT_MAX;
+            cr->pos = hit ? add(org, muls(dir, h.t)) : mk(0.0f, 0.0f, 0.0f);
+            cr->n = hit ? x->ng[h.prim_id] : mk(0.0f, 0.0f, 0.0f);
+        }
         int surface = hit && (!medium || h.t < dsamp);
         if (!medium && !hit) break;
         float dist, pd;
@@ -862,7 +874,7 @@ int orc_path_records(const orc_ctx* x, uint32_t px, uint32_t py, uint64_t s, uin
     srec rec[256];
     pstats st;
     memset(&st, 0, sizeof(st));
-    int n = trace_path(x, o, d, &r, 1.0f / (float)x->integ.incoming_samples, rec, &st);
+    int n = trace_path(x, o, d, &r, 1.0f / (float)x->integ.incoming_samples, rec, &st, NULL);
     if (n > cap) n = cap;
     for (int i = 0; i < n; ++i) {
         bins[i] = rec[i].bin;
@@ -875,6 +887,7 @@ typedef struct {
     const orc_ctx* x; uint32_t x0, x1, y0, y1; uint64_t s0; uint32_t ns;
     double *streak, *steady, *weight;
     double *bstreak, *bsteady, *bweight;
+    double *cdepth, *cpos, *cnorm;
     uint32_t row_begin, row_step;
     uint64_t paths; pstats st;
 } job;
@@ -900,8 +913,16 @@ static void* render_rows(void* arg) {
                 for (uint32_t j = 0; j < ninc; ++j) {
                     pcg r;
                     path_rng(x, &r, pixel, s, j);
-                    int n = trace_path(x, o, d, &r, inv_inc, rec, &J->st);
+                    camrec cr;
+                    int n = trace_path(x, o, d, &r, inv_inc, rec, &J->st, j == 0 ? &cr : NULL);
                     J->paths++;
+                    if (j == 0) {
+                        if (J->cdepth) J->cdepth[pixel] += (double)cr.t;
+                        for (int c = 0; c < 3; ++c) {
+                            if (J->cpos) J->cpos[(size_t)pixel * 3 + c] += (double)comp(cr.pos, c);
+                            if (J->cnorm) J->cnorm[(size_t)pixel * 3 + c] += (double)comp(cr.n, c);
+                        }
+                    }
                     for (int i = 0; i < n; ++i) {
                         const int inside = rec[i].bin != BIN_OUTSIDE;
                         for (int c = 0; c < 3; ++c) {
@@ -938,6 +959,15 @@ int orc_render_bounces(const orc_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, 
                        uint64_t sample_begin, uint32_t sample_count, int nthreads,
                        double* streak, double* steady, double* weight,
                        double* bstreak, double* bsteady, double* bweight, uint64_t* stats) {
+    return orc_render_ex(x, x0, y0, x1, y1, sample_begin, sample_count, nthreads, streak, steady, weight,
+                         bstreak, bsteady, bweight, NULL, NULL, NULL, stats);
+}
+
+int orc_render_ex(const orc_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                  uint64_t sample_begin, uint32_t sample_count, int nthreads,
+                  double* streak, double* steady, double* weight,
+                  double* bstreak, double* bsteady, double* bweight,
+                  double* cdepth, double* cpos, double* cnorm, uint64_t* stats) {
     if (x->film.bounce_films > 64) return 1;
     if (x1 > x->film.width || y1 > x->film.height || x0 > x1 || y0 > y1) return 1;
     if (x->integ.max_bounces > 255) return 1;
@@ -950,6 +980,7 @@ int orc_render_bounces(const orc_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, 
         J[i].s0 = sample_begin; J[i].ns = sample_count;
         J[i].streak = streak; J[i].steady = steady; J[i].weight = weight;
         J[i].bstreak = bstreak; J[i].bsteady = bsteady; J[i].bweight = bweight;
+        J[i].cdepth = cdepth; J[i].cpos = cpos; J[i].cnorm = cnorm;
         J[i].row_begin = (uint32_t)i; J[i].row_step = (uint32_t)nthreads;
         J[i].paths = 0; memset(&J[i].st, 0, sizeof(pstats));
     }

@@ -60,6 +60,7 @@ typedef struct orc_film {
     uint32_t width, height, time_bins; float exposure; float offset;
     uint32_t camera_unwarp;   /* bin by path time minus the camera-to-first-surface distance */
     uint32_t bounce_films;    /* N > 0: per-bounce streak films (MultibounceStreakFilm)       */
+    uint32_t components;      /* FilmComponents bits: 2 depth, 8 positions, 16 normals        */
 } orc_film;
 typedef struct orc_integrator { uint32_t max_bounces, sqrt_spp, incoming_samples, flags; uint64_t seed; } orc_integrator;
 #define ORC_FLAG_ORTHONORMAL_FRAME 1u
@@ -105,6 +106,16 @@ int orc_render_bounces(const orc_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1
                        uint64_t sample_begin, uint32_t sample_count, int nthreads,
                        double* streak, double* steady, double* weight,
                        double* bstreak, double* bsteady, double* bweight, uint64_t* stats);
+
+/* As orc_render_bounces, plus the film components of Film::add_components (Film.h:127-145)
+ * summed per camera sample (any may be NULL): depth [H][W] = distance to the closest surface
+ * along the camera ray (FLT_MAX when none), positions [H][W][3] and normals [H][W][3] of that
+ * surface point (zero when none) -- World::Li's record (World.h:749-766).                     */
+int orc_render_ex(const orc_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                  uint64_t sample_begin, uint32_t sample_count, int nthreads,
+                  double* streak, double* steady, double* weight,
+                  double* bstreak, double* bsteady, double* bweight,
+                  double* depth, double* positions, double* normals, uint64_t* stats);
 
 /* One path's splat records, for per-path comparisons: returns the number of records
  * (<= cap) of path (pixel x, y, camera sample s, incoming sample j). */

@@ -8,9 +8,10 @@ container); the committed .npz files are what the tests read.
 
     python tests/golden/make_golden.py [names]    # writes tests/golden/ref_*.npz
 
-`unwarp` and `bounces` exercise the film options: the camera unwarp of StreakCameraFilm and
-three per-bounce films of MultibounceStreakFilm (their per-bounce streaks are stored as one
-film of 3H rows, their weights and the base steady image beside them).
+`unwarp`, `bounces` and `components` exercise the film options: the camera unwarp of
+StreakCameraFilm, three per-bounce films of MultibounceStreakFilm (their per-bounce streaks are
+stored as one film of 3H rows, their weights and the base steady image beside them) and the
+depth / position / normal components of Film (per-pixel sums beside the streak).
 """
 import os
 import sys
@@ -43,7 +44,11 @@ def golden_scenes():
     b = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
     b.lights[0].position = (0.5, 0.8, 0.5)
     b.bounce_films = 3
-    return {"cornell": c, "medium": m, "arealight": a, "unwarp": u, "bounces": b}
+    k = S.medium(width=12, height=12, time_bins=48, exposure=0.15, sqrt_spp=8, incoming_samples=1,
+                 max_bounces=12)
+    k.lights[0].position = (0.5, 0.8, 0.5)
+    k.components = S.COMP_DEPTH | S.COMP_POSITIONS | S.COMP_NORMALS
+    return {"cornell": c, "medium": m, "arealight": a, "unwarp": u, "bounces": b, "components": k}
 
 
 def main(names=None):
@@ -66,6 +71,11 @@ def main(names=None):
             sd = np.array([r["steady"] for r in runs])
             extra = dict(bweight_mean=bw.mean(0), bweight_se=bw.std(0, ddof=1) / np.sqrt(K),
                          steady_mean=sd.mean(0), steady_se=sd.std(0, ddof=1) / np.sqrt(K))
+        if sc.components:
+            for key in ("depth", "positions", "normals"):
+                arr = np.array([r[key] for r in runs])
+                extra[key + "_mean"] = arr.mean(0)
+                extra[key + "_se"] = arr.std(0, ddof=1) / np.sqrt(K)
         out = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}.npz")
         np.savez_compressed(out, mean=mean.astype(np.float32), se=se.astype(np.float32), energy=energy, k=K, **extra)
         print(name, out, "energy %.4f +- %.4f" % (energy.mean(), energy.std(ddof=1) / np.sqrt(K)))

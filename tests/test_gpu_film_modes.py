@@ -132,3 +132,50 @@ def test_batch_camera_unwarp_and_bounce_films(gpu):
     with gpu.Context(sc) as c:
         with pytest.raises(gpu.TransientError):
             gpu.Batch([c])
+
+
+@pytest.mark.parametrize("name", ["cornell", "medium"])
+def test_film_components_match_oracle(gpu, oracle_lib, name):
+    """Depth / positions / normals (Film::add_components): one camera-ray record per camera
+    sample, the closest surface at any distance (in the medium scene too); FLT_MAX depth and
+    zero position / normal where the camera ray leaves the open room."""
+    sc = _scenes()[name]
+    sc.components = S.COMP_DEPTH | S.COMP_POSITIONS | S.COMP_NORMALS
+    sc.camera_unwarp = 1 if name == "medium" else 0
+    sc.bounce_films = 2 if name == "medium" else 0
+    with gpu.Context(sc) as c:
+        c.render(0, 12)
+        f = c.film()
+        comp = c.components()
+    o = oracle_lib.Oracle(sc).render(sample_count=12, nthreads=8, components=True)
+    _same(f["streak"], o["streak"])
+    for key in ("depth", "positions", "normals"):
+        # FP64 sums of identical FP32 records, in another order (atomics)
+        assert np.allclose(comp[key], o[key], rtol=1e-12, atol=1e-9), key
+    assert (comp["depth"] > 0).all()
+
+
+def test_film_components_written_and_batched(gpu, tmp_path):
+    scs = list(_scenes().values())
+    for sc in scs:
+        sc.components = S.COMP_DEPTH | S.COMP_NORMALS
+    with gpu.Context(scs[0]) as c:
+        c.render(0, 3)
+        c.write(str(tmp_path / "frame"))
+        single = c.components()
+        w = c.film(streak=False, steady=False)["weight"]
+    names = set(os.listdir(tmp_path))
+    assert {"frame.hdr", "frame_depth.hdr", "frame_normals.raw"} <= names and "frame_positions.raw" not in names
+    raw = np.fromfile(tmp_path / "frame_normals.raw", np.float32).reshape(scs[0].height, scs[0].width, 3)
+    assert np.allclose(raw, (single["normals"] / w[:, :, None]).astype(np.float32), rtol=1e-6, atol=1e-7)
+    ctxs = [gpu.Context(sc) for sc in scs]
+    try:
+        with gpu.Batch(ctxs) as B:
+            B.set_config(capacity=65536)
+            B.render(0, 3)
+        batched = ctxs[0].components()
+    finally:
+        for c in ctxs:
+            c.close()
+    for key in ("depth", "normals"):
+        assert np.allclose(batched[key], single[key], rtol=1e-12, atol=1e-9)

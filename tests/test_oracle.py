@@ -152,6 +152,26 @@ def test_oracle_bounce_films_match_reference(oracle_lib):
     assert (g["bweight_mean"] <= 64 + 1e-9).all()
 
 
+def test_oracle_film_components_match_reference(oracle_lib):
+    """Depth / position / normal components (Film::add_components, Film.h:127-145) from World::Li's
+    camera-ray record (World.h:749-766): the closest surface at any distance, also in a medium.
+    Per-pixel sums of 64 samples agree with the reference within 4 standard errors (plus the
+    few-ulp hit-distance difference of the two intersection tests)."""
+    sc = _golden_scene("components")
+    g = _golden("components")
+    o = oracle_lib.Oracle(sc)
+    K = len(g["energy"])
+    runs = [o.render(sample_begin=64 * k, sample_count=64, nthreads=4, components=True) for k in range(K)]
+    films = np.array([r["streak"] for r in runs])
+    r = compare_to_golden(films, g)
+    assert r["frac_z3"] < 0.02 and abs(r["mean_z"]) < 0.1 and abs(r["energy_z"]) < 4.0, r
+    for key in ("depth", "positions", "normals"):
+        arr = np.array([r[key] for r in runs])
+        se = np.sqrt((arr.std(0, ddof=1) / np.sqrt(K)) ** 2 + g[key + "_se"] ** 2)
+        diff = np.abs(arr.mean(0) - g[key + "_mean"])
+        assert (diff <= 4.0 * se + 1e-5 * np.abs(g[key + "_mean"]) + 1e-6).all(), (key, float((diff / (se + 1e-12)).max()))
+
+
 def test_oracle_reference_harness_live(oracle_lib):
     """When the reference sources are present, rebuild and rerun the reference harness and
     check it still reproduces the committed golden statistics."""
