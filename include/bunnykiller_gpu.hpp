@@ -174,13 +174,17 @@ class GpuTransientRenderer : public TransientRenderer<D, Radiance, RadianceAtten
     int m_device;
 
 public:
+    // time_sampling: the reference's TransientRenderer(f_log, time_sampling) argument
+    // (TransientRenderer.h:61-62, "-time-sampling"), i.e. TR_FLAG_TIME_SAMPLING.
     GpuTransientRenderer(FILE* f_log, const SceneCapture& scene, const tr_camera& camera, unsigned max_bounces,
-                         unsigned sqrt_spp, unsigned incoming_samples, uint64_t seed, int device = 0)
-        : Base(f_log, false), m_scene(scene), m_camera(camera), m_integrator{}, m_device(device) {
+                         unsigned sqrt_spp, unsigned incoming_samples, uint64_t seed, int device = 0,
+                         bool time_sampling = false)
+        : Base(f_log, time_sampling), m_scene(scene), m_camera(camera), m_integrator{}, m_device(device) {
         m_integrator.max_bounces = max_bounces;
         m_integrator.sqrt_spp = sqrt_spp;
         m_integrator.incoming_samples = incoming_samples;
         m_integrator.seed = seed;
+        if (time_sampling) m_integrator.flags |= TR_FLAG_TIME_SAMPLING;
     }
 
     void render(const char* name, World<D, Radiance>& world, Integrator<D, Radiance, RadianceAttenuation>* integrator,

@@ -149,6 +149,17 @@ typedef struct tr_integrator {
  * densities by MIS) requires this flag, as does the plain render it is compared against. */
 #define TR_FLAG_ORTHONORMAL_FRAME 1u
 
+/* Time sampling ("-time-sampling": TransientRenderer(f_log, true) ->
+ * BidirectionalPathTracing::set_mode(SamplingMode::Transient),
+ * src/Integrator/BidirectionalPathTracing.h:189-206).  Each path draws one light point; free
+ * flights in the medium have the rate 4 / (time_bins * exposure) instead of the mean extinction;
+ * walks end when their time passes the film's (no Russian roulette); medium directions come
+ * from the time-angular sampler towards the light point (SamplingTechniques.h TimeAngular,
+ * BidirectionalPathTracing.h:342-431), falling back to the phase function.  The reference's
+ * sampler density and weights are reproduced as they are, including its rare huge weights
+ * (inverted time bounds), so films match the reference's distribution, heavy tail included. */
+#define TR_FLAG_TIME_SAMPLING 2u
+
 /* ---- ray-batch interface (correctness batch of World::first_intersection / intersects) --- */
 
 /* One ray = 8 floats: origin xyz, tnear, direction xyz, tfar.                               */
@@ -244,7 +255,7 @@ tr_status tr_trace_rays_device(tr_ctx* ctx, const float* d_rays, uint32_t n, int
  * cannot afford cudaMalloc's implicit device-wide synchronisation in the middle of a frame.
  * tr_render may grow its path buffers with cudaMalloc; this entry
  * point instead keeps the per-path state of the wavefront in one fixed array compiled into
- * the library (24.3 MiB per GPU that loads the library, held until the process exits).
+ * the library (25.3 MiB per GPU that loads the library, held until the process exits).
  * It adds camera samples [sample_begin, sample_begin + sample_count) of the pixel window
  * [x0,x1) x [y0,y1) to the context's film, exactly as tr_render_region does, asynchronously
  * on `stream` (cudaStream_t as void*, NULL = the context's stream).

@@ -88,7 +88,8 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     if (it->sqrt_spp == 0 || it->incoming_samples == 0)
         return fail(TR_ERR_INVALID_ARGUMENT, "sqrt_spp and incoming_samples must be >= 1");
     if (it->max_bounces > kMaxBounces) return fail(TR_ERR_INVALID_ARGUMENT, "max_bounces must be <= 63");
-    if (it->flags & ~TR_FLAG_ORTHONORMAL_FRAME) return fail(TR_ERR_INVALID_ARGUMENT, "unknown integrator flags");
+    if (it->flags & ~(TR_FLAG_ORTHONORMAL_FRAME | TR_FLAG_TIME_SAMPLING))
+        return fail(TR_ERR_INVALID_ARGUMENT, "unknown integrator flags");
     if (!std::isfinite(c->focal_distance)) return fail(TR_ERR_INVALID_ARGUMENT, "camera focal distance not finite");
     return TR_OK;
 }
@@ -127,6 +128,8 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.rec_n = x->alloc<uint8_t>(capacity);
     drop(w.cam_dist);
     w.cam_dist = x->alloc<float>(capacity);
+    drop(w.target);
+    w.target = (x->integ.flags & TR_FLAG_TIME_SAMPLING) ? x->alloc<float4>(capacity) : nullptr;
     if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = x->alloc<unsigned long long>(8);
@@ -434,6 +437,9 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
                                  s->medium.sigma_a[2] + s->medium.sigma_s[2]);
             for (int k = 0; k < 3; ++k) { sc.sig_s[k] = s->medium.sigma_s[k]; sc.sig_t[k] = trd::comp(st, k); }
             sc.lambda = trd::avg3(st);
+            // time sampling: free flights at the rate m_avg_nb_vertices_path (4) per film
+            // duration (BidirectionalPathTracing.h:189-206, :240-307)
+            if (it->flags & TR_FLAG_TIME_SAMPLING) sc.lambda = 4.0f / ((float)f->time_bins * f->exposure);
             sc.g = s->medium.g;
         }
 
@@ -714,7 +720,8 @@ constexpr size_t kNaBytes = 7 * kNaF4                                           
                           + na_align(kNaSlots)                                    // records per slot
                           + na_align(sizeof(uint32_t) * trk::kCounters)           // queue counters
                           + na_align(sizeof(unsigned long long) * 8)              // ray / splat counts
-                          + na_align(sizeof(float) * kNaSlots);                   // camera distances
+                          + na_align(sizeof(float) * kNaSlots)                    // camera distances
+                          + kNaF4;                                                // light points (time sampling)
 
 // The scratch itself.  Its name is only a host-side handle: host code must use the device
 // address from cudaGetSymbolAddress, never &g_noalloc_scratch.
@@ -783,6 +790,7 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
         w.counters = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * trk::kCounters));
         w.stats = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 8));
         w.cam_dist = reinterpret_cast<float*>(take(sizeof(float) * kNaSlots));
+        w.target = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
         w.capacity = (uint32_t)kNaSlots;
         // what the kernels expect to start at zero: queue counters / fetch cursors and the
         // ray counters (records-per-slot are reset by the ray generation kernel)

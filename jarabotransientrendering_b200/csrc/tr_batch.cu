@@ -170,6 +170,10 @@ void ensure_batch_wave(tr_batch* b, uint32_t capacity) {
     w.rec_n = b->alloc<uint8_t>(capacity);
     b->drop(w.cam_dist);
     w.cam_dist = b->alloc<float>(capacity);
+    b->drop(w.target);
+    bool tsm = false;
+    for (tr_ctx* x : b->ctx) tsm = tsm || (x->integ.flags & TR_FLAG_TIME_SAMPLING) != 0;
+    w.target = tsm ? b->alloc<float4>(capacity) : nullptr;
     if (!w.counters) w.counters = b->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = b->alloc<unsigned long long>(8);

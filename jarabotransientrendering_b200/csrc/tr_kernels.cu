@@ -154,6 +154,22 @@ __global__ void __launch_bounds__(256) k_raygen(const __grid_constant__ Params p
     const SceneDev& sc = kMulti ? SS->scene : p.scene;
     Pcg r;
     pcg_seed(r, seed + (unsigned long long)(j + 1) * kGolden64, cam_id(pixel, s));
+    if ((kMulti ? SS->flags : p.flags) & kFlagTimeSampling) {
+        // time sampling: one light point per path, the target of the time-angular sampler
+        // (World::sample_light + LightSource::sample, BidirectionalPathTracing.h:1107-1113;
+        // PointLightSource.h:174-183, RectangularAreaLightSource.h:252-276)
+        const float xl = pcg_float(r);
+        uint32_t lsel = (uint32_t)(xl * (float)sc.num_lights);
+        if (lsel >= sc.num_lights) lsel = sc.num_lights - 1;
+        const float4* L = sc.lights + 5 * lsel;
+        const float4 L0 = __ldg(L);
+        f3 tg = mk(L0.x, L0.y, L0.z);
+        if (__float_as_uint(L0.w) == 1u) {
+            const float xu = pcg_float(r), xv = pcg_float(r);
+            tg = (tg + f3of(__ldg(L + 2)) * xu) + f3of(__ldg(L + 3)) * xv;
+        }
+        p.wave.target[i] = make_float4(tg.x, tg.y, tg.z, 0.0f);
+    }
     float dsamp = __int_as_float(0x7f800000);
     if (sc.medium) dsamp = -tr_log(pcg_float(r)) / sc.lambda;
 
@@ -259,7 +275,75 @@ __device__ __forceinline__ float hg_eval(float g, float cs) {
     return ((1.0f - gg) * kInv4Pi) / (b * sqrtf(b));
 }
 
-template <bool kGuided, bool kMulti>
+// The vector-to-vector matrix of Moeller & Hughes ("Efficiently building a matrix to rotate
+// one vector to another", JGT 4(4), 1999) from +y to `to`, applied to d and normalised, as
+// VectorN::transform_matrix_to (VectorN.h:427-521) builds it.  The time-angular sampler passes
+// the unnormalised target offset as `to` (BidirectionalPathTracing.h:392), for which the matrix
+// is not a rotation; the same construction keeps the sampled directions those of the reference.
+__device__ __forceinline__ f3 mh_from_y(f3 to, f3 d) {
+    // (0,1,0) x to and (0,1,0) . to, every product written out so zero signs match a plain
+    // evaluation of the cross and dot products
+    const f3 v = mk(1.0f * to.z - 0.0f * to.y, 0.0f * to.x - 0.0f * to.z, 0.0f * to.y - 1.0f * to.x);
+    const float e = (0.0f * to.x + 1.0f * to.y) + 0.0f * to.z;
+    float m[3][3];
+    if (fabsf(e) > 1.0f - 1e-4f) {
+        // near-parallel: reflections through the coordinate axis least aligned with +y (z)
+        const f3 u = mk(0.0f, -1.0f, 1.0f);                      // z - y
+        const f3 w = mk(0.0f - to.x, 0.0f - to.y, 1.0f - to.z);  // z - to
+        const float c1 = 2.0f / dot(u, u), c2 = 2.0f / dot(w, w);
+        const float c3 = (c1 * c2) * dot(u, w);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                m[i][j] = ((-c1 * comp(u, i)) * comp(u, j) - (c2 * comp(w, i)) * comp(w, j)) + (c3 * comp(w, i)) * comp(u, j);
+                if (i == j) m[i][j] += 1.0f;
+            }
+    } else {
+        const float h = 1.0f / (1.0f + e);
+        const float hvx = h * v.x, hvz = h * v.z, hvxy = hvx * v.y, hvxz = hvx * v.z, hvyz = hvz * v.y;
+        m[0][0] = e + hvx * v.x; m[0][1] = hvxy - v.z;           m[0][2] = hvxz + v.y;
+        m[1][0] = hvxy + v.z;    m[1][1] = e + (h * v.y) * v.y;   m[1][2] = hvyz - v.x;
+        m[2][0] = hvxz - v.y;    m[2][1] = hvyz + v.x;           m[2][2] = e + hvz * v.z;
+    }
+    const f3 r = mk((m[0][0] * d.x + m[0][1] * d.y) + m[0][2] * d.z, (m[1][0] * d.x + m[1][1] * d.y) + m[1][2] * d.z,
+                    (m[2][0] * d.x + m[2][1] * d.y) + m[2][2] * d.z);
+    return normalize(r);
+}
+
+// One direction of the time-angular sampler (SamplingTechniques.h:170-247 TimeAngular;
+// BidirectionalPathTracing.h:365-405 with p_ts = 1): the time t is uniform on the sampler's
+// bounds [t_a, t_b], theta is the angle to the target at which a scattering after `r` reaches
+// the target at time t, phi is uniform.  Operand types follow the reference (the cosine in
+// double, stored as a float; float products).  When the bounds are inverted (the current delay
+// exceeds 2r) the cosine clamps to -1, theta is the float nearest pi (above pi), its sine the
+// small negative number pi - (float)pi, and the density dtdtheta / (t_b - t_a) / (2 pi) a small
+// positive number; the caller keeps the direction when that density is >= 1e-5 (rare huge
+// weights, as in the reference).  e, e2: the theta and phi draws.
+struct TaSample { f3 nd; float ph; float pa; };
+__device__ __noinline__ TaSample time_angular_sample(f3 l, float mod, float r, float t_a, float t_b, float e, float e2,
+                                                     f3 dir, float g) {
+    const float t = e * (t_b - t_a) + t_a;
+    float ct = (float)((((double)(mod * mod) + ((2.0 * (double)t) * (double)r)) - (double)(t * t)) /
+                       ((2.0 * (double)r) * (double)mod));
+    ct = ct < -1.0f ? -1.0f : (ct > 1.0f ? 1.0f : ct);
+    constexpr float kSinFloatPi = (float)(3.14159265358979323846 - (double)3.14159265358979323846f);
+    const float st = ct == -1.0f ? kSinFloatPi : (float)sqrt(1.0 - (double)ct * (double)ct);
+    float sp2, cp2;
+    tr_sincos2pi(e2, &sp2, &cp2);
+    TaSample o;
+    o.nd = mh_from_y(l, mk(cp2 * st, ct, sp2 * st));
+    o.ph = hg_eval(g, dot(dir, o.nd));
+    const float dtdth = (float)((double)((mod * r) * st) /
+                                sqrt((double)(r * r + mod * mod) - ((2.0 * (double)r) * (double)mod) * (double)ct));
+    const float pdf_theta = dtdth / (t_b - t_a);
+    o.pa = (float)((double)pdf_theta / (2.0 * 3.14159265358979323846));
+    return o;
+}
+
+// kTimeSampling: compiled with the time-sampling branches (a launch whose context, or some
+// context of whose batch, has TR_FLAG_TIME_SAMPLING; the flag is still read per slot).
+template <bool kGuided, bool kMulti, bool kTimeSampling>
 __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p, int depth) {
     uint32_t n0 = p.batch.n_slots;
     if constexpr (kMulti) n0 = cur_batch(p).n_slots;
@@ -450,28 +534,65 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
                         }
                     }
                     if ((uint32_t)depth + 1u < max_bounces) {
-                        // ---- Russian roulette ----
+                        // ---- Russian roulette (none in time-sampling mode: the walk ends when
+                        // its time passes the film's, above) ----
                         const float albedo = surface ? avg3(kd)
                             : avg3(mk(sig_s.x / sig_t.x, sig_s.y / sig_t.y, sig_s.z / sig_t.z));
-                        if (kGuided && surface && !(pcg_float(rng) > albedo)) {
+                        const bool tsm = kTimeSampling && (flags & kFlagTimeSampling) != 0;
+                        const bool survive = tsm || !(pcg_float(rng) > albedo);
+                        const float prr = tsm ? 1.0f : albedo;
+                        if (kGuided && surface && survive) {
                             // ---- direction deferred to the learned proposal (k_guide) ----
                             want_guide = true;
                             gv[0] = make_uint4(__float_as_uint(pos.x), __float_as_uint(pos.y), __float_as_uint(pos.z),
                                                __float_as_uint(time));
                             gv[1] = make_uint4(__float_as_uint(dir.x), __float_as_uint(dir.y), __float_as_uint(dir.z),
-                                               __float_as_uint(albedo));
+                                               __float_as_uint(prr));
                             gv[2] = make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z),
                                                __float_as_uint(__ldg(&sc.tri_ng[id]).w));
                             gv[3] = make_uint4(__float_as_uint(nrm.x), __float_as_uint(nrm.y), __float_as_uint(nrm.z), slot);
-                        } else if ((!kGuided || !surface) && !(pcg_float(rng) > albedo)) {
+                        } else if ((!kGuided || !surface) && survive) {
                             // ---- outgoing direction ----
-                            const float x1 = pcg_float(rng), x2 = pcg_float(rng);
-                            float sp, cp;
-                            tr_sincos2pi(x1, &sp, &cp);
                             f3 fa, nd;
                             float pa;
                             bool alive = true;
-                            if (surface && ggx) {
+                            bool angular = false;
+                            float nds_first = 0.0f;
+                            if (tsm && !surface) {
+                                // time sampling in the medium: the next free flight r first
+                                // (generate_path, BidirectionalPathTracing.h:530-545), then the
+                                // time-angular sampler towards the path's light point with
+                                // probability 1 when its bounds leave at least one exposure
+                                // (:365-405), else (or when its density is < 1e-5) the phase
+                                // function (:408-418)
+                                nds_first = -tr_log(pcg_float(rng)) / lambda;
+                                const float4 tg = p.wave.target[slot];
+                                const f3 l = mk(tg.x, tg.y, tg.z) - pos;
+                                const float mod = sqrtf(dot(l, l));
+                                const float ta = mod + time;
+                                float t_a = ta, t_b = total_time;
+                                if (nds_first > mod) t_a = fmaxf(t_a, 2.0f * nds_first - mod);
+                                else t_a = fmaxf(t_a, mod);
+                                t_b = fminf(t_b, 2.0f * nds_first + mod);
+                                const bool use_ts = !((total_time - (ta + nds_first)) < film.exposure);
+                                (void)pcg_float(rng);                          // the choice xi < p_ts
+                                if (use_ts) {
+                                    const float e = pcg_float(rng), e2 = pcg_float(rng);
+                                    const TaSample ts = time_angular_sample(l, mod, nds_first, t_a, t_b, e, e2, dir, g);
+                                    if (ts.pa >= 1e-5f) {
+                                        angular = true;
+                                        nd = ts.nd;
+                                        fa = mk(ts.ph * sig_s.x, ts.ph * sig_s.y, ts.ph * sig_s.z);
+                                        pa = ts.pa;
+                                    }
+                                }
+                            }
+                            const float x1 = angular ? 0.0f : pcg_float(rng);
+                            const float x2 = angular ? 0.0f : pcg_float(rng);
+                            float sp, cp;
+                            tr_sincos2pi(x1, &sp, &cp);
+                            if (angular) {
+                            } else if (surface && ggx) {
                                 alive = ggx_sample(kd, alpha, nrm, wo, sp, cp, x2, nd, fa, pa);
                             } else if (surface && (flags & kFlagOrthoFrame)) {
                                 // cosine sampling in an orthonormal frame (Duff et al. 2017)
@@ -519,10 +640,10 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
                             if (alive) {
                                 const f3 fn = mulv(f, fa);
                                 float nds = __int_as_float(0x7f800000);
-                                if (medium) nds = -tr_log(pcg_float(rng)) / lambda;
+                                if (medium) nds = (tsm && !surface) ? nds_first : -tr_log(pcg_float(rng)) / lambda;
                                 p.wave.ray_o[slot] = make_float4(pos.x, pos.y, pos.z, nds);
                                 p.wave.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, time);
-                                p.wave.thr[slot] = make_float4(fn.x, fn.y, fn.z, albedo * pa);
+                                p.wave.thr[slot] = make_float4(fn.x, fn.y, fn.z, prr * pa);
                                 want_next = true;
                             }
                         }
@@ -811,12 +932,24 @@ cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s) {
     const uint32_t need = ((multi ? p.wave.capacity : p.batch.n_slots) + block - 1) / block;
     if ((uint32_t)grid > need) grid = (int)need;
     if (grid < 1) grid = 1;
+    const bool tsm = multi ? p.wave.target != nullptr : (p.flags & kFlagTimeSampling) != 0;
+    const bool guided = p.guide.vrec != nullptr;
     if (multi) {
-        if (p.guide.vrec) k_shade<true, true><<<grid, block, 0, s>>>(p, depth);
-        else k_shade<false, true><<<grid, block, 0, s>>>(p, depth);
+        if (tsm) {
+            if (guided) k_shade<true, true, true><<<grid, block, 0, s>>>(p, depth);
+            else k_shade<false, true, true><<<grid, block, 0, s>>>(p, depth);
+        } else {
+            if (guided) k_shade<true, true, false><<<grid, block, 0, s>>>(p, depth);
+            else k_shade<false, true, false><<<grid, block, 0, s>>>(p, depth);
+        }
     } else {
-        if (p.guide.vrec) k_shade<true, false><<<grid, block, 0, s>>>(p, depth);
-        else k_shade<false, false><<<grid, block, 0, s>>>(p, depth);
+        if (tsm) {
+            if (guided) k_shade<true, false, true><<<grid, block, 0, s>>>(p, depth);
+            else k_shade<false, false, true><<<grid, block, 0, s>>>(p, depth);
+        } else {
+            if (guided) k_shade<true, false, false><<<grid, block, 0, s>>>(p, depth);
+            else k_shade<false, false, false><<<grid, block, 0, s>>>(p, depth);
+        }
     }
     return cudaGetLastError();
 }

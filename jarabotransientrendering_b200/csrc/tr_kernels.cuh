@@ -25,13 +25,15 @@ struct SceneDev {
     uint32_t num_lights;
     uint32_t medium;          // 0/1
     float sig_s[3], sig_t[3];
-    float lambda;             // mean extinction avg(sigma_t)
+    float lambda;             // free-flight rate: mean extinction avg(sigma_t), or 4 / (film
+                              // duration) in time-sampling mode
     float g;
     uint32_t bvh_depth;       // deepest leaf; the traversal stack holds bvh_depth + 1 entries
     float bmin[3], binv[3];   // scene box (feature normalisation of the learned proposal)
 };
 
 constexpr uint32_t kFlagOrthoFrame = 1u;   // TR_FLAG_ORTHONORMAL_FRAME
+constexpr uint32_t kFlagTimeSampling = 2u; // TR_FLAG_TIME_SAMPLING
 
 // Guided mode state (all null when rendering without the learned proposal).
 struct GuideWave {
@@ -91,6 +93,7 @@ struct Wave {
     float4* sh_L;             // shadow: contribution rgb, slot (bits)
     float4* rec;              // splat records [bounce][capacity]: rgb, bin | depth << 24 (bits)
     float* cam_dist;          // camera-to-first-surface distance per slot (camera unwarp)
+    float4* target;           // light point drawn for the path (time-sampling mode)
     uint8_t* rec_n;           // records per slot
     uint32_t* counters;       // see counter_* helpers below
     unsigned long long* stats;// closest, shadow, splats, paths (accumulated)

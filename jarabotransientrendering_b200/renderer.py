@@ -530,8 +530,9 @@ class TransientRenderer:
     """GPU replacement of ``TransientRenderer::render`` (TransientRenderer.h:76-201)."""
 
     def __init__(self, f_log=None, time_sampling=False, device=0):
-        if time_sampling:
-            raise NotImplementedError("time-sampling mode is not part of the GPU path")
+        # time_sampling: TransientRenderer(f_log, true) -> set_mode(SamplingMode::Transient)
+        # (TransientRenderer.h:61-74, BidirectionalPathTracing.h:189-206)
+        self.time_sampling = bool(time_sampling)
         self.device = device
 
     def render(self, name, world: World, integrator: BidirectionalPathTracing, camera: PinholeCamera,
@@ -547,6 +548,8 @@ class TransientRenderer:
         scene.camera_unwarp = int(film.camera_unwarp)
         scene.bounce_films = int(film.bounce_films)
         scene.components = int(film.components)
+        if self.time_sampling:
+            scene.flags |= S.FLAG_TIME_SAMPLING
         ctx = Context(scene, self.device)
         ctx.render(0, scene.spp)
         f = ctx.film()

@@ -46,6 +46,8 @@ LIGHT_POINT = 0
 LIGHT_RECT = 1
 
 FLAG_ORTHONORMAL_FRAME = 1
+FLAG_TIME_SAMPLING = 2       # "-time-sampling": time-based free flight, time-angular directions in media,
+                             # total-time termination (the reference's SamplingMode::Transient)
 COMP_DEPTH, COMP_POSITIONS, COMP_NORMALS = 2, 8, 16     # FilmComponents bits (FilmComponents.h)
 
 

@@ -21,7 +21,9 @@
  *     applies the camera unwarp of StreakCameraFilm.h:167 (sample time minus the record's
  *     camera distance) and, for N > 0, routes the samples to N per-bounce films with the
  *     weights of MultibounceStreakFilm::add_samples (MultibounceStreakCameraFilm.h:151-171),
- *     the main steady image then being the base Film's (all samples, Film.h:263-284).
+ *     the main steady image then being the base Film's (all samples, Film.h:263-284);
+ *     `mode transient` selects the time-sampling mode (-time-sampling, bunnykiller.cpp:1337-1345,
+ *     1754, 1812-1817).
  *
  * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
  *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
@@ -148,6 +150,7 @@ int main(int argc, char** argv) {
     if (!in) fail("cannot open scene");
     std::string tag;
     unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1, unwarp = 0, nbounce = 0, comps = 0;
+    bool time_sampling = false;
     Real exposure = 0, offset = 0, fov = 40;
     unsigned long long seed = 1;
     Vector3 cpos, cfoc, cup;
@@ -159,6 +162,7 @@ int main(int argc, char** argv) {
     while (in >> tag) {
         if (tag == "film") { in >> W >> H >> T >> exposure >> offset; }
         else if (tag == "filmopts") { in >> unwarp >> nbounce >> comps; }
+        else if (tag == "mode") { std::string m; in >> m; time_sampling = (m == "transient"); }
         else if (tag == "camera") {
             float a[9]; for (float& v : a) in >> v; in >> fov;
             cpos = Vector3(a[0], a[1], a[2]); cfoc = Vector3(a[3], a[4], a[5]); cup = Vector3(a[6], a[7], a[8]);
@@ -221,13 +225,15 @@ int main(int argc, char** argv) {
     PinholeCamera camera(cpos, cfoc, cup, fd);
     AccumStreakFilm film(W, H, T, exposure, offset, keep_streak, unwarp != 0, nbounce, comps);
     StratifiedSampler sampler(W, H, sqrt_spp, true);
-    TransientRenderer<3, Radiance, RadianceAttenuation> engine(nullptr, false);
+    TransientRenderer<3, Radiance, RadianceAttenuation> engine(nullptr, time_sampling);   /* bunnykiller.cpp:1754 */
     Random::StdRNG.seed(seed);                                           /* bunnykiller.cpp:1794 */
     BidirectionalPathTracing<3, Radiance, RadianceAttenuation> bpt(w, ninc, nullptr, &film);
     bpt.set_max_path_size(maxb);
     bpt.set_path_tracing_only(true);
     bpt.set_scattering_components(Scattering::ALL);
-    bpt.set_mode(BidirectionalPathTracing<3, Radiance, RadianceAttenuation>::SamplingMode::SteadyState);
+    bpt.set_mode(time_sampling                                           /* bunnykiller.cpp:1812-1817 */
+                     ? BidirectionalPathTracing<3, Radiance, RadianceAttenuation>::SamplingMode::Transient
+                     : BidirectionalPathTracing<3, Radiance, RadianceAttenuation>::SamplingMode::SteadyState);
 
     FILE* devnull = freopen("/dev/null", "w", stdout);   /* the renderer prints progress */
     (void)devnull;

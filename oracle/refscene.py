@@ -41,6 +41,8 @@ def write_scene(scene, path, seed=None):
     cm = int(getattr(scene, "components", 0))
     if uw or nb or cm:
         lines.append(f"filmopts {uw} {nb} {cm}")
+    if int(getattr(scene, "flags", 0)) & 2:                  # time-sampling mode
+        lines.append("mode transient")
     c = scene.camera
     lines.append("camera " + " ".join(repr(float(v)) for v in (*c.position, *c.focus, *c.up)) + f" {c.fov_deg!r}")
     lines.append(f"integrator {scene.max_bounces} {scene.sqrt_spp} {scene.incoming_samples} "

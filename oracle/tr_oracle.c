@@ -17,6 +17,7 @@
 
 #define SIGMA_VIS 1e-5f            /* _SIGMA_VISIBILITY_, src/bunnykiller.h:76-78 */
 #define INV_PI_F 0.318309873f
+#define INV_2PI_F 0.159154943f
 #define INV_4PI_F 0.0795774683f
 #define MAX_STACK 128
 
@@ -627,6 +628,40 @@ void orc_ggx_eval_cos(const float* kd, float alpha, const float* n, const float*
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
 }
 
+/* The vector-to-vector matrix of Moeller & Hughes ("Efficiently building a matrix to rotate
+ * one vector to another", JGT 4(4), 1999) from +y to `to`, applied to d and normalised -- the
+ * reference's transform_matrix_to (VectorN.h:427-521).  The time-angular sampler passes the
+ * unnormalised target offset as `to` (BidirectionalPathTracing.h:392), for which the matrix is
+ * not a rotation; the same construction is used here so the sampled directions match. */
+static v3 mh_from_y(v3 to, v3 d) {
+    const v3 fr = mk(0.0f, 1.0f, 0.0f);
+    v3 v = mk(fr.y * to.z - fr.z * to.y, fr.z * to.x - fr.x * to.z, fr.x * to.y - fr.y * to.x);
+    float e = (fr.x * to.x + fr.y * to.y) + fr.z * to.z;
+    float m[3][3];
+    if (fabsf(e) > 1.0f - 1e-4f) {
+        /* near-parallel: reflections through the coordinate axis least aligned with +y (z) */
+        v3 xa = mk(0.0f, 0.0f, 1.0f);
+        v3 u = sub(xa, fr);
+        v3 w = sub(xa, to);
+        float c1 = 2.0f / dot(u, u), c2 = 2.0f / dot(w, w);
+        float c3 = (c1 * c2) * dot(u, w);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                m[i][j] = ((-c1 * comp(u, i)) * comp(u, j) - (c2 * comp(w, i)) * comp(w, j)) + (c3 * comp(w, i)) * comp(u, j);
+                if (i == j) m[i][j] += 1.0f;
+            }
+    } else {
+        float h = 1.0f / (1.0f + e);
+        float hvx = h * v.x, hvz = h * v.z, hvxy = hvx * v.y, hvxz = hvx * v.z, hvyz = hvz * v.y;
+        m[0][0] = e + hvx * v.x; m[0][1] = hvxy - v.z;           m[0][2] = hvxz + v.y;
+        m[1][0] = hvxy + v.z;    m[1][1] = e + (h * v.y) * v.y;   m[1][2] = hvyz - v.x;
+        m[2][0] = hvxz - v.y;    m[2][1] = hvyz + v.x;           m[2][2] = e + hvz * v.z;
+    }
+    v3 r = mk((m[0][0] * d.x + m[0][1] * d.y) + m[0][2] * d.z, (m[1][0] * d.x + m[1][1] * d.y) + m[1][2] * d.z,
+              (m[2][0] * d.x + m[2][1] * d.y) + m[2][2] * d.z);
+    return normalize(r);
+}
+
 /* World::Li's record of a camera ray: closest surface distance (FLT_MAX when none), position
  * and normal of that point (zero when none). */
 typedef struct { float t; v3 pos, n; } camrec;
@@ -652,6 +687,25 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
 
     v3 f = mk(1.0f, 1.0f, 1.0f);
     float pi = 1.0f, time = 0.0f;
+    /* time-sampling mode (set_mode(Transient), BidirectionalPathTracing.h:189-206): free flight
+     * at rate m_avg_nb_vertices_path (4) / film length (:240-307), medium directions aimed at a
+     * light point drawn for the path (:1107-1113, :385-431), total-time termination (:447-481) */
+    const int tsm = (x->integ.flags & ORC_FLAG_TIME_SAMPLING) != 0;
+    v3 target = mk(0.0f, 0.0f, 0.0f);
+    if (tsm) {
+        /* World::sample_light + LightSource::sample(light_sample, pdf): the emission point
+         * (PointLightSource.h:174-183, RectangularAreaLightSource.h:252-276) */
+        float xl = pcg_float(rng);
+        uint32_t li = (uint32_t)(xl * (float)x->nl);
+        if (li >= x->nl) li = x->nl - 1;
+        const orc_light* L = &x->lights[li];
+        target = ld3(L->position);
+        if (L->kind == 1) {
+            float xu = pcg_float(rng), xv = pcg_float(rng);
+            target = add(add(target, muls(ld3(L->left), xu)), muls(ld3(L->up), xv));
+        }
+        if (medium) lambda = 4.0f / ((float)F->time_bins * F->exposure);
+    }
     float dsamp = INFINITY;
     if (medium) dsamp = -orc_log(pcg_float(rng)) / lambda;
 
@@ -775,15 +829,70 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
 
         if (depth + 1 >= maxb) break;
 
-        /* ---- Russian roulette (sample_termination) ---- */
+        /* ---- termination (sample_termination): Russian roulette, or none with total-time
+         * termination (the film-time test above ends the walk) ---- */
         float albedo = surface ? avg3(kd) : avg3(mk(sig_s.x / sig_t.x, sig_s.y / sig_t.y, sig_s.z / sig_t.z));
-        if (pcg_float(rng) > albedo) break;
+        float prr = 1.0f;
+        if (!tsm) {
+            if (pcg_float(rng) > albedo) break;
+            prr = albedo;
+        }
 
         /* ---- outgoing direction (sample_outgoing_ray) ---- */
+        v3 fa; float pa; v3 nd;
+        float nds_first = 0.0f;
+        int angular_done = 0;
+        if (tsm && !surface) {
+            /* the next free-flight distance r is drawn first (generate_path, :530-545) and the
+             * direction from the time-angular sampler towards the target (SamplingTechniques.h
+             * TimeAngular) with probability p_ts = 1, else the phase function (:371-431) */
+            nds_first = -orc_log(pcg_float(rng)) / lambda;
+            const float r = nds_first;
+            v3 l = sub(target, pos);
+            float mod = sqrtf(dot(l, l));
+            float ta = mod + time;
+            float tb = (float)F->time_bins * F->exposure + F->offset;
+            float t_a = ta, t_b = tb;
+            if (r > mod) t_a = fmaxf(t_a, 2.0f * r - mod); else t_a = fmaxf(t_a, mod);
+            t_b = fminf(t_b, 2.0f * r + mod);
+            int use_ts = !((tb - (ta + r)) < F->exposure);
+            (void)pcg_float(rng);                          /* the technique choice xi < p_ts */
+            if (use_ts) {
+                float e = pcg_float(rng), e2 = pcg_float(rng);
+                float t = e * (t_b - t_a) + t_a;
+                /* TimeAngular::theta_t (SamplingTechniques.h:186-191): the cosine is evaluated in
+                 * double (its constants are double) and stored as a float, then clamped */
+                float ct = (float)((((double)(mod * mod) + ((2.0 * (double)t) * (double)r)) - (double)(t * t)) /
+                                   ((2.0 * (double)r) * (double)mod));
+                ct = ct < -1.0f ? -1.0f : (ct > 1.0f ? 1.0f : ct);
+                /* theta = acos(ct) is a float.  At ct = -1 it is the float nearest pi, which lies
+                 * above pi, so sin(theta) is the small negative number pi - (float)pi: this is
+                 * what the reference gets whenever the bounds are inverted (t_a > t_b, the current
+                 * delay exceeding 2r), and its density dtdtheta / (t_b - t_a) is then a small
+                 * positive number that can pass the 1e-5 test.  Elsewhere sin(acos(ct)) agrees
+                 * with sqrt(1 - ct^2) to rounding. */
+                float st = ct == -1.0f ? (float)(3.14159265358979323846 - (double)3.14159265358979323846f)
+                                       : (float)sqrt(1.0 - (double)ct * (double)ct);
+                float sp2, cp2;
+                orc_sincos2pi(e2, &sp2, &cp2);
+                nd = mh_from_y(l, mk(cp2 * st, ct, sp2 * st));
+                float ph = hg_eval(g, dot(dir, nd));
+                fa = mk(ph * sig_s.x, ph * sig_s.y, ph * sig_s.z);
+                /* the reference's density: TimeAngular::pdf(theta) / (2 pi) (:233-236, and
+                 * BidirectionalPathTracing.h:400-402 with p_ts = 1), a density in theta used as
+                 * a solid-angle density (no 1 / sin(theta)); restated as is, with its operand
+                 * types (float products and sums, double where a double constant enters) */
+                float dtdth = (float)((double)((mod * r) * st) /
+                                      sqrt((double)(r * r + mod * mod) - ((2.0 * (double)r) * (double)mod) * (double)ct));
+                float pdf_theta = dtdth / (t_b - t_a);
+                pa = (float)((double)pdf_theta / (2.0 * 3.14159265358979323846));
+                angular_done = pa >= 1e-5f;                /* else phase-function sampling */
+            }
+        }
+        if (!angular_done) {
         float x1 = pcg_float(rng), x2 = pcg_float(rng);
         float sp, cp;
         orc_sincos2pi(x1, &sp, &cp);
-        v3 fa; float pa; v3 nd;
         if (surface && ggx) {
             if (!ggx_sample(kd, alpha, n, wo, sp, cp, x2, &nd, &fa, &pa)) break;
         } else if (surface && (x->integ.flags & ORC_FLAG_ORTHONORMAL_FRAME)) {
@@ -829,10 +938,11 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
             fa = mk(ph * sig_s.x, ph * sig_s.y, ph * sig_s.z);
             pa = ph;
         }
+        }
         f = mulv(f, fa);
-        pi = albedo * pa;
+        pi = prr * pa;
         org = pos; dir = nd;
-        if (medium) dsamp = -orc_log(pcg_float(rng)) / lambda;
+        if (medium) dsamp = (tsm && !surface) ? nds_first : -orc_log(pcg_float(rng)) / lambda;
     }
     return nrec;
 }

@@ -64,6 +64,7 @@ typedef struct orc_film {
 } orc_film;
 typedef struct orc_integrator { uint32_t max_bounces, sqrt_spp, incoming_samples, flags; uint64_t seed; } orc_integrator;
 #define ORC_FLAG_ORTHONORMAL_FRAME 1u
+#define ORC_FLAG_TIME_SAMPLING 2u      /* "-time-sampling": BidirectionalPathTracing SamplingMode::Transient */
 typedef struct orc_hit { float t; uint32_t prim_id; float u, v; } orc_hit;
 
 typedef struct orc_ctx orc_ctx;

@@ -12,6 +12,10 @@ container); the committed .npz files are what the tests read.
 StreakCameraFilm, three per-bounce films of MultibounceStreakFilm (their per-bounce streaks are
 stored as one film of 3H rows, their weights and the base steady image beside them) and the
 depth / position / normal components of Film (per-pixel sums beside the streak).
+
+`timesampling` (time sampling in a medium: the time-angular direction sampler) has a heavy-tailed
+per-run energy, so its fixture holds per-run statistics of KR runs instead of per-bin moments:
+the total energy and the energy in each window of 8 time bins.
 """
 import os
 import sys
@@ -25,6 +29,20 @@ from jarabotransientrendering_b200 import scenes as S  # noqa: E402
 from oracle import refscene  # noqa: E402
 
 K = 96
+KR = 512              # runs of the per-run (robust) fixtures
+ROBUST = ("timesampling",)
+
+
+def window_sums(streak, width=8):
+    """Energy of a streak film [H][W][T][3] in consecutive windows of `width` time bins."""
+    prof = streak.sum(axis=(0, 1, 3))
+    return prof.reshape(-1, width).sum(1)
+
+
+def _robust_run(args):
+    name, seed = args
+    r = refscene.render(golden_scenes()[name], seed=seed)
+    return r["streak"].sum(), window_sums(r["streak"])
 
 
 def golden_scenes():
@@ -48,7 +66,15 @@ def golden_scenes():
                  max_bounces=12)
     k.lights[0].position = (0.5, 0.8, 0.5)
     k.components = S.COMP_DEPTH | S.COMP_POSITIONS | S.COMP_NORMALS
-    return {"cornell": c, "medium": m, "arealight": a, "unwarp": u, "bounces": b, "components": k}
+    ts = S.medium(width=12, height=12, time_bins=48, exposure=0.15, sqrt_spp=8, incoming_samples=1,
+                  max_bounces=12)
+    ts.lights[0].position = (0.5, 0.8, 0.5)
+    ts.flags = S.FLAG_TIME_SAMPLING
+    tc = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
+    tc.lights[0].position = (0.5, 0.8, 0.5)
+    tc.flags = S.FLAG_TIME_SAMPLING
+    return {"cornell": c, "medium": m, "arealight": a, "unwarp": u, "bounces": b, "components": k,
+            "timesampling": ts, "timesampling_surface": tc}
 
 
 def main(names=None):
@@ -56,6 +82,16 @@ def main(names=None):
         raise SystemExit("reference sources not available: cannot build oracle/_ref/ref_render")
     for name, sc in golden_scenes().items():
         if names and name not in names:
+            continue
+        if name in ROBUST:
+            from multiprocessing import get_context
+            with get_context("spawn").Pool(os.cpu_count() or 4) as pool:
+                res = pool.map(_robust_run, [(name, s) for s in range(1, KR + 1)])
+            energy = np.array([e for e, _ in res])
+            windows = np.array([w for _, w in res])
+            out = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}.npz")
+            np.savez_compressed(out, energy=energy, windows=windows, k=KR)
+            print(name, out, "energy median %.4f mean %.4f" % (np.median(energy), energy.mean()))
             continue
         runs = [refscene.render(sc, seed=s) for s in range(1, K + 1)]
         films = np.array([r["streak"] for r in runs])

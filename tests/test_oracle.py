@@ -70,12 +70,16 @@ def _golden(name):
     return np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
 
 
-def _golden_scene(name):
+def _make_golden():
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
-    return mod.golden_scenes()[name]
+    return mod
+
+
+def _golden_scene(name):
+    return _make_golden().golden_scenes()[name]
 
 
 def compare_to_golden(films, g, energy_tol=0.005):
@@ -170,6 +174,48 @@ def test_oracle_film_components_match_reference(oracle_lib):
         se = np.sqrt((arr.std(0, ddof=1) / np.sqrt(K)) ** 2 + g[key + "_se"] ** 2)
         diff = np.abs(arr.mean(0) - g[key + "_mean"])
         assert (diff <= 4.0 * se + 1e-5 * np.abs(g[key + "_mean"]) + 1e-6).all(), (key, float((diff / (se + 1e-12)).max()))
+
+
+def test_oracle_time_sampling_surfaces_match_reference(oracle_lib):
+    """Time sampling (-time-sampling, SamplingMode::Transient) without a medium: one light
+    target per path, termination by total time instead of Russian roulette
+    (BidirectionalPathTracing.h:448-483); per-bin statistics agree with the reference."""
+    sc = _golden_scene("timesampling_surface")
+    g = _golden("timesampling_surface")
+    o = oracle_lib.Oracle(sc)
+    K = len(g["energy"])
+    films = np.array([o.render(sample_begin=64 * k, sample_count=64, nthreads=4)["streak"] for k in range(K)])
+    r = compare_to_golden(films, g)
+    assert r["frac_z3"] < 0.02 and abs(r["mean_z"]) < 0.1 and r["max_z"] < 7.0, r
+    assert abs(r["energy_z"]) < 4.0 and r["one_sided_bins"] == 0, r
+
+
+def test_oracle_time_sampling_medium_matches_reference(oracle_lib):
+    """Time sampling in a medium: free flights at the rate 4 / (film duration), directions from
+    the time-angular sampler towards the light target (SamplingTechniques.h TimeAngular,
+    BidirectionalPathTracing.h:342-431).  The reference's density there has rare tiny values
+    (inverted time bounds give theta = (float)pi, whose sine is negative) and so rare huge
+    weights: the per-run energy is heavy-tailed.  The oracle's per-run energies and 8-bin window
+    energies follow the reference's distribution (rank tests), and so does its tail."""
+    from scipy import stats
+    mg = _make_golden()
+    sc = mg.golden_scenes()["timesampling"]
+    g = _golden("timesampling")
+    K = int(g["k"])
+    o = oracle_lib.Oracle(sc)
+    runs = [o.render(sample_begin=64 * k, sample_count=64, nthreads=4, steady=False)["streak"] for k in range(K)]
+    energy = np.array([r.sum() for r in runs])
+    windows = np.array([mg.window_sums(r) for r in runs])
+    assert stats.mannwhitneyu(energy, g["energy"]).pvalue > 1e-3
+    assert stats.ks_2samp(energy, g["energy"]).pvalue > 1e-3
+    nw = windows.shape[1]
+    for w in range(nw):
+        if not windows[:, w].any() and not g["windows"][:, w].any():
+            continue
+        assert stats.mannwhitneyu(windows[:, w], g["windows"][:, w]).pvalue > 1e-3 / nw, w
+    # the tail: runs above the reference's 95th percentile (binomial, 5% of K)
+    above = int((energy > np.percentile(g["energy"], 95)).sum())
+    assert stats.binomtest(above, K, 0.05).pvalue > 1e-3, above
 
 
 def test_oracle_reference_harness_live(oracle_lib):
