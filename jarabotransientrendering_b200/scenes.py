@@ -48,6 +48,8 @@ LIGHT_RECT = 1
 FLAG_ORTHONORMAL_FRAME = 1
 FLAG_TIME_SAMPLING = 2       # "-time-sampling": time-based free flight, time-angular directions in media,
                              # total-time termination (the reference's SamplingMode::Transient)
+FLAG_BIDIRECTIONAL = 4       # light subpaths + vertex connections (set_path_tracing_only(false)); needs
+                             # FLAG_TIME_SAMPLING and no medium
 COMP_DEPTH, COMP_POSITIONS, COMP_NORMALS = 2, 8, 16     # FilmComponents bits (FilmComponents.h)
 
 

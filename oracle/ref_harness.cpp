@@ -23,7 +23,8 @@
  *     weights of MultibounceStreakFilm::add_samples (MultibounceStreakCameraFilm.h:151-171),
  *     the main steady image then being the base Film's (all samples, Film.h:263-284);
  *     `mode transient` selects the time-sampling mode (-time-sampling, bunnykiller.cpp:1337-1345,
- *     1754, 1812-1817).
+ *     1754, 1812-1817); `bidir 1` turns off path-tracing-only (light subpaths and vertex
+ *     connections; BidirectionalPathTracing::set_path_tracing_only, reachable through the API).
  *
  * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
  *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
@@ -151,6 +152,7 @@ int main(int argc, char** argv) {
     std::string tag;
     unsigned W = 0, H = 0, T = 0, maxb = 0, sqrt_spp = 0, ninc = 1, unwarp = 0, nbounce = 0, comps = 0;
     bool time_sampling = false;
+    int bidir = 0;
     Real exposure = 0, offset = 0, fov = 40;
     unsigned long long seed = 1;
     Vector3 cpos, cfoc, cup;
@@ -163,6 +165,7 @@ int main(int argc, char** argv) {
         if (tag == "film") { in >> W >> H >> T >> exposure >> offset; }
         else if (tag == "filmopts") { in >> unwarp >> nbounce >> comps; }
         else if (tag == "mode") { std::string m; in >> m; time_sampling = (m == "transient"); }
+        else if (tag == "bidir") { in >> bidir; }
         else if (tag == "camera") {
             float a[9]; for (float& v : a) in >> v; in >> fov;
             cpos = Vector3(a[0], a[1], a[2]); cfoc = Vector3(a[3], a[4], a[5]); cup = Vector3(a[6], a[7], a[8]);
@@ -229,7 +232,7 @@ int main(int argc, char** argv) {
     Random::StdRNG.seed(seed);                                           /* bunnykiller.cpp:1794 */
     BidirectionalPathTracing<3, Radiance, RadianceAttenuation> bpt(w, ninc, nullptr, &film);
     bpt.set_max_path_size(maxb);
-    bpt.set_path_tracing_only(true);
+    bpt.set_path_tracing_only(bidir == 0);                              /* bunnykiller.cpp:1809 (API only) */
     bpt.set_scattering_components(Scattering::ALL);
     bpt.set_mode(time_sampling                                           /* bunnykiller.cpp:1812-1817 */
                      ? BidirectionalPathTracing<3, Radiance, RadianceAttenuation>::SamplingMode::Transient

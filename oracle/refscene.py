@@ -43,6 +43,8 @@ def write_scene(scene, path, seed=None):
         lines.append(f"filmopts {uw} {nb} {cm}")
     if int(getattr(scene, "flags", 0)) & 2:                  # time-sampling mode
         lines.append("mode transient")
+    if int(getattr(scene, "flags", 0)) & 4:                  # light subpaths + vertex connections
+        lines.append("bidir 1")
     c = scene.camera
     lines.append("camera " + " ".join(repr(float(v)) for v in (*c.position, *c.focus, *c.up)) + f" {c.fov_deg!r}")
     lines.append(f"integrator {scene.max_bounces} {scene.sqrt_spp} {scene.incoming_samples} "

@@ -19,6 +19,8 @@
 #define INV_PI_F 0.318309873f
 #define INV_2PI_F 0.159154943f
 #define INV_4PI_F 0.0795774683f
+#define LIGHT_STATE_SALT 0xD1B54A32D192ED03ULL
+#define LIGHT_SEQ_SALT 0x3C6EF372FE94F82AULL
 #define MAX_STACK 128
 
 typedef struct { float x, y, z; } v3;
@@ -255,6 +257,14 @@ static uint32_t build_rec(bld* B, uint32_t first, uint32_t count, uint32_t depth
 int orc_create(const orc_scene* s, const orc_camera* c, const orc_film* f, const orc_integrator* it,
                orc_ctx** out) {
     if (!s || !c || !f || !it || !out || s->num_triangles == 0 || s->num_lights == 0) return 1;
+    if (it->flags & ORC_FLAG_BIDIRECTIONAL) {
+        /* the well-defined part of the reference: time-sampling mode, no medium, Lambertian
+         * surfaces, at most 16 bounces (see bidirectional connections below) */
+        if (!(it->flags & ORC_FLAG_TIME_SAMPLING) || s->medium.enabled || it->max_bounces > ORC_BIDIR_MAX_BOUNCES)
+            return 1;
+        for (uint32_t m = 0; m < s->num_materials; ++m)
+            if (s->materials[m].kind != 0) return 1;
+    }
     orc_ctx* x = (orc_ctx*)calloc(1, sizeof(orc_ctx));
     uint32_t nt = s->num_triangles;
     x->nt = nt; x->nm = s->num_materials; x->nl = s->num_lights;
@@ -666,9 +676,147 @@ static v3 mh_from_y(v3 to, v3 d) {
  * and normal of that point (zero when none). */
 typedef struct { float t; v3 pos, n; } camrec;
 
+/* ---- bidirectional connections (set_path_tracing_only(false)) ----
+ * Defined here as in the reference for time-sampling mode in scenes without a medium.  (Outside
+ * time-sampling mode the reference draws no light sample before its light subpath,
+ * BidirectionalPathTracing.h:1108-1113, so the subpath starts from an uninitialised LightSample
+ * with pdf 0 and every connection is non-finite and dropped; with a medium its time-sampled
+ * connections build a medium vertex from a ray without a medium, :766-790, and dereference a null
+ * medium.)  Light subpaths start in vacuum as in the reference (Ray(pos, dir, false) carries no
+ * medium, :1121-1124).
+ *
+ * A subpath vertex (Path::Vertex, Path.h:36-140): position, delay, geometric normal, vertex pdf
+ * (m_pi), Lambertian albedo, vertex value (m_f, throughput over pdfs). */
+typedef struct { v3 pos; float time; v3 n; float pdf; v3 kd; v3 f; } bvert;
+
+/* PathMIS::connection_probability (PathMIS.h:49-60): the density with which path0[i0] samples
+ * the direction towards path1[i1]; Lambertian::p = max(0, cos) / pi (Lambertian.h:82-93). */
+static float conn_prob(const bvert* from, const bvert* to) {
+    v3 d = normalize(sub(to->pos, from->pos));
+    float c = dot(d, from->n);
+    return (c > 0.0f ? c : 0.0f) * INV_PI_F;
+}
+
+/* PathMIS::compute_weight with beta = 1 (MIS_Balance, BidirectionalPathTracing.h:902-924,
+ * PathMIS.h:63-111), restated as it is: the ratios are accumulated by addition along each
+ * subpath, and the caller divides by the result. */
+static float mis_weight(const bvert* ev, const bvert* lv, int t, int s) {
+    float iw = 1.0f;
+    if (s > 1) {
+        float p_s_1 = conn_prob(&ev[t], &lv[s]) / lv[s].pdf;
+        iw = iw + p_s_1;
+        float p_i_0 = p_s_1;
+        for (int i = s - 1; i > 0; --i) {
+            float p_i = conn_prob(&lv[i + 1], &lv[i]);
+            p_i = p_i_0 + p_i / lv[i].pdf;
+            iw = iw + p_i;
+            p_i_0 = p_i;
+        }
+    }
+    if (t > 1) {
+        float p_t_1 = conn_prob(&lv[s], &ev[t]) / ev[t].pdf;
+        iw = iw + p_t_1;
+        float p_i_0 = p_t_1;
+        for (int i = t - 1; i > 0; --i) {
+            float p_i = conn_prob(&ev[i + 1], &ev[i]);
+            p_i = p_i_0 + p_i / ev[i].pdf;
+            iw = iw + p_i;
+            p_i_0 = p_i;
+        }
+    }
+    return (float)(1.0 / (double)iw);
+}
+
+/* Lambertian direction sampling at a surface vertex, in the frame the eye path uses (the
+ * orthonormal frame with ORC_FLAG_ORTHONORMAL_FRAME, else Intersection::set_coordinate_system's). */
+static void lambert_sample(const orc_ctx* x, v3 n, v3 kd, float x1, float x2, v3* nd, v3* fa, float* pa) {
+    float sp, cp;
+    orc_sincos2pi(x1, &sp, &cp);
+    float ct = sqrtf(x2);
+    float stt = sqrtf(1.0f - ct * ct);
+    if (x->integ.flags & ORC_FLAG_ORTHONORMAL_FRAME) {
+        frame3 Fr = make_frame(n);
+        *nd = to_world(&Fr, mk(cp * stt, sp * stt, ct));
+        *fa = mk((kd.x * INV_PI_F) * ct, (kd.y * INV_PI_F) * ct, (kd.z * INV_PI_F) * ct);
+    } else {
+        v3 aux = fabsf(n.x) > fabsf(n.z) ? mk(-n.y, n.x, n.z) : mk(0.0f, -n.z, n.y);
+        v3 tv = normalize(aux);
+        v3 tu = cross(n, tv);
+        v3 w = add(add(muls(tu, cp * stt), muls(n, ct)), muls(tv, sp * stt));
+        *nd = normalize(w);
+        float ca = fabsf(dot(n, *nd));
+        *fa = mk((kd.x * INV_PI_F) * ca, (kd.y * INV_PI_F) * ca, (kd.z * INV_PI_F) * ca);
+    }
+    *pa = ct * INV_PI_F;
+}
+
+/* The light subpath (generate_path FROM_LIGHT, BidirectionalPathTracing.h:486-644, started at
+ * :1121-1124): emission from the path's light point in a direction drawn from the light stream
+ * rl (PointLightSource::sample: uniform sphere, PointLightSource.h:174-183, Sampling.h:80-94;
+ * RectangularAreaLightSource::sample: cosine lobe about the normal, RectangularAreaLightSource.h:
+ * 252-276, Sampling.h:131-143), initial pdf p0 = (1 / lights) * emission pdf, value L0 = the
+ * emitted intensity (times cos for the rectangle).  Vertices are stored while the subpath's
+ * time stays within the film (TotalTime termination, no Russian roulette); at most maxv. */
+static int light_subpath(const orc_ctx* x, pcg* rl, const orc_light* L, v3 lpos, int maxv, float total_time,
+                         bvert* lv, v3* L0, pstats* st) {
+    float e1 = pcg_float(rl), e2 = pcg_float(rl);
+    float sp, cp;
+    orc_sincos2pi(e1, &sp, &cp);
+    v3 dir;
+    float pdf_dir;
+    if (L->kind == 1) {
+        float ct = sqrtf(e2);
+        float stt = sqrtf(1.0f - ct * ct);
+        v3 ln = ld3(L->normal);
+        dir = mh_from_y(ln, mk(cp * stt, ct, sp * stt));
+        pdf_dir = ct * INV_PI_F;
+        float dl = dot(dir, ln);
+        *L0 = mk(L->intensity[0] * dl, L->intensity[1] * dl, L->intensity[2] * dl);
+        pdf_dir = (1.0f / L->area) * pdf_dir;
+    } else {
+        float ct = (float)(1.0 - 2.0 * (double)e2);
+        float stt = sqrtf(1.0f - ct * ct);
+        dir = mk(cp * stt, ct, sp * stt);
+        pdf_dir = INV_4PI_F;
+        *L0 = ld3(L->intensity);
+    }
+    float pi = (1.0f / (float)x->nl) * pdf_dir;
+    v3 org = lpos, f = mk(1.0f, 1.0f, 1.0f);
+    float time = 0.0f;
+    int n = 0;
+    while (n < maxv) {
+        wray r;
+        wray_setup(&r, org, dir, SIGMA_VIS, INFINITY);
+        orc_hit h;
+        st->closest++;
+        uint32_t cv = 0, ct2 = 0;
+        int hit = trace1(x, &r, 0, &h, &cv, &ct2);
+        st->c_nodes += cv; st->c_tris += ct2;
+        if (!hit) break;
+        float dist = h.t;
+        f = mk(f.x / pi, f.y / pi, f.z / pi);
+        time = time + dist;
+        if (time > total_time) break;
+        v3 pos = add(org, muls(dir, dist));
+        v3 nrm = x->ng[h.prim_id];
+        v3 kd = ld3(x->mats[x->mat[h.prim_id]].kd);
+        lv[n].pos = pos; lv[n].time = time; lv[n].n = nrm; lv[n].pdf = pi; lv[n].kd = kd; lv[n].f = f;
+        ++n;
+        if (n >= maxv) break;
+        float x1 = pcg_float(rl), x2 = pcg_float(rl);
+        v3 nd, fa;
+        float pa;
+        lambert_sample(x, nrm, kd, x1, x2, &nd, &fa, &pa);
+        f = mulv(f, fa);
+        pi = 1.0f * pa;
+        org = pos; dir = nd;
+    }
+    return n;
+}
+
 /* One random walk; appends its splat records (at most max_bounces) to rec; fills cr (if not
  * NULL) with the camera ray's record. */
-static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc, srec* rec, pstats* st,
+static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, pcg* rl, float inv_inc, srec* rec, pstats* st,
                       camrec* cr) {
     const orc_film* F = &x->film;
     const int medium = x->med.enabled != 0;
@@ -692,6 +840,10 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
      * light point drawn for the path (:1107-1113, :385-431), total-time termination (:447-481) */
     const int tsm = (x->integ.flags & ORC_FLAG_TIME_SAMPLING) != 0;
     v3 target = mk(0.0f, 0.0f, 0.0f);
+    const int bidir = rl != NULL && (x->integ.flags & ORC_FLAG_BIDIRECTIONAL) != 0;
+    bvert lv[ORC_BIDIR_MAX_BOUNCES], ev[ORC_BIDIR_MAX_BOUNCES];
+    int nlv = 0;
+    v3 L0 = mk(0.0f, 0.0f, 0.0f);
     if (tsm) {
         /* World::sample_light + LightSource::sample(light_sample, pdf): the emission point
          * (PointLightSource.h:174-183, RectangularAreaLightSource.h:252-276) */
@@ -705,6 +857,8 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
             target = add(add(target, muls(ld3(L->left), xu)), muls(ld3(L->up), xv));
         }
         if (medium) lambda = 4.0f / ((float)F->time_bins * F->exposure);
+        /* the light subpath from the same light point (its own random stream) */
+        if (bidir && maxb >= 2) nlv = light_subpath(x, rl, L, target, (int)maxb - 1, total_time, lv, &L0, st);
     }
     float dsamp = INFINITY;
     if (medium) dsamp = -orc_log(pcg_float(rng)) / lambda;
@@ -824,6 +978,55 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, float inv_inc,
                         st->splats++;
                     }
                 }
+            }
+        }
+
+        /* ---- connections of this eye vertex with the light subpath's vertices (transient
+         * connect_paths, BidirectionalPathTracing.h:1018-1041; connect_vertices' shadow
+         * connection, :840-871): only pairs with ie + il + 2 <= max_bounces and delays within
+         * the film; the connection counts when World::intersects reports a blocker between the
+         * two vertices (that query returns true on a hit, World.h:617-639 / 693-697, and the
+         * reference connects on true); value fe * (fv * (f_l * L0)) / (1 * w) with w the
+         * MIS quantity above, time = distance + both delays, bounce ie + il + 1 ---- */
+        if (bidir && surface && depth + 2 <= maxb) {
+            bvert* E = &ev[depth];
+            E->pos = pos; E->time = time; E->n = n; E->pdf = ptot; E->kd = kd; E->f = f;
+            for (int il = 0; il < nlv; ++il) {
+                if (depth + (uint32_t)il + 2 > maxb) break;
+                if (time + lv[il].time > total_time) break;
+                const bvert* Lv = &lv[il];
+                v3 l2e = sub(pos, Lv->pos);
+                float dd = sqrtf(dot(l2e, l2e));
+                l2e = divs(l2e, dd);
+                if ((dd + time) + Lv->time > total_time) continue;
+                wray sr;
+                wray_setup(&sr, Lv->pos, l2e, SIGMA_VIS, dd - SIGMA_VIS);
+                orc_hit sh;
+                st->shadow++;
+                uint32_t sv = 0, stt2 = 0;
+                int blocked = trace1(x, &sr, 1, &sh, &sv, &stt2);
+                st->s_nodes += sv; st->s_tris += stt2;
+                if (!blocked) continue;
+                float ce = -dot(l2e, n), cl = dot(l2e, Lv->n);
+                ce = ce > 0.0f ? ce : 0.0f;
+                cl = cl > 0.0f ? cl : 0.0f;
+                v3 fe = mk((kd.x * INV_PI_F) * ce, (kd.y * INV_PI_F) * ce, (kd.z * INV_PI_F) * ce);
+                v3 fl = mk((Lv->kd.x * INV_PI_F) * cl, (Lv->kd.y * INV_PI_F) * cl, (Lv->kd.z * INV_PI_F) * cl);
+                float att = 1.0f / (dd * dd);
+                v3 fv = mk((fe.x * fl.x) * att, (fe.y * fl.y) * att, (fe.z * fl.z) * att);
+                float w = mis_weight(ev, lv, (int)depth, il);
+                float Lc[3] = {((f.x * (fv.x * (Lv->f.x * L0.x))) / w) * inv_inc,
+                               ((f.y * (fv.y * (Lv->f.y * L0.y))) / w) * inv_inc,
+                               ((f.z * (fv.z * (Lv->f.z * L0.z))) / w) * inv_inc};
+                float tt = dd + (time + Lv->time);
+                float tc = unwarp ? tt - cam_dist : tt;
+                float ps = (tc - F->offset) / F->exposure;
+                int inside = ps < (float)F->time_bins && ps >= 0.0f;
+                int finite = is_finite3(Lc);
+                rec[nrec].bin = inside ? (uint32_t)floorf(ps) : BIN_OUTSIDE;
+                rec[nrec].depth = depth + (uint32_t)il + 1u;
+                for (int c = 0; c < 3; ++c) rec[nrec].L[c] = finite ? Lc[c] : 0.0f;
+                if (inside || bounce_films) { nrec++; st->splats++; }
             }
         }
 
@@ -975,6 +1178,12 @@ static inline void path_rng(const orc_ctx* x, pcg* r, uint32_t pixel, uint64_t s
     pcg_seed(r, x->integ.seed + (uint64_t)(j + 1) * GOLDEN64, cam_id(pixel, s));
 }
 
+/* The light subpath's stream (bidirectional connections): another state and increment, so the
+ * eye walk draws exactly what it draws without light subpaths. */
+static inline void light_rng(const orc_ctx* x, pcg* r, uint32_t pixel, uint64_t s, uint32_t j) {
+    pcg_seed(r, x->integ.seed + (uint64_t)(j + 1) * GOLDEN64 + LIGHT_STATE_SALT, cam_id(pixel, s) ^ LIGHT_SEQ_SALT);
+}
+
 int orc_path_records(const orc_ctx* x, uint32_t px, uint32_t py, uint64_t s, uint32_t j,
                      uint32_t* bins, float* rgb, int cap) {
     v3 o, d;
@@ -984,7 +1193,9 @@ int orc_path_records(const orc_ctx* x, uint32_t px, uint32_t py, uint64_t s, uin
     srec rec[256];
     pstats st;
     memset(&st, 0, sizeof(st));
-    int n = trace_path(x, o, d, &r, 1.0f / (float)x->integ.incoming_samples, rec, &st, NULL);
+    pcg rl;
+    light_rng(x, &rl, py * x->film.width + px, s, j);
+    int n = trace_path(x, o, d, &r, &rl, 1.0f / (float)x->integ.incoming_samples, rec, &st, NULL);
     if (n > cap) n = cap;
     for (int i = 0; i < n; ++i) {
         bins[i] = rec[i].bin;
@@ -1021,10 +1232,11 @@ static void* render_rows(void* arg) {
                 if (J->weight) J->weight[pixel] += 1.0;
                 uint64_t present = 0;          /* bounce films with a sample of this camera sample */
                 for (uint32_t j = 0; j < ninc; ++j) {
-                    pcg r;
+                    pcg r, rl;
                     path_rng(x, &r, pixel, s, j);
+                    light_rng(x, &rl, pixel, s, j);
                     camrec cr;
-                    int n = trace_path(x, o, d, &r, inv_inc, rec, &J->st, j == 0 ? &cr : NULL);
+                    int n = trace_path(x, o, d, &r, &rl, inv_inc, rec, &J->st, j == 0 ? &cr : NULL);
                     J->paths++;
                     if (j == 0) {
                         if (J->cdepth) J->cdepth[pixel] += (double)cr.t;

@@ -65,6 +65,9 @@ typedef struct orc_film {
 typedef struct orc_integrator { uint32_t max_bounces, sqrt_spp, incoming_samples, flags; uint64_t seed; } orc_integrator;
 #define ORC_FLAG_ORTHONORMAL_FRAME 1u
 #define ORC_FLAG_TIME_SAMPLING 2u      /* "-time-sampling": BidirectionalPathTracing SamplingMode::Transient */
+#define ORC_FLAG_BIDIRECTIONAL 4u      /* light subpaths + vertex connections (set_path_tracing_only(false));
+                                          with ORC_FLAG_TIME_SAMPLING, scenes without a medium */
+#define ORC_BIDIR_MAX_BOUNCES 16u
 typedef struct orc_hit { float t; uint32_t prim_id; float u, v; } orc_hit;
 
 typedef struct orc_ctx orc_ctx;

@@ -73,8 +73,15 @@ def golden_scenes():
     tc = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
     tc.lights[0].position = (0.5, 0.8, 0.5)
     tc.flags = S.FLAG_TIME_SAMPLING
+    bd = S.cornell(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=6)
+    bd.lights[0].position = (0.5, 0.8, 0.5)
+    bd.flags = S.FLAG_TIME_SAMPLING | S.FLAG_BIDIRECTIONAL
+    br = S.guided(width=12, height=12, time_bins=48, exposure=0.1, sqrt_spp=8, max_bounces=5,
+                  lambertian_floor=True)
+    br.lights = [S.rect_light((0.6, 0.8, 0.6), (0.6, 0.0, 0.6), (0.2, 0.2), 4.0)]
+    br.flags = S.FLAG_TIME_SAMPLING | S.FLAG_BIDIRECTIONAL
     return {"cornell": c, "medium": m, "arealight": a, "unwarp": u, "bounces": b, "components": k,
-            "timesampling": ts, "timesampling_surface": tc}
+            "timesampling": ts, "timesampling_surface": tc, "bidir": bd, "bidir_rect": br}
 
 
 def main(names=None):

@@ -218,6 +218,42 @@ def test_oracle_time_sampling_medium_matches_reference(oracle_lib):
     assert stats.binomtest(above, K, 0.05).pvalue > 1e-3, above
 
 
+@pytest.mark.parametrize("name", ["bidir", "bidir_rect"])
+def test_oracle_bidirectional_matches_reference(oracle_lib, name):
+    """Light subpaths and vertex connections (set_path_tracing_only(false)) in time-sampling mode:
+    emission sampling of point and rectangle lights, eye-light vertex connections with the
+    reference's MIS quantity and its visibility convention; per-bin statistics and total energy
+    agree with the reference, and the connections carry a large share of the energy (so a
+    missing or mis-weighted connection fails the comparison)."""
+    sc = _golden_scene(name)
+    g = _golden(name)
+    o = oracle_lib.Oracle(sc)
+    K = len(g["energy"])
+    films = np.array([o.render(sample_begin=64 * k, sample_count=64, nthreads=4)["streak"] for k in range(K)])
+    r = compare_to_golden(films, g)
+    assert r["frac_z3"] < 0.02 and abs(r["mean_z"]) < 0.1 and r["max_z"] < 7.0, r
+    assert abs(r["energy_z"]) < 4.0 and r["one_sided_bins"] == 0, r
+    sc.flags &= ~S.FLAG_BIDIRECTIONAL
+    o = oracle_lib.Oracle(sc)
+    pt = np.mean([o.render(sample_begin=64 * k, sample_count=64, nthreads=4)["streak"].sum() for k in range(16)])
+    assert g["energy"].mean() > 1.15 * pt
+
+
+def test_oracle_bidirectional_scope(oracle_lib):
+    """Bidirectional connections are defined for time-sampling mode without a medium: the other
+    combinations are refused (the reference reads an uninitialised light sample outside
+    time-sampling mode and dereferences a null medium in time-sampled medium connections)."""
+    for name, flags in (("cornell", S.FLAG_BIDIRECTIONAL), ("medium", S.FLAG_BIDIRECTIONAL | S.FLAG_TIME_SAMPLING)):
+        sc = _golden_scene(name)
+        sc.flags = flags
+        with pytest.raises(ValueError):
+            oracle_lib.Oracle(sc)
+    sc = _golden_scene("bidir")
+    sc.max_bounces = 17
+    with pytest.raises(ValueError):
+        oracle_lib.Oracle(sc)
+
+
 def test_oracle_reference_harness_live(oracle_lib):
     """When the reference sources are present, rebuild and rerun the reference harness and
     check it still reproduces the committed golden statistics."""
