@@ -160,6 +160,22 @@ typedef struct tr_integrator {
  * (inverted time bounds), so films match the reference's distribution, heavy tail included. */
 #define TR_FLAG_TIME_SAMPLING 2u
 
+/* Bidirectional connections: light subpaths and eye-light vertex connections
+ * (BidirectionalPathTracing::set_path_tracing_only(false), reachable through the reference's
+ * API; src/Integrator/BidirectionalPathTracing.h:1099-1140, :975-1045, :697-897,
+ * src/Integrator/PathMIS.h:63-111).  Defined as the reference defines it: with
+ * TR_FLAG_TIME_SAMPLING, in scenes without a medium, Lambertian materials, max_bounces <= 16
+ * (other combinations return TR_ERR_NOT_SUPPORTED: outside time-sampling mode the reference's
+ * light subpath starts from an uninitialised light sample, and in a medium its time-sampled
+ * connections dereference a null medium).  Each path draws one light point, emits a light
+ * subpath from it and connects every eye vertex ie with every light vertex il for
+ * ie + il + 2 <= max_bounces, with the reference's MIS quantity (accumulated by addition,
+ * divided by) and its visibility convention (a pair counts when the segment between the
+ * vertices is blocked: World::intersects returns true on a hit and the reference connects on
+ * true).  Not with the learned proposal, multi-scene batches or tr_render_region_noalloc. */
+#define TR_FLAG_BIDIRECTIONAL 4u
+#define TR_BIDIR_MAX_BOUNCES 16u
+
 /* ---- ray-batch interface (correctness batch of World::first_intersection / intersects) --- */
 
 /* One ray = 8 floats: origin xyz, tnear, direction xyz, tfar.                               */

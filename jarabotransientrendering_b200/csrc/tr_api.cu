@@ -88,8 +88,22 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     if (it->sqrt_spp == 0 || it->incoming_samples == 0)
         return fail(TR_ERR_INVALID_ARGUMENT, "sqrt_spp and incoming_samples must be >= 1");
     if (it->max_bounces > kMaxBounces) return fail(TR_ERR_INVALID_ARGUMENT, "max_bounces must be <= 63");
-    if (it->flags & ~(TR_FLAG_ORTHONORMAL_FRAME | TR_FLAG_TIME_SAMPLING))
+    if (it->flags & ~(TR_FLAG_ORTHONORMAL_FRAME | TR_FLAG_TIME_SAMPLING | TR_FLAG_BIDIRECTIONAL))
         return fail(TR_ERR_INVALID_ARGUMENT, "unknown integrator flags");
+    if (it->flags & TR_FLAG_BIDIRECTIONAL) {
+        if (!(it->flags & TR_FLAG_TIME_SAMPLING))
+            return fail(TR_ERR_NOT_SUPPORTED, "bidirectional connections need TR_FLAG_TIME_SAMPLING (without it the "
+                                              "reference's light subpath starts from an uninitialised light sample "
+                                              "and all its connections are dropped: render without the flag)");
+        if (s->medium.enabled)
+            return fail(TR_ERR_NOT_SUPPORTED, "bidirectional connections in a medium are not defined by the reference "
+                                              "(its time-sampled connections dereference a null medium)");
+        if (it->max_bounces > TR_BIDIR_MAX_BOUNCES)
+            return fail(TR_ERR_NOT_SUPPORTED, "bidirectional connections support max_bounces <= 16");
+        for (uint32_t m = 0; m < s->num_materials; ++m)
+            if (s->materials[m].kind != TR_MAT_LAMBERTIAN)
+                return fail(TR_ERR_NOT_SUPPORTED, "bidirectional connections support Lambertian materials only");
+    }
     if (!std::isfinite(c->focal_distance)) return fail(TR_ERR_INVALID_ARGUMENT, "camera focal distance not finite");
     return TR_OK;
 }
@@ -113,7 +127,10 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     trk::Wave& w = x->wave;
     drop(w.ray_o); drop(w.ray_d); drop(w.thr); drop(w.rng); drop(w.hit); drop(w.q[0]); drop(w.q[1]);
     drop(w.sh_o); drop(w.sh_d); drop(w.sh_L); drop(w.rec); drop(w.rec_n);
-    const size_t R = std::max<uint32_t>(1u, x->integ.max_bounces);
+    size_t R = std::max<uint32_t>(1u, x->integ.max_bounces);
+    // records per slot: one next-event estimate per bounce, plus with light subpaths one per
+    // eye-light vertex pair with ie + il + 2 <= max_bounces
+    if (x->integ.flags & TR_FLAG_BIDIRECTIONAL) R += R * (R - 1) / 2;
     w.ray_o = x->alloc<float4>(capacity);
     w.ray_d = x->alloc<float4>(capacity);
     w.thr = x->alloc<float4>(capacity);
@@ -130,6 +147,31 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.cam_dist = x->alloc<float>(capacity);
     drop(w.target);
     w.target = (x->integ.flags & TR_FLAG_TIME_SAMPLING) ? x->alloc<float4>(capacity) : nullptr;
+    if (x->integ.flags & TR_FLAG_BIDIRECTIONAL) {
+        // light wave (own rays, queues, counters; shares target and ray counts) and the
+        // subpath vertex arrays
+        trk::Wave& lw = x->lwave;
+        trk::BidirWave& bd = x->bd;
+        drop(lw.ray_o); drop(lw.ray_d); drop(lw.thr); drop(lw.rng); drop(lw.hit); drop(lw.q[0]); drop(lw.q[1]);
+        drop(bd.lvert); drop(bd.evert); drop(bd.nl); drop(bd.ne); drop(bd.L0);
+        lw = trk::Wave{};
+        lw.ray_o = x->alloc<float4>(capacity);
+        lw.ray_d = x->alloc<float4>(capacity);
+        lw.thr = x->alloc<float4>(capacity);
+        lw.rng = x->alloc<unsigned long long>(capacity);
+        lw.hit = x->alloc<float4>(capacity);
+        lw.q[0] = x->alloc<uint32_t>(capacity);
+        lw.q[1] = x->alloc<uint32_t>(capacity);
+        if (!x->d_lcounters) x->d_lcounters = x->alloc<uint32_t>(trk::kCounters);
+        lw.counters = x->d_lcounters;
+        bd.nvert = std::max<uint32_t>(1u, x->integ.max_bounces) - 1u;
+        const size_t nv = std::max<uint32_t>(1u, bd.nvert);
+        bd.lvert = x->alloc<float4>(nv * 4 * capacity);
+        bd.evert = x->alloc<float4>(nv * 4 * capacity);
+        bd.nl = x->alloc<uint8_t>(capacity);
+        bd.ne = x->alloc<uint8_t>(capacity);
+        bd.L0 = x->alloc<float4>(capacity);
+    }
     if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = x->alloc<unsigned long long>(8);
@@ -175,6 +217,7 @@ trk::Params make_params(tr_ctx* x) {
     p.film.W = x->film.width; p.film.H = x->film.height; p.film.T = x->film.time_bins;
     p.film.exposure = x->film.exposure; p.film.offset = x->film.offset;
     p.wave = x->wave;
+    p.bd = x->bd;
     p.seed = x->integ.seed;
     p.max_bounces = x->integ.max_bounces;
     p.sqrt_spp = x->integ.sqrt_spp;
@@ -204,10 +247,13 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     const uint32_t win_w = x1 - x0, win_h = y1 - y0;
     const uint64_t win_pix = (uint64_t)win_w * win_h;
     const uint64_t total_slots = win_pix * (uint64_t)ns_total * ninc;
-    uint32_t cap = (uint32_t)std::min<uint64_t>(total_slots, kDefaultCapacity);
+    // with light subpaths a slot also holds two subpaths' vertices and its connection records
+    const uint32_t cap_max = (x->integ.flags & TR_FLAG_BIDIRECTIONAL) ? kDefaultCapacity / 2 : kDefaultCapacity;
+    uint32_t cap = (uint32_t)std::min<uint64_t>(total_slots, cap_max);
     cap = std::max<uint32_t>(cap, ninc);
     ensure_wave(x, cap);
     const bool guided = x->guide != nullptr;
+    const bool bidir = (x->integ.flags & TR_FLAG_BIDIRECTIONAL) != 0;
     if (guided) {
         ensure_guided(x, cap);
         // about 1.5 guided vertices per path; keep enough of them to fill the training pool
@@ -253,6 +299,22 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             p.batch.n_slots = npix * per_pix;
             TR_CUDA(cudaMemsetAsync(x->wave.counters, 0, trk::kCounters * sizeof(uint32_t), strm));
             timed(0, [&] { return trk::launch_raygen(p, strm); });
+            if (bidir) {
+                // the light subpaths, on the light wave, from the light points raygen drew
+                trk::Params pl = p;
+                pl.wave = x->lwave;
+                pl.wave.target = x->wave.target;
+                pl.wave.stats = x->wave.stats;
+                pl.wave.capacity = x->wave.capacity;
+                TR_CUDA(cudaMemsetAsync(pl.wave.counters, 0, trk::kCounters * sizeof(uint32_t), strm));
+                timed(0, [&] { return trk::launch_light_raygen(pl, strm); });
+                for (uint32_t d = 0; d < x->bd.nvert; ++d) {
+                    timed(1, [&] { return trk::launch_extend(pl, (int)d, x->trace_grid, strm); });
+                    timed(2, [&] { return trk::launch_light_shade(pl, (int)d, strm); });
+                }
+                launches += 1 + 2ull * x->bd.nvert;
+                ext_l += x->bd.nvert;
+            }
             for (uint32_t d = 0; d < x->integ.max_bounces; ++d) {
                 timed(1, [&] { return trk::launch_extend(p, (int)d, x->trace_grid, strm); });
                 timed(2, [&] { return trk::launch_shade(p, (int)d, strm); });
@@ -265,6 +327,10 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             if (guided && x->guide_pool) {
                 TR_CUDA(trk::launch_train_gather(p, x->pool_state, strm));
                 launches += 2;
+            }
+            if (bidir && x->bd.nvert) {
+                timed(3, [&] { return trk::launch_connect(p, x->connect_grid, strm); });
+                launches += 1;
             }
             timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm); });
             for (uint32_t b = 0; b < x->film.bounce_films; ++b)
@@ -480,6 +546,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         }
 
         x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);
+        if (it->flags & TR_FLAG_BIDIRECTIONAL) x->connect_grid = trk::connect_grid_size(device, x->bvh_depth);
         int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
         x->splat_g = std::max(1, std::min(g, 16));
         x->d_cursor = x->alloc<uint32_t>(1);
@@ -754,6 +821,8 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
         return fail(TR_ERR_INVALID_ARGUMENT, "pixel window out of range or empty");
     if (ns == 0) return TR_OK;
     if (s0 + ns > (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "camera sample index must stay below 2^32");
+    if (x->integ.flags & TR_FLAG_BIDIRECTIONAL)
+        return fail(TR_ERR_NOT_SUPPORTED, "light subpaths need their vertex arrays: render with tr_render");
     if (x->integ.max_bounces > TR_NOALLOC_MAX_BOUNCES)
         return fail(TR_ERR_INVALID_ARGUMENT, "tr_render_region_noalloc supports max_bounces <= " +
                                                  std::to_string(TR_NOALLOC_MAX_BOUNCES) + " (scene has " +
@@ -1037,6 +1106,8 @@ extern "C" tr_status tr_set_guide(tr_ctx* x, tr_guide* g, float mix_prob, float 
     if (!g) { x->guide = nullptr; return TR_OK; }
     if (!(x->integ.flags & TR_FLAG_ORTHONORMAL_FRAME))
         return fail(TR_ERR_INVALID_ARGUMENT, "guided rendering needs TR_FLAG_ORTHONORMAL_FRAME (MIS needs the exact BSDF density)");
+    if (x->integ.flags & TR_FLAG_BIDIRECTIONAL)
+        return fail(TR_ERR_NOT_SUPPORTED, "the learned proposal is not combined with light subpaths");
     if (g->device != x->device) return fail(TR_ERR_INVALID_ARGUMENT, "guide and context are on different devices");
     if (!(mix_prob > 0.0f && mix_prob < 1.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "mix_prob must be in (0, 1)");
     if (!(lr >= 0.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "learning rate must be >= 0");

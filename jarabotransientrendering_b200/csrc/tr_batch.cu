@@ -351,6 +351,8 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
             return fail(TR_ERR_INVALID_ARGUMENT, "all contexts of a batch must be on one device");
         if (contexts[i]->film.bounce_films)
             return fail(TR_ERR_NOT_SUPPORTED, "contexts with bounce films render through tr_render, not in a batch");
+        if (contexts[i]->integ.flags & TR_FLAG_BIDIRECTIONAL)
+            return fail(TR_ERR_NOT_SUPPORTED, "contexts with light subpaths render through tr_render, not in a batch");
     }
     tr_batch* b = new (std::nothrow) tr_batch();
     if (!b) return fail(TR_ERR_OUT_OF_MEMORY, "host allocation");

@@ -129,6 +129,10 @@ struct tr_ctx {
 
     // wavefront state
     trk::Wave wave{};
+    trk::Wave lwave{};                      // light subpaths (TR_FLAG_BIDIRECTIONAL)
+    trk::BidirWave bd{};
+    uint32_t* d_lcounters = nullptr;
+    int connect_grid = 0;
     int trace_grid = 0;
     int splat_g = 1;
 

@@ -168,8 +168,9 @@ __global__ void __launch_bounds__(256) k_raygen(const __grid_constant__ Params p
             const float xu = pcg_float(r), xv = pcg_float(r);
             tg = (tg + f3of(__ldg(L + 2)) * xu) + f3of(__ldg(L + 3)) * xv;
         }
-        p.wave.target[i] = make_float4(tg.x, tg.y, tg.z, 0.0f);
+        p.wave.target[i] = make_float4(tg.x, tg.y, tg.z, __uint_as_float(lsel));
     }
+    if (p.bd.ne) p.bd.ne[i] = 0;
     float dsamp = __int_as_float(0x7f800000);
     if (sc.medium) dsamp = -tr_log(pcg_float(r)) / sc.lambda;
 
@@ -533,6 +534,20 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
                             }
                         }
                     }
+                    if constexpr (kTimeSampling) {
+                        // ---- bidirectional connections: keep the eye vertex (value, pdf,
+                        // delay) for k_connect (connect_paths, BidirectionalPathTracing.h:
+                        // 1018-1041); scenes without a medium, so every vertex is a surface ----
+                        if ((flags & kFlagBidirectional) && surface && (uint32_t)depth + 2u <= max_bounces) {
+                            const size_t cap = p.wave.capacity;
+                            float4* v = p.bd.evert + (size_t)depth * 4 * cap + slot;
+                            v[0] = make_float4(pos.x, pos.y, pos.z, time);
+                            v[cap] = make_float4(nrm.x, nrm.y, nrm.z, ptot);
+                            v[2 * cap] = make_float4(kd.x, kd.y, kd.z, 0.0f);
+                            v[3 * cap] = make_float4(f.x, f.y, f.z, 0.0f);
+                            p.bd.ne[slot] = (uint8_t)(depth + 1);
+                        }
+                    }
                     if ((uint32_t)depth + 1u < max_bounces) {
                         // ---- Russian roulette (none in time-sampling mode: the walk ends when
                         // its time passes the film's, above) ----
@@ -881,6 +896,309 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_user(Sce
 }
 
 // -----------------------------------------------------------------------------------------
+// Bidirectional connections (BidirectionalPathTracing with set_path_tracing_only(false)) in
+// time-sampling mode, scenes without a medium.  Per batch: k_raygen draws the path's light
+// point (as for time sampling); k_light_raygen emits the light subpath from it on the light
+// wave (its own rays, queues, counters and PCG32 stream); k_extend + k_light_shade walk it,
+// storing its vertices; the eye walk (k_extend / k_shade / k_shadow) stores the eye vertices
+// next to its next-event estimates; k_connect connects them and appends splat records.
+// -----------------------------------------------------------------------------------------
+
+// slot -> (pixel, camera sample, incoming sample) of a single-scene batch
+struct SlotId { uint32_t pixel; unsigned long long s; uint32_t j; };
+__device__ __forceinline__ SlotId slot_id(const Params& p, uint32_t i) {
+    const Batch& B = p.batch;
+    const uint32_t per_pix = B.ns * B.ninc;
+    const uint32_t li = i - B.slot_begin;
+    const uint32_t pl = li / per_pix;
+    const uint32_t rem = li - pl * per_pix;
+    const uint32_t sl = rem / B.ninc;
+    const uint32_t wpix = B.pix_begin + pl;
+    SlotId r;
+    r.pixel = (B.win_y0 + wpix / B.win_w) * p.film.W + (B.win_x0 + wpix % B.win_w);
+    r.s = B.s0 + sl;
+    r.j = rem - sl * B.ninc;
+    return r;
+}
+
+// Lambertian direction at a surface vertex, in the frame the eye walk uses (orthonormal frame
+// with TR_FLAG_ORTHONORMAL_FRAME, else Intersection::set_coordinate_system's, Intersection.h:
+// 167-178); same operations as k_shade's.
+__device__ __forceinline__ void lambert_sample(uint32_t flags, f3 nrm, f3 kd, float x1, float x2, f3& nd, f3& fa,
+                                               float& pa) {
+    float sp, cp;
+    tr_sincos2pi(x1, &sp, &cp);
+    const float ct = sqrtf(x2);
+    const float stt = sqrtf(1.0f - ct * ct);
+    if (flags & kFlagOrthoFrame) {
+        const Frame3 Fr = make_frame(nrm);
+        nd = to_world(Fr, mk(cp * stt, sp * stt, ct));
+        fa = mk((kd.x * kInvPi) * ct, (kd.y * kInvPi) * ct, (kd.z * kInvPi) * ct);
+    } else {
+        const f3 aux = fabsf(nrm.x) > fabsf(nrm.z) ? mk(-nrm.y, nrm.x, nrm.z) : mk(0.0f, -nrm.z, nrm.y);
+        const f3 tv = normalize(aux);
+        const f3 tu = cross(nrm, tv);
+        const f3 w = ((tu * (cp * stt)) + (nrm * ct)) + (tv * (sp * stt));
+        nd = normalize(w);
+        const float ca = fabsf(dot(nrm, nd));
+        fa = mk((kd.x * kInvPi) * ca, (kd.y * kInvPi) * ca, (kd.z * kInvPi) * ca);
+    }
+    pa = ct * kInvPi;
+}
+
+// light subpath emission (generate_path FROM_LIGHT started at BidirectionalPathTracing.h:
+// 1121-1124): direction from PointLightSource::sample (uniform sphere, PointLightSource.h:
+// 174-183, Sampling.h:80-94) or RectangularAreaLightSource::sample (cosine lobe about the
+// normal, RectangularAreaLightSource.h:252-276, Sampling.h:131-143); initial pdf (1 / lights) x
+// emission pdf; subpath value = emitted intensity (times cos for the rectangle).
+__global__ void __launch_bounds__(256) k_light_raygen(const __grid_constant__ Params pl) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pl.batch.n_slots) return;
+    const SlotId id = slot_id(pl, i);
+    Pcg rl;
+    pcg_seed(rl, pl.seed + (unsigned long long)(id.j + 1) * kGolden64 + kLightStateSalt,
+             cam_id(id.pixel, id.s) ^ kLightSeqSalt);
+    const float4 tg = pl.wave.target[i];
+    const SceneDev& sc = pl.scene;
+    const float4* L = sc.lights + 5 * __float_as_uint(tg.w);
+    const float4 L0 = __ldg(L), L1 = __ldg(L + 1);
+    const float e1 = pcg_float(rl), e2 = pcg_float(rl);
+    float sp, cp;
+    tr_sincos2pi(e1, &sp, &cp);
+    f3 dir, val;
+    float pdf_dir;
+    if (__float_as_uint(L0.w) == 1u) {
+        const float ct = sqrtf(e2);
+        const float stt = sqrtf(1.0f - ct * ct);
+        const f3 ln = f3of(__ldg(L + 4));
+        dir = mh_from_y(ln, mk(cp * stt, ct, sp * stt));
+        pdf_dir = ct * kInvPi;
+        const float dl = dot(dir, ln);
+        val = mk(L1.x * dl, L1.y * dl, L1.z * dl);
+        pdf_dir = (1.0f / L1.w) * pdf_dir;
+    } else {
+        const float ct = (float)(1.0 - 2.0 * (double)e2);
+        const float stt = sqrtf(1.0f - ct * ct);
+        dir = mk(cp * stt, ct, sp * stt);
+        pdf_dir = kInv4Pi;
+        val = mk(L1.x, L1.y, L1.z);
+    }
+    const float pi = (1.0f / (float)sc.num_lights) * pdf_dir;
+    pl.wave.ray_o[i] = make_float4(tg.x, tg.y, tg.z, __int_as_float(0x7f800000));
+    pl.wave.ray_d[i] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+    pl.wave.thr[i] = make_float4(1.0f, 1.0f, 1.0f, pi);
+    pl.wave.rng[i] = rl.state;
+    pl.bd.L0[i] = make_float4(val.x, val.y, val.z, 0.0f);
+    pl.bd.nl[i] = 0;
+}
+
+// one light subpath vertex per queued slot: throughput over the step's pdf, delay, stored
+// while within the film (TotalTime termination, no Russian roulette); then the next Lambertian
+// direction.  The walk is in vacuum (the reference's light ray carries no medium).
+__global__ void __launch_bounds__(256) k_light_shade(const __grid_constant__ Params pl, int depth) {
+    const uint32_t n = depth == 0 ? pl.batch.n_slots : pl.wave.counters[cnt_ext(depth)];
+    const uint32_t* qin = pl.wave.q[depth & 1];
+    uint32_t* qout = pl.wave.q[(depth + 1) & 1];
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const SceneDev& sc = pl.scene;
+    const float total_time = (float)pl.film.T * pl.film.exposure + pl.film.offset;
+    const size_t cap = pl.wave.capacity;
+    for (uint32_t base = warp_global * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t idx = base + lane;
+        bool want_next = false;
+        uint32_t slot = 0;
+        if (idx < n) {
+            slot = depth == 0 ? idx : qin[idx];
+            const float4 h = pl.wave.hit[slot];
+            const uint32_t tid = __float_as_uint(h.y);
+            if (tid != kInvalid) {
+                const float4 ro = pl.wave.ray_o[slot], rd = pl.wave.ray_d[slot], th = pl.wave.thr[slot];
+                const float dist = h.x;
+                const f3 f = mk(th.x / th.w, th.y / th.w, th.z / th.w);
+                const float time = rd.w + dist;
+                if (!(time > total_time)) {
+                    const f3 pos = mk(ro.x, ro.y, ro.z) + mk(rd.x, rd.y, rd.z) * dist;
+                    const float4 ng = __ldg(&sc.tri_ng[tid]);
+                    const float4 m = __ldg(&sc.mats[__float_as_uint(ng.w)]);
+                    const f3 nrm = mk(ng.x, ng.y, ng.z), kd = mk(m.x, m.y, m.z);
+                    float4* v = pl.bd.lvert + (size_t)depth * 4 * cap + slot;
+                    v[0] = make_float4(pos.x, pos.y, pos.z, time);
+                    v[cap] = make_float4(nrm.x, nrm.y, nrm.z, th.w);
+                    v[2 * cap] = make_float4(kd.x, kd.y, kd.z, 0.0f);
+                    v[3 * cap] = make_float4(f.x, f.y, f.z, 0.0f);
+                    pl.bd.nl[slot] = (uint8_t)(depth + 1);
+                    if ((uint32_t)depth + 1u < pl.bd.nvert) {
+                        const SlotId id = slot_id(pl, slot);
+                        Pcg rl;
+                        rl.state = pl.wave.rng[slot];
+                        rl.inc = ((cam_id(id.pixel, id.s) ^ kLightSeqSalt) << 1u) | 1ull;
+                        const float x1 = pcg_float(rl), x2 = pcg_float(rl);
+                        f3 nd, fa;
+                        float pa;
+                        lambert_sample(pl.flags, nrm, kd, x1, x2, nd, fa, pa);
+                        const f3 fn = mulv(f, fa);
+                        pl.wave.ray_o[slot] = make_float4(pos.x, pos.y, pos.z, __int_as_float(0x7f800000));
+                        pl.wave.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, time);
+                        pl.wave.thr[slot] = make_float4(fn.x, fn.y, fn.z, 1.0f * pa);
+                        pl.wave.rng[slot] = rl.state;
+                        want_next = true;
+                    }
+                }
+            }
+        }
+        const unsigned mn = __ballot_sync(kFull, want_next);
+        uint32_t bn = 0;
+        if (lane == 0 && mn) bn = atomicAdd(&pl.wave.counters[cnt_ext(depth + 1)], (uint32_t)__popc(mn));
+        bn = __shfl_sync(kFull, bn, 0);
+        if (want_next) qout[bn + (uint32_t)__popc(mn & lanemask_lt())] = slot;
+    }
+}
+
+struct BVert { f3 pos; float time; f3 n; float pdf; f3 kd; f3 f; };
+__device__ __forceinline__ BVert load_vert(const float4* base, uint32_t v, size_t cap, uint32_t slot) {
+    const float4* q = base + (size_t)v * 4 * cap + slot;
+    const float4 a = q[0], b = q[cap], c = q[2 * cap], d = q[3 * cap];
+    BVert r;
+    r.pos = mk(a.x, a.y, a.z); r.time = a.w;
+    r.n = mk(b.x, b.y, b.z); r.pdf = b.w;
+    r.kd = mk(c.x, c.y, c.z);
+    r.f = mk(d.x, d.y, d.z);
+    return r;
+}
+__device__ __forceinline__ f3 load_pos(const float4* base, uint32_t v, size_t cap, uint32_t slot) {
+    const float4 a = base[(size_t)v * 4 * cap + slot];
+    return mk(a.x, a.y, a.z);
+}
+__device__ __forceinline__ float4 load_npdf(const float4* base, uint32_t v, size_t cap, uint32_t slot) {
+    return base[((size_t)v * 4 + 1) * cap + slot];
+}
+
+// PathMIS::connection_probability (PathMIS.h:49-60) for Lambertian vertices: the density with
+// which the vertex at `from` (normal nf) samples the direction towards `to`.
+__device__ __forceinline__ float conn_prob(f3 from, f3 nf, f3 to) {
+    const f3 d = normalize(to - from);
+    const float c = dot(d, nf);
+    return (c > 0.0f ? c : 0.0f) * kInvPi;
+}
+
+// PathMIS::compute_weight with beta = 1 (PathMIS.h:63-111): ratios accumulated by addition
+// along each subpath, as the reference does; the caller divides by the result
+// (BidirectionalPathTracing.h:1034).  t = eye vertex index, s = light vertex index.
+__device__ float mis_quantity(const Params& p, uint32_t slot, uint32_t t, uint32_t s, f3 et_pos, float4 et_npdf,
+                              f3 ls_pos, float4 ls_npdf) {
+    const size_t cap = p.wave.capacity;
+    float iw = 1.0f;
+    if (s > 1) {
+        const float p_s_1 = conn_prob(et_pos, mk(et_npdf.x, et_npdf.y, et_npdf.z), ls_pos) / ls_npdf.w;
+        iw = iw + p_s_1;
+        float p_i_0 = p_s_1;
+        f3 nxt_pos = ls_pos;
+        f3 nxt_n = mk(ls_npdf.x, ls_npdf.y, ls_npdf.z);
+        for (uint32_t i = s - 1; i > 0; --i) {
+            const f3 pos_i = load_pos(p.bd.lvert, i, cap, slot);
+            const float4 np_i = load_npdf(p.bd.lvert, i, cap, slot);
+            float p_i = conn_prob(nxt_pos, nxt_n, pos_i);
+            p_i = p_i_0 + p_i / np_i.w;
+            iw = iw + p_i;
+            p_i_0 = p_i;
+            nxt_pos = pos_i;
+            nxt_n = mk(np_i.x, np_i.y, np_i.z);
+        }
+    }
+    if (t > 1) {
+        const float p_t_1 = conn_prob(ls_pos, mk(ls_npdf.x, ls_npdf.y, ls_npdf.z), et_pos) / et_npdf.w;
+        iw = iw + p_t_1;
+        float p_i_0 = p_t_1;
+        f3 nxt_pos = et_pos;
+        f3 nxt_n = mk(et_npdf.x, et_npdf.y, et_npdf.z);
+        for (uint32_t i = t - 1; i > 0; --i) {
+            const f3 pos_i = load_pos(p.bd.evert, i, cap, slot);
+            const float4 np_i = load_npdf(p.bd.evert, i, cap, slot);
+            float p_i = conn_prob(nxt_pos, nxt_n, pos_i);
+            p_i = p_i_0 + p_i / np_i.w;
+            iw = iw + p_i;
+            p_i_0 = p_i;
+            nxt_pos = pos_i;
+            nxt_n = mk(np_i.x, np_i.y, np_i.z);
+        }
+    }
+    return (float)(1.0 / (double)iw);
+}
+
+// Eye-light vertex connections of one path slot per thread (transient connect_paths,
+// BidirectionalPathTracing.h:1018-1041; connect_vertices' shadow connection, :840-871): pairs
+// with ie + il + 2 <= max_bounces whose delays fit the film; the pair counts when
+// World::intersects reports a blocker between the two vertices (the query returns true on a
+// hit, World.h:617-639 / 693-697, and the reference connects on true); value
+// fe * (fv * (f_l * L0)) / w, time = distance + both delays, bounce ie + il + 1.  Records go
+// after the slot's next-event records, for k_splat.
+__global__ void __launch_bounds__(kTraceBlock, 4) k_connect(const __grid_constant__ Params p) {
+    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
+    const SceneDev& sc = p.scene;
+    const FilmDev& film = p.film;
+    const size_t cap = p.wave.capacity;
+    const float total_time = (float)film.T * film.exposure + film.offset;
+    const float inv_inc = 1.0f / (float)p.batch.ninc;
+    unsigned long long rays = 0, splats = 0;
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < p.batch.n_slots;
+         slot += gridDim.x * blockDim.x) {
+        const uint32_t ne = p.bd.ne[slot], nl = p.bd.nl[slot];
+        if (ne == 0 || nl == 0) continue;
+        const float4 L0 = p.bd.L0[slot];
+        const float cam_d = film.unwarp ? p.wave.cam_dist[slot] : 0.0f;
+        uint32_t k = p.wave.rec_n[slot];
+        for (uint32_t ie = 0; ie < ne; ++ie) {
+            const BVert E = load_vert(p.bd.evert, ie, cap, slot);
+            const float4 e_npdf = make_float4(E.n.x, E.n.y, E.n.z, E.pdf);
+            for (uint32_t il = 0; il < nl; ++il) {
+                if (ie + il + 2u > p.max_bounces) break;
+                const BVert Lv = load_vert(p.bd.lvert, il, cap, slot);
+                if (E.time + Lv.time > total_time) break;
+                f3 l2e = E.pos - Lv.pos;
+                const float dd = sqrtf(dot(l2e, l2e));
+                l2e = divs(l2e, dd);
+                if ((dd + E.time) + Lv.time > total_time) continue;
+                WRay r;
+                wray_setup(r, Lv.pos, l2e, kSigmaVis);
+                float th, tu, tv;
+                ++rays;
+                const uint32_t hid = traverse<true>(sc, r, dd - kSigmaVis, th, tu, tv, stack + threadIdx.x, kTraceBlock);
+                if (hid == kInvalid) continue;
+                float ce = -dot(l2e, E.n), cl = dot(l2e, Lv.n);
+                ce = ce > 0.0f ? ce : 0.0f;
+                cl = cl > 0.0f ? cl : 0.0f;
+                const f3 fe = mk((E.kd.x * kInvPi) * ce, (E.kd.y * kInvPi) * ce, (E.kd.z * kInvPi) * ce);
+                const f3 fl = mk((Lv.kd.x * kInvPi) * cl, (Lv.kd.y * kInvPi) * cl, (Lv.kd.z * kInvPi) * cl);
+                const float att = 1.0f / (dd * dd);
+                const f3 fv = mk((fe.x * fl.x) * att, (fe.y * fl.y) * att, (fe.z * fl.z) * att);
+                const float w = mis_quantity(p, slot, ie, il, E.pos, e_npdf, Lv.pos,
+                                             make_float4(Lv.n.x, Lv.n.y, Lv.n.z, Lv.pdf));
+                const float Lr = ((E.f.x * (fv.x * (Lv.f.x * L0.x))) / w) * inv_inc;
+                const float Lg = ((E.f.y * (fv.y * (Lv.f.y * L0.y))) / w) * inv_inc;
+                const float Lb = ((E.f.z * (fv.z * (Lv.f.z * L0.z))) / w) * inv_inc;
+                const float tt = dd + (E.time + Lv.time);
+                const float tc = film.unwarp ? tt - cam_d : tt;
+                const float ps = (tc - film.offset) / film.exposure;
+                const bool inside = ps < (float)film.T && ps >= 0.0f;
+                if (!(inside || film.nbounce)) continue;
+                const bool fin = finite3(Lr, Lg, Lb);
+                const uint32_t bin = inside ? (uint32_t)floorf(ps) : kBinOutside;
+                const uint32_t bounce = ie + il + 1u;
+                p.wave.rec[(size_t)k * cap + slot] = fin ? make_float4(Lr, Lg, Lb, __uint_as_float(bin | (bounce << 24)))
+                                                         : make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(bin | (bounce << 24)));
+                ++k;
+                ++splats;
+            }
+        }
+        p.wave.rec_n[slot] = (uint8_t)k;
+    }
+    if (rays) atomicAdd(&p.wave.stats[1], rays);
+    if (splats) atomicAdd(&p.wave.stats[2], splats);
+}
+
+// -----------------------------------------------------------------------------------------
 // launchers
 // -----------------------------------------------------------------------------------------
 size_t trace_smem_bytes(uint32_t bvh_depth) { return (size_t)(bvh_depth + 1u) * kTraceBlock * sizeof(int); }
@@ -977,6 +1295,34 @@ cudaError_t launch_splat(const Params& p, int G, cudaStream_t s, int bsel) {
 cudaError_t launch_bounce_weights(const Params& p, cudaStream_t s) {
     const uint32_t ncs = p.batch.npix * p.batch.ns;
     k_bounce_weights<<<std::max(1u, std::min(4096u, (ncs + 255) / 256)), 256, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_light_raygen(const Params& pl, cudaStream_t s) {
+    const uint32_t n = pl.batch.n_slots;
+    k_light_raygen<<<std::max(1u, (n + 255) / 256), 256, 0, s>>>(pl);
+    return cudaGetLastError();
+}
+cudaError_t launch_light_shade(const Params& pl, int depth, cudaStream_t s) {
+    int dev = 0, grid = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&grid, cudaDevAttrMultiProcessorCount, dev);
+    grid *= 8;
+    const uint32_t need = (pl.batch.n_slots + 255) / 256;
+    if ((uint32_t)grid > need) grid = (int)need;
+    k_light_shade<<<std::max(1, grid), 256, 0, s>>>(pl, depth);
+    return cudaGetLastError();
+}
+int connect_grid_size(int device, uint32_t bvh_depth) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_connect, kTraceBlock, trace_smem_bytes(bvh_depth));
+    return std::max(1, sms * std::max(1, per_sm));
+}
+cudaError_t launch_connect(const Params& p, int grid, cudaStream_t s) {
+    const uint32_t need = (p.batch.n_slots + kTraceBlock - 1) / kTraceBlock;
+    if ((uint32_t)grid > need) grid = (int)need;
+    k_connect<<<std::max(1, grid), kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p);
     return cudaGetLastError();
 }
 

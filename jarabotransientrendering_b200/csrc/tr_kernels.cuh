@@ -34,6 +34,23 @@ struct SceneDev {
 
 constexpr uint32_t kFlagOrthoFrame = 1u;   // TR_FLAG_ORTHONORMAL_FRAME
 constexpr uint32_t kFlagTimeSampling = 2u; // TR_FLAG_TIME_SAMPLING
+constexpr uint32_t kFlagBidirectional = 4u; // TR_FLAG_BIDIRECTIONAL
+constexpr uint32_t kBidirMaxBounces = 16u;
+
+// Bidirectional connections (light subpaths; all null unless TR_FLAG_BIDIRECTIONAL).  Subpath
+// vertices are [vertex][4][capacity] float4 records, slot-minor so a warp's loads coalesce:
+// (position, delay) (geometric normal, vertex pdf) (Lambertian albedo, 0) (vertex value, 0).
+struct BidirWave {
+    float4* lvert;            // light subpath vertices
+    float4* evert;            // eye subpath vertices
+    uint8_t* nl;              // light vertices per slot
+    uint8_t* ne;              // eye vertices per slot
+    float4* L0;               // light subpath value (emitted intensity, times cos for a rectangle)
+    uint32_t nvert;           // vertices kept per subpath: max_bounces - 1
+};
+// state of the light subpath stream (another PCG32 state and increment than the eye walk's)
+constexpr unsigned long long kLightStateSalt = 0xD1B54A32D192ED03ULL;
+constexpr unsigned long long kLightSeqSalt = 0x3C6EF372FE94F82AULL;
 
 // Guided mode state (all null when rendering without the learned proposal).
 struct GuideWave {
@@ -153,6 +170,7 @@ struct Params {
     uint32_t flags;
     GuideWave guide;
     MultiDev multi;              // used by the kMulti kernel variants only
+    BidirWave bd;                // light subpaths and vertex connections
 };
 
 // ---- per-slot view (device) ------------------------------------------------------------
@@ -198,6 +216,12 @@ cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s, int bsel = -1);
 // per-bounce film weights: +1 per camera sample with a record of that bounce film
 cudaError_t launch_bounce_weights(const Params& p, cudaStream_t s);
+// bidirectional connections: light subpath generation on the light wave `pl` (its own rays,
+// queues and counters; target, stats and vertex arrays shared), then the connections
+cudaError_t launch_light_raygen(const Params& pl, cudaStream_t s);
+cudaError_t launch_light_shade(const Params& pl, int depth, cudaStream_t s);
+cudaError_t launch_connect(const Params& p, int grid, cudaStream_t s);
+int connect_grid_size(int device, uint32_t bvh_depth);      // resident k_connect blocks
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);

@@ -507,20 +507,23 @@ class StratifiedSampler:
 
 class BidirectionalPathTracing:
     """Path tracing with next-event estimation, the mode the reference CLI runs
-    (BidirectionalPathTracing.h:122-137; ProgramParams.h:162-164)."""
+    (BidirectionalPathTracing.h:122-137; ProgramParams.h:162-164), or, after
+    ``set_path_tracing_only(False)``, with light subpaths and eye-light vertex connections
+    (TR_FLAG_BIDIRECTIONAL: with a time-sampling renderer, scenes without a medium)."""
 
     def __init__(self, world, incoming_samples=1, f_log=None, film=None):
         self.world = world
         self.incoming_samples = int(incoming_samples)
         self.max_path_size = 30
         self.seed = 0
+        self.path_tracing_only = True
 
     def set_max_path_size(self, n):
         self.max_path_size = int(n)
 
     def set_path_tracing_only(self, on):
-        if not on:
-            raise NotImplementedError("bidirectional connections are not part of the GPU path")
+        # BidirectionalPathTracing::set_path_tracing_only (BidirectionalPathTracing.h:214-217)
+        self.path_tracing_only = bool(on)
 
     def set_seed(self, seed):
         self.seed = int(seed)
@@ -550,6 +553,8 @@ class TransientRenderer:
         scene.components = int(film.components)
         if self.time_sampling:
             scene.flags |= S.FLAG_TIME_SAMPLING
+        if not integrator.path_tracing_only:
+            scene.flags |= S.FLAG_BIDIRECTIONAL
         ctx = Context(scene, self.device)
         ctx.render(0, scene.spp)
         f = ctx.film()
