@@ -426,33 +426,50 @@ def main():
         pt = torch.from_numpy(t_).pin_memory().numpy()
         pm = torch.from_numpy(m).pin_memory().numpy()
         H, W, Tb = sc.height, sc.width, sc.time_bins
-        streak = torch.empty((H, W, Tb, 3), dtype=torch.float64, pin_memory=True).numpy()
-        steady = torch.empty((H, W, 3), dtype=torch.float64, pin_memory=True).numpy()
-        weight = torch.empty((H, W), dtype=torch.float64, pin_memory=True).numpy()
+
+        def host_film(dt):
+            return (torch.empty((H, W, Tb, 3), dtype=dt, pin_memory=True).numpy(),
+                    torch.empty((H, W, 3), dtype=dt, pin_memory=True).numpy(),
+                    torch.empty((H, W), dtype=dt, pin_memory=True).numpy())
+
+        def e2e_run(arrays, steps):
+            """tr_create + tr_render_film (film rows streamed into the pinned arrays while the
+            remaining rows render) + tr_destroy; the first iteration warms the allocator."""
+            times, phases = [], []
+            for i in range(steps + 1):
+                t0 = time.perf_counter()
+                c = T.Context(sc, device=local, arrays=(pv, pt, pm))
+                t1 = time.perf_counter()
+                c.render_film(0, spp, *arrays)
+                t2 = time.perf_counter()
+                bvh_ms = c.stats()["bvh_build_ms"]
+                c.close()
+                t3 = time.perf_counter()
+                times.append(t3 - t0)
+                phases.append({"create_ms": (t1 - t0) * 1e3, "bvh_build_ms": bvh_ms,
+                               "render_and_film_d2h_ms": (t2 - t1) * 1e3, "destroy_ms": (t3 - t2) * 1e3})
+            return sum(times[1:]) / steps, phases[-1]
+
         e2e_steps = max(1, min(args.steps, 3))
-        times, phases = [], []
-        for i in range(e2e_steps + 1):
-            t0 = time.perf_counter()
-            c = T.Context(sc, device=local, arrays=(pv, pt, pm))
-            t1 = time.perf_counter()
-            c.render(0, spp)
-            t2 = time.perf_counter()
-            c.film_into(streak, steady, weight)
-            t3 = time.perf_counter()
-            bvh_ms = c.stats()["bvh_build_ms"]
-            c.close()
-            t4 = time.perf_counter()
-            times.append(t4 - t0)
-            phases.append({"create_ms": (t1 - t0) * 1e3, "bvh_build_ms": bvh_ms, "render_ms": (t2 - t1) * 1e3,
-                           "film_d2h_ms": (t3 - t2) * 1e3, "destroy_ms": (t4 - t3) * 1e3})
-        et = sum(times[1:]) / e2e_steps          # first iteration warms the allocator
+        f32 = host_film(torch.float32)
+        et, ph = e2e_run(f32, e2e_steps)
+        d2h = sum(a.nbytes for a in f32)
+        del f32
+        f64 = host_film(torch.float64)
+        et64, ph64 = e2e_run(f64, 1)
+        d2h64 = sum(a.nbytes for a in f64)
+        del f64
         out["e2e"] = {"value": paths_per_step * world / et, "unit": "paths/s",
                       "h2d_bytes_per_step": int(pv.nbytes + pt.nbytes + pm.nbytes),
-                      "d2h_bytes_per_step": int(streak.nbytes + steady.nbytes + weight.nbytes),
+                      "d2h_bytes_per_step": int(d2h),
                       "ms_per_step": et * 1e3,
-                      "phases_last_step": phases[-1],
+                      "film": "FP32 sums (the reference's film precision)",
+                      "phases_last_step": ph,
+                      "fp64_film": {"value": paths_per_step * world / et64, "d2h_bytes_per_step": int(d2h64),
+                                    "ms_per_step": et64 * 1e3, "phases": ph64},
                       "includes": "tr_create (scene H2D from pinned memory + host BVH build + film alloc), "
-                                  "tr_render, tr_get_film (D2H into pinned memory), tr_destroy"}
+                                  "tr_render_film (render with the film streamed into pinned host memory as "
+                                  "pixel rows complete), tr_destroy"}
     else:
         ctx.close()
 

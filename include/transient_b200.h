@@ -237,6 +237,20 @@ tr_status tr_clear_film(tr_ctx* ctx);
  * Dividing streak/steady by weight gives what StreakCameraFilm::average_and_save_slice writes. */
 tr_status tr_get_film(tr_ctx* ctx, double* streak, double* steady, double* weight);
 
+/* Renders like tr_render and delivers the film's accumulated sums (all samples rendered so
+ * far, same layout as tr_get_film) into host memory, copying each group of pixel rows as soon
+ * as its last samples are splatted, so the device-to-host transfer overlaps the rendering of
+ * the remaining rows -- as the reference saves each scanline once it is done
+ * (StreakCameraFilm::average_and_save_slice, StreakCameraFilm.h:356-437).  type TR_FILM_F64
+ * delivers double sums; TR_FILM_F32 delivers float sums (rounded on the device; the
+ * reference's film itself accumulates in float), half the bytes.  streak/steady/weight point
+ * to arrays of that type (any may be NULL).  The copies overlap the rendering only when the
+ * host arrays are page-locked (cudaHostAlloc / cudaHostRegister); with pageable memory the call
+ * is still correct but serialises them.  Returns when the film is in host memory.            */
+enum { TR_FILM_F64 = 0, TR_FILM_F32 = 1 };
+tr_status tr_render_film(tr_ctx* ctx, uint64_t sample_begin, uint32_t sample_count, int type, void* streak,
+                         void* steady, void* weight);
+
 /* Same as tr_get_film but into device memory owned by the caller (no host copy).  Both copy on
  * the context's stream after its pending renders and return when the copy is complete; the
  * caller's own pending work on the destination must be finished first.                      */

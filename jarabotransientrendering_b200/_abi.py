@@ -66,6 +66,9 @@ class Stats(C.Structure):
                 ("guide_ms", C.c_double), ("train_steps", C.c_uint64), ("train_loss", C.c_float)]
 
 
+FILM_F64, FILM_F32 = 0, 1     # tr_render_film delivery types
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("shade_block", C.c_uint32), ("splat_div", C.c_uint32),
                 ("use_graph", C.c_uint32)]
@@ -84,6 +87,7 @@ PROTOTYPES = {
                                    C.c_uint32]),
     "tr_clear_film": (C.c_int, [C.c_void_p]),
     "tr_get_film": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tr_render_film": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_bounce": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_components": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

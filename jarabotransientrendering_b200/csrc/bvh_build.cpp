@@ -9,6 +9,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
+#include <memory>
 #include <string>
 
 namespace trh {
@@ -30,57 +32,159 @@ struct Box {
     }
 };
 
-struct Node { Box box; int32_t left = -1, right = -1; uint32_t first = 0, count = 0; };
+struct Node {                         // filled by Builder::build (no initialisers: the array is
+    Box box;                          // allocated for 2 nt nodes and only the used ones are written)
+    int32_t left, right;
+    uint32_t first, count;
+    uint32_t n_inner, n_tris;         // interior nodes and triangles in the subtree
+};
 
 constexpr int kBins = 32;
 
-// Subtrees larger than this are built on their own thread (up to the hardware's thread count).
+// Subtrees larger than this are built on their own thread (up to the hardware's thread count);
+// nodes larger than kParallelBinning bin their triangles on several threads.
 constexpr uint32_t kParallelCutoff = 16384;
+constexpr uint32_t kParallelBinning = 1u << 16;
+
+// Triangle bounds and centroid bounds of a range plus, per axis, the bins of the centroids
+// (bin boxes and counts).  Built by one pass over the range; partial results merge exactly
+// (min / max and counts), so the split chosen does not depend on how the range was divided.
+struct Binning {
+    Box nb, cb;
+    Box bb[3][kBins];
+    uint32_t bc[3][kBins];
+    void clear() {
+        nb.empty(); cb.empty();
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < kBins; ++b) { bb[a][b].empty(); bc[a][b] = 0; }
+    }
+    void merge(const Binning& o) {
+        nb.grow(o.nb); cb.grow(o.cb);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < kBins; ++b) { bb[a][b].grow(o.bb[a][b]); bc[a][b] += o.bc[a][b]; }
+    }
+};
+
+// a triangle as the builder moves it: bounds, centroid, id (partitioned in place, so every
+// pass over a node's range reads memory sequentially)
+struct Prim { Box b; float c[3]; uint32_t id; };
 
 struct Builder {
-    const Box* tb;
-    const float* cen;
-    std::vector<uint32_t> idx;
-    std::vector<Node> nodes;          // preallocated 2*nt; slots handed out by `next`
+    Prim* prim;
+    std::unique_ptr<Node[]> nodes;    // Builder::capacity(nt) slots handed out by `take`
     std::atomic<uint32_t> next{0};
     std::atomic<uint32_t> depth{0};
     std::atomic<int> threads{1};
     int max_threads = 1;
     uint32_t max_leaf;
 
-    int bin_of(float c, float lo, float scale) const {
+    static int bin_of(float c, float lo, float scale) {
         int b = (int)((c - lo) * scale);
         return b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
     }
 
-    uint32_t build(uint32_t first, uint32_t count, uint32_t d) {
-        uint32_t me = next.fetch_add(1, std::memory_order_relaxed);
-        Box nb, cb; nb.empty(); cb.empty();
+    // node and centroid bounds of [first, first + count)
+    void bounds(uint32_t first, uint32_t count, Box& nb, Box& cb) const {
+        nb.empty(); cb.empty();
         for (uint32_t i = first; i < first + count; ++i) {
-            uint32_t t = idx[i];
-            nb.grow(tb[t]);
-            cb.growp(&cen[3 * t]);
+            nb.grow(prim[i].b);
+            cb.growp(prim[i].c);
         }
-        nodes[me].box = nb;
+    }
+    // bins of [first, first + count) over the centroid box cb
+    void bin_range(uint32_t first, uint32_t count, const Box& cb, Binning& B) const {
+        float scale[3];
+        for (int a = 0; a < 3; ++a) {
+            const float ext = cb.hi[a] - cb.lo[a];
+            scale[a] = ext > 0.f ? (float)kBins / ext : 0.f;
+        }
+        for (uint32_t i = first; i < first + count; ++i) {
+            const Prim& q = prim[i];
+            for (int a = 0; a < 3; ++a) {
+                if (!(scale[a] > 0.f)) continue;
+                const int b = bin_of(q.c[a], cb.lo[a], scale[a]);
+                B.bb[a][b].grow(q.b);
+                B.bc[a][b]++;
+            }
+        }
+    }
+    // the same two passes split over `nt` threads
+    void bin_parallel(uint32_t first, uint32_t count, Binning& B, int nt) const {
+        std::vector<Binning> part((size_t)nt);
+        std::vector<std::thread> th;
+        const uint32_t chunk = (count + (uint32_t)nt - 1) / (uint32_t)nt;
+        auto run = [&](auto&& f) {
+            th.clear();
+            for (int k = 0; k < nt; ++k) {
+                const uint32_t a = first + (uint32_t)k * chunk;
+                const uint32_t n = a >= first + count ? 0u : std::min(chunk, first + count - a);
+                th.emplace_back([&, k, a, n] { f(k, a, n); });
+            }
+            for (auto& t : th) t.join();
+        };
+        run([&](int k, uint32_t a, uint32_t n) { part[k].clear(); bounds(a, n, part[k].nb, part[k].cb); });
+        B.clear();
+        for (int k = 0; k < nt; ++k) { B.nb.grow(part[k].nb); B.cb.grow(part[k].cb); }
+        const Box cb = B.cb;
+        run([&](int k, uint32_t a, uint32_t n) { bin_range(a, n, cb, part[k]); });
+        for (int k = 0; k < nt; ++k)
+            for (int ax = 0; ax < 3; ++ax)
+                for (int b = 0; b < kBins; ++b) { B.bb[ax][b].grow(part[k].bb[ax][b]); B.bc[ax][b] += part[k].bc[ax][b]; }
+    }
+
+    // Node slots are handed out in chunks of kChunk per thread, so threads write disjoint parts
+    // of the node array (no false sharing, one atomic per chunk).
+    static constexpr uint32_t kChunk = 1024;
+    struct Slots { uint32_t cur = 0, end = 0; };
+    uint32_t take(Slots& sl) {
+        if (sl.cur == sl.end) {
+            sl.cur = next.fetch_add(kChunk, std::memory_order_relaxed);
+            sl.end = sl.cur + kChunk;
+        }
+        return sl.cur++;
+    }
+    static size_t capacity(uint32_t nt) {
+        // 2 nt - 1 nodes, plus one partly used chunk per thread (at most one thread per node
+        // of more than kParallelCutoff triangles, and the first)
+        return 2 * (size_t)nt + (size_t)kChunk * (2 * (size_t)nt / kParallelCutoff + 3);
+    }
+
+    uint32_t build(uint32_t first, uint32_t count, uint32_t d) {
+        Slots sl;
+        return build(first, count, d, sl);
+    }
+    uint32_t build(uint32_t first, uint32_t count, uint32_t d, Slots& sl) {
+        const uint32_t me = take(sl);
+        Node& nd = nodes[me];
+        nd.left = nd.right = -1;
+        nd.first = 0; nd.count = 0;
         uint32_t dd = depth.load(std::memory_order_relaxed);
         while (d > dd && !depth.compare_exchange_weak(dd, d)) {}
-        if (count <= max_leaf) {
-            // SAH leaf test: keep as a leaf when small enough
-            nodes[me].first = first; nodes[me].count = count;
-            if (count <= 2) return me;
+        Binning B;
+        const bool wide = count >= kParallelBinning && max_threads > 1;
+        if (wide) {
+            bin_parallel(first, count, B, std::min(max_threads, 16));
+        } else {
+            B.clear();
+            bounds(first, count, B.nb, B.cb);
         }
+        const Box& nb = B.nb;
+        const Box& cb = B.cb;
+        nd.box = nb;
+        auto make_leaf = [&]() {
+            nd.first = first; nd.count = count;
+            nd.n_inner = 0; nd.n_tris = count;
+            return me;
+        };
+        // SAH leaf test: keep as a leaf when small enough
+        if (count <= max_leaf && count <= 2) return make_leaf();
+        if (!wide && count > 2) bin_range(first, count, cb, B);
         float best = 3.4e38f; int bax = -1, bsplit = -1;
         for (int ax = 0; ax < 3; ++ax) {
-            float ext = cb.hi[ax] - cb.lo[ax];
+            const float ext = cb.hi[ax] - cb.lo[ax];
             if (!(ext > 0.f)) continue;
-            float scale = (float)kBins / ext;
-            Box bb[kBins]; uint32_t bc[kBins];
-            for (int b = 0; b < kBins; ++b) { bb[b].empty(); bc[b] = 0; }
-            for (uint32_t i = first; i < first + count; ++i) {
-                uint32_t t = idx[i];
-                int b = bin_of(cen[3 * t + ax], cb.lo[ax], scale);
-                bb[b].grow(tb[t]); bc[b]++;
-            }
+            const Box* bb = B.bb[ax];
+            const uint32_t* bc = B.bc[ax];
             float ra[kBins]; uint32_t rc[kBins]; Box acc; acc.empty(); uint32_t n = 0;
             for (int b = kBins - 1; b > 0; --b) { acc.grow(bb[b]); n += bc[b]; ra[b] = acc.area(); rc[b] = n; }
             acc.empty(); n = 0;
@@ -94,33 +198,35 @@ struct Builder {
         if (count <= max_leaf) {
             // leaf if splitting does not pay (traversal cost ~ 1 triangle test)
             float leaf_cost = nb.area() * (float)count;
-            if (bax < 0 || best + nb.area() >= leaf_cost) return me;
+            if (bax < 0 || best + nb.area() >= leaf_cost) return make_leaf();
         }
         uint32_t mid;
         if (bax < 0) {
             mid = first + count / 2;
         } else {
             float scale = (float)kBins / (cb.hi[bax] - cb.lo[bax]);
-            auto it = std::partition(idx.begin() + first, idx.begin() + first + count, [&](uint32_t t) {
-                return bin_of(cen[3 * t + bax], cb.lo[bax], scale) <= bsplit;
+            Prim* it = std::partition(prim + first, prim + first + count, [&](const Prim& q) {
+                return bin_of(q.c[bax], cb.lo[bax], scale) <= bsplit;
             });
-            mid = (uint32_t)(it - idx.begin());
+            mid = (uint32_t)(it - prim);
             if (mid == first || mid == first + count) mid = first + count / 2;
         }
         int32_t l, r;
         if (count > kParallelCutoff && threads.fetch_add(1) < max_threads) {
             uint32_t rr = 0;
             std::thread t([&] { rr = build(mid, first + count - mid, d + 1); });
-            l = (int32_t)build(first, mid - first, d + 1);
+            l = (int32_t)build(first, mid - first, d + 1, sl);
             t.join();
             threads.fetch_sub(1);
             r = (int32_t)rr;
         } else {
             if (count > kParallelCutoff) threads.fetch_sub(1);
-            l = (int32_t)build(first, mid - first, d + 1);
-            r = (int32_t)build(mid, first + count - mid, d + 1);
+            l = (int32_t)build(first, mid - first, d + 1, sl);
+            r = (int32_t)build(mid, first + count - mid, d + 1, sl);
         }
-        nodes[me].left = l; nodes[me].right = r; nodes[me].count = 0;
+        nd.left = l; nd.right = r; nd.count = 0;
+        nd.n_inner = 1 + nodes[l].n_inner + nodes[r].n_inner;
+        nd.n_tris = nodes[l].n_tris + nodes[r].n_tris;
         return me;
     }
 };
@@ -131,51 +237,75 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
                BvhBuildResult& out, std::string* msg) {
     auto t0 = std::chrono::steady_clock::now();
     if (nt == 0) { if (msg) *msg = "scene has no triangles"; return false; }
+    if (nt >= (1u << 28)) { if (msg) *msg = "too many triangles"; return false; }
     if (max_leaf < 1 || max_leaf > 7) max_leaf = 4;
-    std::vector<Box> tb(nt);
-    std::vector<float> cen(3 * (size_t)nt);
-    for (uint32_t t = 0; t < nt; ++t) {
-        tb[t].empty();
-        for (int j = 0; j < 3; ++j) {
-            uint32_t vi = tri[3 * (size_t)t + j];
-            if (vi >= nv) { if (msg) *msg = "triangle " + std::to_string(t) + " references vertex " + std::to_string(vi) + " out of range"; return false; }
-            const float* p = &v[3 * (size_t)vi];
-            if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) {
-                if (msg) *msg = "vertex " + std::to_string(vi) + " is not finite";
-                return false;
-            }
-            tb[t].growp(p);
+    const int hw = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    // run f(begin, end) over [0, n) on up to hw threads
+    auto parallel_for = [&](uint32_t n, auto&& f) {
+        const int k = (int)std::min<uint32_t>((uint32_t)hw, std::max(1u, n / 8192u));
+        if (k <= 1) { f(0u, n); return; }
+        std::vector<std::thread> th;
+        const uint32_t chunk = (n + (uint32_t)k - 1) / (uint32_t)k;
+        for (int i = 0; i < k; ++i) {
+            const uint32_t a = (uint32_t)i * chunk, b = std::min(n, a + chunk);
+            if (a < b) th.emplace_back([&f, a, b] { f(a, b); });
         }
-        for (int k = 0; k < 3; ++k) cen[3 * (size_t)t + k] = 0.5f * (tb[t].lo[k] + tb[t].hi[k]);
+        for (auto& t : th) t.join();
+    };
+
+    std::unique_ptr<Prim[]> prim(new Prim[nt]);
+    std::atomic<int64_t> bad{-1};                // first bad vertex index seen (-1: none)
+    std::atomic<int64_t> bad_tri{-1};
+    parallel_for(nt, [&](uint32_t a, uint32_t b) {
+        for (uint32_t t = a; t < b; ++t) {
+            Prim& q = prim[t];
+            q.b.empty();
+            q.id = t;
+            for (int j = 0; j < 3; ++j) {
+                const uint32_t vi = tri[3 * (size_t)t + j];
+                if (vi >= nv) { bad_tri.store(t); return; }
+                const float* p = &v[3 * (size_t)vi];
+                if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) { bad.store(vi); return; }
+                q.b.growp(p);
+            }
+            for (int k = 0; k < 3; ++k) q.c[k] = 0.5f * (q.b.lo[k] + q.b.hi[k]);
+        }
+    });
+    if (bad_tri.load() >= 0) {
+        // report the first offending triangle of the input (sequential scan)
+        for (uint32_t t = 0; t < nt; ++t)
+            for (int j = 0; j < 3; ++j)
+                if (tri[3 * (size_t)t + j] >= nv) {
+                    if (msg) *msg = "triangle " + std::to_string(t) + " references vertex " +
+                                    std::to_string(tri[3 * (size_t)t + j]) + " out of range";
+                    return false;
+                }
+    }
+    if (bad.load() >= 0) {
+        for (uint32_t t = 0; t < nt; ++t)
+            for (int j = 0; j < 3; ++j) {
+                const uint32_t vi = tri[3 * (size_t)t + j];
+                const float* p = &v[3 * (size_t)vi];
+                if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) {
+                    if (msg) *msg = "vertex " + std::to_string(vi) + " is not finite";
+                    return false;
+                }
+            }
     }
     Builder B;
-    B.tb = tb.data(); B.cen = cen.data(); B.max_leaf = max_leaf;
-    B.idx.resize(nt);
-    for (uint32_t t = 0; t < nt; ++t) B.idx[t] = t;
-    B.nodes.resize(2 * (size_t)nt);
-    B.max_threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    B.prim = prim.get(); B.max_leaf = max_leaf;
+    B.nodes.reset(new Node[Builder::capacity(nt)]);
+    B.max_threads = hw;
     B.build(0, nt, 0);
-    B.nodes.resize(B.next.load());
 
-    // Flatten: one GpuNode per interior node, depth-first, left child adjacent to its parent.
-    out.nodes.clear(); out.tris.clear(); out.leaves = 0;
-    out.tris.reserve(nt);
-    std::vector<int32_t> gpu_index(B.nodes.size(), -1);
-    auto leaf_ref = [&](const Node& n) -> int32_t {
-        uint32_t first = (uint32_t)out.tris.size();
-        for (uint32_t i = n.first; i < n.first + n.count; ++i) {
-            uint32_t t = B.idx[i];
-            GpuTri g;
-            const uint32_t* ti = &tri[3 * (size_t)t];
-            std::memcpy(g.v0, &v[3 * (size_t)ti[0]], 12);
-            std::memcpy(g.v1, &v[3 * (size_t)ti[1]], 12);
-            std::memcpy(g.v2, &v[3 * (size_t)ti[2]], 12);
-            g.id = t; g.pad1 = 0.f; g.pad2 = 0.f;
-            out.tris.push_back(g);
-        }
-        out.leaves++;
-        return ~(int32_t)((first << 3) | n.count);
-    };
+    // Flatten: one GpuNode per interior node in depth-first preorder (left child adjacent to
+    // its parent), leaf triangles in the same order.  Every subtree's interior-node and
+    // triangle counts are known, so each subtree is written at its own offsets, large ones on
+    // their own threads.
+    const Node& root = B.nodes[0];
+    out.nodes.assign(std::max<uint32_t>(1u, root.n_inner), GpuNode{});
+    out.tris.resize(nt);
+    std::atomic<uint32_t> leaves{0};
     auto write_box = [](GpuNode& g, int slot, const Box& bin) {
         // one ulp outward: a ray lying exactly in a face plane of a box (zero direction
         // component, origin on the face) still sees a non-empty slab interval
@@ -194,46 +324,57 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
             g.c[2] = b.lo[2]; g.c[3] = b.hi[2];
         }
     };
-    Box emptybox; emptybox.empty();
-    if (nt >= (1u << 28)) { if (msg) *msg = "too many triangles"; return false; }
-    const Node& root = B.nodes[0];
+    auto leaf_ref = [&](const Node& n, uint32_t toff) -> int32_t {
+        for (uint32_t i = 0; i < n.count; ++i) {
+            const uint32_t t = prim[n.first + i].id;
+            GpuTri& g = out.tris[toff + i];
+            const uint32_t* ti = &tri[3 * (size_t)t];
+            std::memcpy(g.v0, &v[3 * (size_t)ti[0]], 12);
+            std::memcpy(g.v1, &v[3 * (size_t)ti[1]], 12);
+            std::memcpy(g.v2, &v[3 * (size_t)ti[2]], 12);
+            g.id = t; g.pad1 = 0.f; g.pad2 = 0.f;
+        }
+        leaves.fetch_add(1, std::memory_order_relaxed);
+        return ~(int32_t)((toff << 3) | n.count);
+    };
+    std::atomic<int> fthreads{1};
+    // interior node ni at GPU index gi, its leaf triangles from toff
+    std::function<void(uint32_t, uint32_t, uint32_t)> flat = [&](uint32_t ni, uint32_t gi, uint32_t toff) {
+        const Node& n = B.nodes[ni];
+        const Node& L = B.nodes[n.left];
+        const Node& R = B.nodes[n.right];
+        GpuNode& g = out.nodes[gi];
+        write_box(g, 0, L.box);
+        write_box(g, 1, R.box);
+        const uint32_t gl = gi + 1, gr = gi + 1 + L.n_inner;
+        const uint32_t tl = toff, tr = toff + L.n_tris;
+        g.d[0] = L.left < 0 ? leaf_ref(L, tl) : (int32_t)gl;
+        g.d[1] = R.left < 0 ? leaf_ref(R, tr) : (int32_t)gr;
+        g.d[2] = 0; g.d[3] = 0;
+        const bool lin = L.left >= 0, rin = R.left >= 0;
+        if (lin && rin && L.n_tris > kParallelCutoff && fthreads.fetch_add(1) < hw) {
+            std::thread t([&, gl, tl] { flat((uint32_t)n.left, gl, tl); });
+            flat((uint32_t)n.right, gr, tr);
+            t.join();
+            fthreads.fetch_sub(1);
+        } else {
+            if (lin && rin && L.n_tris > kParallelCutoff) fthreads.fetch_sub(1);
+            if (lin) flat((uint32_t)n.left, gl, tl);
+            if (rin) flat((uint32_t)n.right, gr, tr);
+        }
+    };
     if (root.left < 0) {
         // single-leaf scene: a root whose second child is empty
-        GpuNode g{};
-        out.nodes.push_back(g);
+        Box emptybox; emptybox.empty();
         write_box(out.nodes[0], 0, root.box);
         write_box(out.nodes[0], 1, emptybox);
-        out.nodes[0].d[0] = leaf_ref(root);
+        out.nodes[0].d[0] = leaf_ref(root, 0);
         out.nodes[0].d[1] = ~(int32_t)0;   // empty leaf (count 0)
+        out.nodes[0].d[2] = 0; out.nodes[0].d[3] = 0;
     } else {
-        std::vector<uint32_t> stack;
-        stack.push_back(0);
-        gpu_index[0] = 0;
-        out.nodes.emplace_back();
-        while (!stack.empty()) {
-            uint32_t ni = stack.back(); stack.pop_back();
-            const Node& n = B.nodes[ni];
-            int32_t gi = gpu_index[ni];
-            int32_t child[2] = {n.left, n.right};
-            int32_t refs[2];
-            for (int s = 0; s < 2; ++s) {
-                const Node& c = B.nodes[child[s]];
-                write_box(out.nodes[gi], s, c.box);
-                if (c.left < 0) {
-                    refs[s] = leaf_ref(c);
-                } else {
-                    gpu_index[child[s]] = (int32_t)out.nodes.size();
-                    out.nodes.emplace_back();
-                    refs[s] = gpu_index[child[s]];
-                }
-            }
-            out.nodes[gi].d[0] = refs[0]; out.nodes[gi].d[1] = refs[1];
-            out.nodes[gi].d[2] = 0; out.nodes[gi].d[3] = 0;
-            // push right first so the left subtree is laid out next
-            for (int s = 1; s >= 0; --s)
-                if (B.nodes[child[s]].left >= 0) stack.push_back((uint32_t)child[s]);
-        }
+        flat(0, 0, 0);
     }
+    out.leaves = leaves.load();
     out.depth = B.depth.load();
     out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return true;

@@ -237,8 +237,12 @@ namespace {
 
 tr_status guide_after_render(tr_ctx* x, cudaStream_t s);
 
+// Host buffers the film is streamed into while rendering (tr_render_film): FP64 or FP32 sums
+// of the whole frame.
+struct FilmSink { int type; void* streak; void* steady; void* weight; };
+
 tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
-                        uint64_t s0, uint32_t ns_total) {
+                        uint64_t s0, uint32_t ns_total, const FilmSink* sink = nullptr) {
     if (x1 > x->film.width || y1 > x->film.height || x0 >= x1 || y0 >= y1)
         return fail(TR_ERR_INVALID_ARGUMENT, "pixel window out of range or empty");
     if (ns_total == 0) return TR_OK;
@@ -285,6 +289,21 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         marks.push_back({kind, a});
     };
     uint64_t launches = 0, ext_l = 0, sh_l = 0;
+    // film streaming: once a pixel batch of the last sample chunk is splatted its film rows are
+    // final; the copy stream waits for that point and copies them (FP32: converted on the
+    // device first, into a staging buffer the copy stream reuses in order)
+    const uint32_t T = x->film.time_bins;
+    const bool f32 = sink && sink->type == TR_FILM_F32;
+    if (sink) {
+        if (!x->copy_stream) TR_CUDA(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
+        const uint32_t per_pix_max = std::min<uint32_t>(ns_total, std::max<uint32_t>(1u, cap / ninc)) * ninc;
+        const size_t ppb_max = std::max<uint32_t>(1u, cap / per_pix_max);
+        const size_t stage = ppb_max * ((size_t)T * 3u + 4u);
+        if (f32 && x->stage_floats < stage) {
+            x->d_stage = x->alloc<float>(stage);
+            x->stage_floats = stage;
+        }
+    }
     TR_CUDA(cudaEventRecord(x->ev0, strm));
     for (uint64_t sb = 0; sb < ns_total; sb += ns_chunk) {
         const uint32_t ns = (uint32_t)std::min<uint64_t>(ns_chunk, ns_total - sb);
@@ -342,8 +361,47 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             launches += 2 + 3ull * x->integ.max_bounces;
             ext_l += x->integ.max_bounces;
             sh_l += x->integ.max_bounces;
+            if (sink && sb + ns >= ns_total) {
+                // window = whole frame: the batch's pixels are contiguous film rows
+                cudaEvent_t done = ev_get();
+                TR_CUDA(cudaEventRecord(done, strm));
+                TR_CUDA(cudaStreamWaitEvent(x->copy_stream, done, 0));
+                const size_t p0 = pb, np = npix;
+                const size_t es = f32 ? sizeof(float) : sizeof(double);
+                const size_t n_st = np * T * 3u, n_sd = np * 3u;
+                if (f32) {
+                    float* st = x->d_stage;
+                    float* sd = st + n_st;
+                    float* wt = sd + n_sd;
+                    TR_CUDA(trk::launch_to_f32(x->d_streak + p0 * T * 3u, st, n_st, x->copy_stream));
+                    TR_CUDA(trk::launch_to_f32(x->d_steady + p0 * 3u, sd, n_sd, x->copy_stream));
+                    TR_CUDA(trk::launch_to_f32(x->d_weight + p0, wt, np, x->copy_stream));
+                    launches += 3;
+                    if (sink->streak)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->streak) + p0 * T * 3u * es, st, n_st * es,
+                                                cudaMemcpyDeviceToHost, x->copy_stream));
+                    if (sink->steady)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->steady) + p0 * 3u * es, sd, n_sd * es,
+                                                cudaMemcpyDeviceToHost, x->copy_stream));
+                    if (sink->weight)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->weight) + p0 * es, wt, np * es,
+                                                cudaMemcpyDeviceToHost, x->copy_stream));
+                } else {
+                    if (sink->streak)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->streak) + p0 * T * 3u * es,
+                                                x->d_streak + p0 * T * 3u, n_st * es, cudaMemcpyDeviceToHost,
+                                                x->copy_stream));
+                    if (sink->steady)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->steady) + p0 * 3u * es, x->d_steady + p0 * 3u,
+                                                n_sd * es, cudaMemcpyDeviceToHost, x->copy_stream));
+                    if (sink->weight)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->weight) + p0 * es, x->d_weight + p0,
+                                                np * es, cudaMemcpyDeviceToHost, x->copy_stream));
+                }
+            }
         }
     }
+    if (sink) TR_CUDA(cudaStreamSynchronize(x->copy_stream));
     TR_CUDA(cudaEventRecord(x->ev1, strm));
     TR_CUDA(cudaEventSynchronize(x->ev1));
     float ms = 0.f;
@@ -582,6 +640,26 @@ tr_status tr_render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uin
 tr_status tr_render(tr_ctx* x, uint64_t sample_begin, uint32_t sample_count) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
     return tr_render_region(x, 0, 0, x->film.width, x->film.height, sample_begin, sample_count);
+}
+
+static tr_status copy_film(tr_ctx* x, double* streak, double* steady, double* weight, cudaMemcpyKind kind);
+
+tr_status tr_render_film(tr_ctx* x, uint64_t sample_begin, uint32_t sample_count, int type, void* streak,
+                         void* steady, void* weight) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    if (type != TR_FILM_F64 && type != TR_FILM_F32) return fail(TR_ERR_INVALID_ARGUMENT, "unknown film type");
+    if (sample_count == 0) {
+        // nothing to render: deliver the current sums
+        if (type == TR_FILM_F64) return copy_film(x, (double*)streak, (double*)steady, (double*)weight, cudaMemcpyDeviceToHost);
+        return fail(TR_ERR_INVALID_ARGUMENT, "sample_count must be >= 1 for FP32 delivery");
+    }
+    try {
+        TR_CUDA(cudaSetDevice(x->device));
+        FilmSink sink{type, streak, steady, weight};
+        return render_region(x, 0, 0, x->film.width, x->film.height, sample_begin, sample_count, &sink);
+    } catch (const CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
+    }
 }
 
 tr_status tr_clear_film(tr_ctx* x) {

@@ -133,6 +133,10 @@ struct tr_ctx {
     trk::BidirWave bd{};
     uint32_t* d_lcounters = nullptr;
     int connect_grid = 0;
+    // film streaming (tr_render_film)
+    cudaStream_t copy_stream = nullptr;
+    float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows
+    size_t stage_floats = 0;
     int trace_grid = 0;
     int splat_g = 1;
 
@@ -170,6 +174,8 @@ struct tr_ctx {
         allocs.clear();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        copy_stream = nullptr;
         if (stream) cudaStreamDestroy(stream);
         ev0 = ev1 = nullptr;
         stream = nullptr;

@@ -1326,6 +1326,22 @@ cudaError_t launch_connect(const Params& p, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// FP64 film sums to FP32 (round to nearest); grid-stride, streaming loads
+__global__ void __launch_bounds__(256) k_to_f32(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (float)__ldcs(&src[i]);
+}
+cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t need = (n + 255) / 256;
+    const int grid = (int)std::min<size_t>(need, (size_t)sms * 8);
+    k_to_f32<<<std::max(1, grid), 256, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
 // last node of a multi-scene batch: the next replay renders the next batch descriptor
 __global__ void k_advance(uint32_t* cur) { *cur += 1u; }
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s) {

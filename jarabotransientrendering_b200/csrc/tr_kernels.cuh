@@ -222,6 +222,8 @@ cudaError_t launch_light_raygen(const Params& pl, cudaStream_t s);
 cudaError_t launch_light_shade(const Params& pl, int depth, cudaStream_t s);
 cudaError_t launch_connect(const Params& p, int grid, cudaStream_t s);
 int connect_grid_size(int device, uint32_t bvh_depth);      // resident k_connect blocks
+// FP64 film sums -> FP32 (film streaming)
+cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);

@@ -133,6 +133,25 @@ class Context:
                                           steady.ctypes.data if steady is not None else None,
                                           weight.ctypes.data if weight is not None else None))
 
+    def render_film(self, sample_begin, sample_count, streak=None, steady=None, weight=None):
+        """tr_render_film: render and stream the film's sums into caller-provided host arrays
+        (float64 or float32, all of one type; pinned arrays let the copies overlap the
+        rendering).  Returns nothing; the arrays hold the film when it returns."""
+        arrs = [a for a in (streak, steady, weight) if a is not None]
+        dt = arrs[0].dtype if arrs else np.dtype(np.float64)
+        if any(a.dtype != dt for a in arrs) or dt not in (np.float64, np.float32):
+            raise ValueError("film arrays must all be float64 or all float32")
+        sc = self.scene
+        H, W, T = sc.height, sc.width, sc.time_bins
+        for a, shape in ((streak, (H, W, T, 3)), (steady, (H, W, 3)), (weight, (H, W))):
+            if a is not None and (a.shape != shape or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError(f"film array must be C-contiguous with shape {shape}")
+        kind = _abi.FILM_F32 if dt == np.float32 else _abi.FILM_F64
+        _abi.check(_abi.lib().tr_render_film(self.h, int(sample_begin), int(sample_count), kind,
+                                             streak.ctypes.data if streak is not None else None,
+                                             steady.ctypes.data if steady is not None else None,
+                                             weight.ctypes.data if weight is not None else None))
+
     def write(self, name: str):
         _abi.check(_abi.lib().tr_write_film(self.h, name.encode()))
 

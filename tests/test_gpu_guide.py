@@ -33,6 +33,13 @@ def _bits(x):
     return torch.from_numpy(G.to_bf16_bits(x).view(np.int16)).cuda()
 
 
+def _ready():
+    """Inputs and outputs are made on torch's stream; the guide's entry points called with a
+    NULL stream run on the guide's own stream, which is not ordered after torch's work."""
+    import torch
+    torch.cuda.synchronize()
+
+
 @pytest.mark.parametrize("n", [1, 127, 128, 1000, 65536])
 def test_forward_matches_oracle(gpu, n):
     import torch
@@ -44,6 +51,7 @@ def test_forward_matches_oracle(gpu, n):
         _abi.check(_abi.lib().tr_guide_set_params(g, params.ctypes.data))
         xd = _bits(x)
         out = torch.zeros((n, 40), dtype=torch.float32, device="cuda")
+        _ready()
         _abi.check(_abi.lib().tr_guide_forward(g, C.c_void_p(xd.data_ptr()), n, C.c_void_p(out.data_ptr()), None))
         got = out.cpu().numpy()
     finally:
@@ -71,6 +79,7 @@ def test_gradients_match_oracle(gpu):
         dd = _dev(dirs.astype(np.float32), torch.float32)
         wd = _dev(w, torch.float32)
         loss = C.c_float()
+        _ready()
         _abi.check(_abi.lib().tr_guide_train_step(g, C.c_void_p(xd.data_ptr()), C.c_void_p(dd.data_ptr()),
                                                   C.c_void_p(wd.data_ptr()), n, 0.0, C.byref(loss), None))
         grads = np.zeros(G.NP, np.float32)
@@ -109,6 +118,7 @@ def test_training_fits_a_feature_dependent_distribution(gpu):
             w = np.ones(n, np.float32)
             xd, dd, wd = _bits(x), _dev(dirs.astype(np.float32), torch.float32), _dev(w, torch.float32)
             loss = C.c_float()
+            _ready()
             _abi.check(_abi.lib().tr_guide_train_step(g, C.c_void_p(xd.data_ptr()), C.c_void_p(dd.data_ptr()),
                                                       C.c_void_p(wd.data_ptr()), n, 1e-3, C.byref(loss), None))
             losses.append(loss.value)
