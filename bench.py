@@ -448,7 +448,7 @@ def main():
                 times.append(t3 - t0)
                 phases.append({"create_ms": (t1 - t0) * 1e3, "bvh_build_ms": bvh_ms,
                                "render_and_film_d2h_ms": (t2 - t1) * 1e3, "destroy_ms": (t3 - t2) * 1e3})
-            return sum(times[1:]) / steps, phases[-1]
+            return sum(times[1:]) / steps, phases[1:]
 
         e2e_steps = max(1, min(args.steps, 3))
         f32 = host_film(torch.float32)
@@ -464,7 +464,7 @@ def main():
                       "d2h_bytes_per_step": int(d2h),
                       "ms_per_step": et * 1e3,
                       "film": "FP32 sums (the reference's film precision)",
-                      "phases_last_step": ph,
+                      "phases_per_step": ph,
                       "fp64_film": {"value": paths_per_step * world / et64, "d2h_bytes_per_step": int(d2h64),
                                     "ms_per_step": et64 * 1e3, "phases": ph64},
                       "includes": "tr_create (scene H2D from pinned memory + host BVH build + film alloc), "

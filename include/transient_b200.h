@@ -217,6 +217,12 @@ typedef struct tr_ctx tr_ctx;
 tr_status tr_create(const tr_scene* scene, const tr_camera* camera, const tr_film* film,
                     const tr_integrator* integrator, int device, tr_ctx** out);
 
+/* Device memory that destroyed contexts, guides and batches freed is kept by the library (one
+ * memory pool per device) and reused by later ones, so creating and destroying contexts in a
+ * loop does not map and unmap the film each time.  This returns the kept memory of `device`
+ * to the driver (after waiting for the device); no counterpart in the reference.            */
+tr_status tr_release_cached_memory(int device);
+
 /* Renders camera samples [sample_begin, sample_begin + sample_count) of every pixel and adds
  * them to the film (the while-loop of TransientRenderer::render).  Additive: calling it for
  * [0,a) then [a,b) equals one call for [0,b).  Camera sample s uses stratum s mod sqrt_spp^2. */

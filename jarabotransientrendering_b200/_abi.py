@@ -87,6 +87,7 @@ PROTOTYPES = {
                                    C.c_uint32]),
     "tr_clear_film": (C.c_int, [C.c_void_p]),
     "tr_get_film": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tr_release_cached_memory": (C.c_int, [C.c_int]),
     "tr_render_film": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tr_get_film_bounce": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -45,6 +45,9 @@ constexpr int kBins = 32;
 // nodes larger than kParallelBinning bin their triangles on several threads.
 constexpr uint32_t kParallelCutoff = 16384;
 constexpr uint32_t kParallelBinning = 1u << 16;
+// nodes of at most kSmall triangles evaluate the SAH candidates without bins
+constexpr uint32_t kSmall = 16;
+static_assert(kBins <= 32, "occupied-bin masks are 32 bits");
 
 // Triangle bounds and centroid bounds of a range plus, per axis, the bins of the centroids
 // (bin boxes and counts).  Built by one pass over the range; partial results merge exactly
@@ -149,11 +152,31 @@ struct Builder {
         return 2 * (size_t)nt + (size_t)kChunk * (2 * (size_t)nt / kParallelCutoff + 3);
     }
 
+    // Splits [first, first + count) so the triangles whose centroid bin on `ax` is <= split
+    // come first; returns the boundary and the triangle and centroid bounds of both sides.
+    uint32_t partition(uint32_t first, uint32_t count, int ax, float lo, float scale, int split, Box bx[2],
+                       Box cx[2]) const {
+        bx[0].empty(); bx[1].empty(); cx[0].empty(); cx[1].empty();
+        uint32_t i = first, j = first + count;
+        while (true) {
+            while (i < j && bin_of(prim[i].c[ax], lo, scale) <= split) {
+                bx[0].grow(prim[i].b); cx[0].growp(prim[i].c); ++i;
+            }
+            while (i < j && bin_of(prim[j - 1].c[ax], lo, scale) > split) {
+                --j; bx[1].grow(prim[j].b); cx[1].growp(prim[j].c);
+            }
+            if (i >= j) break;
+            std::swap(prim[i], prim[j - 1]);
+        }
+        return i;
+    }
+
     uint32_t build(uint32_t first, uint32_t count, uint32_t d) {
         Slots sl;
-        return build(first, count, d, sl);
+        return build(first, count, d, sl, nullptr, nullptr);
     }
-    uint32_t build(uint32_t first, uint32_t count, uint32_t d, Slots& sl) {
+    // nb0 / cb0: the range's triangle and centroid bounds when the parent already has them
+    uint32_t build(uint32_t first, uint32_t count, uint32_t d, Slots& sl, const Box* nb0, const Box* cb0) {
         const uint32_t me = take(sl);
         Node& nd = nodes[me];
         nd.left = nd.right = -1;
@@ -166,7 +189,8 @@ struct Builder {
             bin_parallel(first, count, B, std::min(max_threads, 16));
         } else {
             B.clear();
-            bounds(first, count, B.nb, B.cb);
+            if (nb0) { B.nb = *nb0; B.cb = *cb0; }
+            else bounds(first, count, B.nb, B.cb);
         }
         const Box& nb = B.nb;
         const Box& cb = B.cb;
@@ -178,8 +202,36 @@ struct Builder {
         };
         // SAH leaf test: keep as a leaf when small enough
         if (count <= max_leaf && count <= 2) return make_leaf();
-        if (!wide && count > 2) bin_range(first, count, cb, B);
         float best = 3.4e38f; int bax = -1, bsplit = -1;
+        if (count <= kSmall) {
+            // the same candidates as the binned sweep below, evaluated directly: a split after
+            // each occupied bin but the last (splits between two occupied bins all give that
+            // cost, and the sweep keeps the first), axes and bins in the same order
+            for (int ax = 0; ax < 3; ++ax) {
+                const float ext = cb.hi[ax] - cb.lo[ax];
+                if (!(ext > 0.f)) continue;
+                const float scale = (float)kBins / ext;
+                int bins[kSmall];
+                uint32_t occupied = 0;                    // bit mask of occupied bins
+                for (uint32_t i = 0; i < count; ++i) {
+                    bins[i] = bin_of(prim[first + i].c[ax], cb.lo[ax], scale);
+                    occupied |= 1u << bins[i];
+                }
+                const int top = 31 - __builtin_clz(occupied);
+                for (uint32_t m = occupied & ~(1u << top); m; m &= m - 1) {
+                    const int v = __builtin_ctz(m);
+                    Box lbox, rbox; lbox.empty(); rbox.empty();
+                    uint32_t nl = 0, nr = 0;
+                    for (uint32_t i = 0; i < count; ++i) {
+                        if (bins[i] <= v) { lbox.grow(prim[first + i].b); ++nl; }
+                        else { rbox.grow(prim[first + i].b); ++nr; }
+                    }
+                    const float cost = lbox.area() * (float)nl + rbox.area() * (float)nr;
+                    if (cost < best) { best = cost; bax = ax; bsplit = v; }
+                }
+            }
+        } else {
+        if (!wide) bin_range(first, count, cb, B);
         for (int ax = 0; ax < 3; ++ax) {
             const float ext = cb.hi[ax] - cb.lo[ax];
             if (!(ext > 0.f)) continue;
@@ -195,34 +247,42 @@ struct Builder {
                 if (cost < best) { best = cost; bax = ax; bsplit = b; }
             }
         }
+        }
         if (count <= max_leaf) {
             // leaf if splitting does not pay (traversal cost ~ 1 triangle test)
             float leaf_cost = nb.area() * (float)count;
             if (bax < 0 || best + nb.area() >= leaf_cost) return make_leaf();
         }
         uint32_t mid;
+        Box bx[2], cx[2];
+        bool known = false;                 // children's bounds come from the partition
         if (bax < 0) {
             mid = first + count / 2;
         } else {
             float scale = (float)kBins / (cb.hi[bax] - cb.lo[bax]);
-            Prim* it = std::partition(prim + first, prim + first + count, [&](const Prim& q) {
-                return bin_of(q.c[bax], cb.lo[bax], scale) <= bsplit;
-            });
-            mid = (uint32_t)(it - prim);
-            if (mid == first || mid == first + count) mid = first + count / 2;
+            mid = partition(first, count, bax, cb.lo[bax], scale, bsplit, bx, cx);
+            known = true;
+            if (mid == first || mid == first + count) { mid = first + count / 2; known = false; }
         }
+        const Box* lb = known ? &bx[0] : nullptr;
+        const Box* lc = known ? &cx[0] : nullptr;
+        const Box* rb = known ? &bx[1] : nullptr;
+        const Box* rc2 = known ? &cx[1] : nullptr;
         int32_t l, r;
         if (count > kParallelCutoff && threads.fetch_add(1) < max_threads) {
             uint32_t rr = 0;
-            std::thread t([&] { rr = build(mid, first + count - mid, d + 1); });
-            l = (int32_t)build(first, mid - first, d + 1, sl);
+            std::thread t([&] {
+                Slots ts;
+                rr = build(mid, first + count - mid, d + 1, ts, rb, rc2);
+            });
+            l = (int32_t)build(first, mid - first, d + 1, sl, lb, lc);
             t.join();
             threads.fetch_sub(1);
             r = (int32_t)rr;
         } else {
             if (count > kParallelCutoff) threads.fetch_sub(1);
-            l = (int32_t)build(first, mid - first, d + 1, sl);
-            r = (int32_t)build(mid, first + count - mid, d + 1, sl);
+            l = (int32_t)build(first, mid - first, d + 1, sl, lb, lc);
+            r = (int32_t)build(mid, first + count - mid, d + 1, sl, rb, rc2);
         }
         nd.left = l; nd.right = r; nd.count = 0;
         nd.n_inner = 1 + nodes[l].n_inner + nodes[r].n_inner;

@@ -116,6 +116,34 @@ void upload(void* dst, const void* src, size_t bytes) {
 
 namespace tri {
 
+cudaMemPool_t device_pool(int device) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0) throw CudaError(cudaErrorInvalidDevice, "device_pool");
+    if ((size_t)device >= pools.size()) pools.resize((size_t)device + 1, nullptr);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        TR_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = ~0ull;
+        TR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
+size_t pool_idle_bytes(int device) {
+    uint64_t reserved = 0, used = 0;
+    cudaMemPool_t pool = device_pool(device);
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess) return 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) return 0;
+    return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
 void ensure_wave(tr_ctx* x, uint32_t capacity) {
     if (x->wave.capacity >= capacity) return;
     // grow: drop the old buffers (they are only scratch between calls)
@@ -461,9 +489,14 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(TR_ERR_NO_DEVICE, "no CUDA device");
     if (device < 0 || device >= ndev) return fail(TR_ERR_NO_DEVICE, "device index out of range");
-    cudaDeviceProp prop{};
-    cudaGetDeviceProperties(&prop, device);
-    if (prop.major != 10) return fail(TR_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+    // one attribute query (cudaGetDeviceProperties reads every property and costs milliseconds)
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (major != 10) {
+        cudaDeviceProp prop{};
+        cudaGetDeviceProperties(&prop, device);
+        return fail(TR_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+    }
     tr_ctx* x = new (std::nothrow) tr_ctx();
     if (!x) return fail(TR_ERR_OUT_OF_MEMORY, "host allocation failed");
     try {
@@ -571,6 +604,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         const size_t nstreak = (size_t)f->width * f->height * f->time_bins * 3u;
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
+        free_b += tri::pool_idle_bytes(device);      // kept by the pool for reuse
         const size_t nb = f->bounce_films;
         if ((1 + nb) * nstreak * sizeof(double) + ((size_t)2 << 30) > free_b) {
             x->release();
@@ -635,6 +669,20 @@ tr_status tr_render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uin
     } catch (const CudaError& e) {
         return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
     }
+}
+
+tr_status tr_release_cached_memory(int device) {
+    try {
+        int n = 0;
+        TR_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) return fail(TR_ERR_INVALID_ARGUMENT, "no such device");
+        TR_CUDA(cudaSetDevice(device));
+        TR_CUDA(cudaDeviceSynchronize());
+        TR_CUDA(cudaMemPoolTrimTo(tri::device_pool(device), 0));
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
 }
 
 tr_status tr_render(tr_ctx* x, uint64_t sample_begin, uint32_t sample_count) {
@@ -989,9 +1037,14 @@ extern "C" tr_status tr_guide_create(int device, uint64_t seed, tr_guide** out) 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(TR_ERR_NO_DEVICE, "no CUDA device");
     if (device < 0 || device >= ndev) return fail(TR_ERR_NO_DEVICE, "device index out of range");
-    cudaDeviceProp prop{};
-    cudaGetDeviceProperties(&prop, device);
-    if (prop.major != 10) return fail(TR_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+    // one attribute query (cudaGetDeviceProperties reads every property and costs milliseconds)
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (major != 10) {
+        cudaDeviceProp prop{};
+        cudaGetDeviceProperties(&prop, device);
+        return fail(TR_ERR_NO_DEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+    }
     tr_guide* g = new (std::nothrow) tr_guide();
     if (!g) return fail(TR_ERR_OUT_OF_MEMORY, "host allocation failed");
     try {

@@ -29,12 +29,24 @@ struct CudaError : std::runtime_error {
         if (e_ != cudaSuccess) throw CudaError(e_, #call);      \
     } while (0)
 
+// Device memory of contexts, guides and batches comes from one stream-ordered pool per device
+// that keeps freed memory for the next allocations (release threshold unlimited), so creating
+// and destroying contexts does not map and unmap gigabytes each time; memory goes back to the
+// driver only through tr_release_cached_memory or at exit.  Frees stay cudaFree (which waits
+// for the device and returns the block to its pool).
+cudaMemPool_t device_pool(int device);
+// pool memory of `device` reserved but not in use (free for the next allocations)
+size_t pool_idle_bytes(int device);
+
 template <class T>
 T* dalloc(size_t count, size_t& total) {
     if (count == 0) count = 1;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e != cudaSuccess) throw CudaError(e, "cudaMalloc");
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&p, count * sizeof(T), device_pool(dev), 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);     // usable from every stream
+    if (e != cudaSuccess) throw CudaError(e, "device allocation");
     total += count * sizeof(T);
     return static_cast<T*>(p);
 }

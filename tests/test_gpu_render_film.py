@@ -93,3 +93,27 @@ def test_render_film_rejects_mixed_or_bad_arrays(gpu):
             c.render_film(0, 1, np.empty((8, 8, 15, 3)))
         from jarabotransientrendering_b200 import _abi
         assert _abi.lib().tr_render_film(c.h, 0, 1, 7, None, None, None) == 1
+
+
+def test_device_memory_is_kept_for_reuse_and_released_on_request(gpu):
+    """Destroyed contexts leave their device memory in the library's pool (a second context
+    of the same size takes it without the free device memory dropping again);
+    tr_release_cached_memory hands it back to the driver."""
+    import torch
+    from jarabotransientrendering_b200 import _abi
+    sc = S.cornell(width=128, height=128, time_bins=2048, exposure=0.005, sqrt_spp=1, max_bounces=2)
+    film_bytes = sc.width * sc.height * sc.time_bins * 3 * 8          # 805 MB
+    _abi.check(_abi.lib().tr_release_cached_memory(0))
+    free0 = torch.cuda.mem_get_info()[0]
+    with gpu.Context(sc) as c:
+        c.render(0, 1)
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 >= film_bytes                                  # kept by the pool
+    with gpu.Context(sc) as c:
+        c.render(0, 1)
+    free2 = torch.cuda.mem_get_info()[0]
+    assert abs(free2 - free1) < film_bytes // 4                         # reused, not mapped again
+    _abi.check(_abi.lib().tr_release_cached_memory(0))
+    free3 = torch.cuda.mem_get_info()[0]
+    assert free3 - free2 >= film_bytes
+    assert _abi.lib().tr_release_cached_memory(99) == 1
