@@ -4,6 +4,7 @@
 #include "bvh_build.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <thread>
 #include <chrono>
@@ -358,32 +359,65 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
     B.max_threads = hw;
     B.build(0, nt, 0);
 
-    // Flatten: one GpuNode per interior node in depth-first preorder (left child adjacent to
-    // its parent), leaf triangles in the same order.  Every subtree's interior-node and
-    // triangle counts are known, so each subtree is written at its own offsets, large ones on
-    // their own threads.
+    // Collapse to four-child nodes: a node starts with its binary children and repeatedly
+    // opens the interior child of largest surface area (the first on ties) while it has fewer
+    // than four.  Pass 1 records each four-child node's binary children and its subtree's
+    // node count and depth; pass 2 writes every subtree at its own offsets (depth-first
+    // preorder, children in left-to-right order, leaf triangles in the same order), large
+    // subtrees on their own threads.
     const Node& root = B.nodes[0];
-    out.nodes.assign(std::max<uint32_t>(1u, root.n_inner), GpuNode{});
-    out.tris.resize(nt);
-    std::atomic<uint32_t> leaves{0};
-    auto write_box = [](GpuNode& g, int slot, const Box& bin) {
-        // one ulp outward: a ray lying exactly in a face plane of a box (zero direction
-        // component, origin on the face) still sees a non-empty slab interval
-        Box b = bin;
-        for (int k = 0; k < 3; ++k) {
-            if (b.lo[k] <= b.hi[k]) {
-                b.lo[k] = std::nextafter(b.lo[k], -INFINITY);
-                b.hi[k] = std::nextafter(b.hi[k], INFINITY);
+    const size_t cap = Builder::capacity(nt);
+    std::unique_ptr<std::array<int32_t, 4>[]> kids(new std::array<int32_t, 4>[cap]);
+    std::unique_ptr<uint32_t[]> n4(new uint32_t[cap]);
+    std::unique_ptr<uint32_t[]> d4(new uint32_t[cap]);
+    std::atomic<int> cthreads{1};
+    std::function<void(int32_t)> collapse = [&](int32_t n) {
+        int32_t c[4] = {B.nodes[n].left, B.nodes[n].right, -1, -1};
+        int k = 2;
+        while (k < 4) {
+            int best = -1;
+            float ba = -1.0f;
+            for (int j = 0; j < k; ++j) {
+                const Node& q = B.nodes[c[j]];
+                if (q.left < 0) continue;
+                const float a = q.box.area();
+                if (a > ba) { ba = a; best = j; }
+            }
+            if (best < 0) break;
+            const Node& q = B.nodes[c[best]];
+            for (int j = k; j > best + 1; --j) c[j] = c[j - 1];
+            c[best] = q.left;
+            c[best + 1] = q.right;
+            ++k;
+        }
+        kids[n] = {c[0], c[1], c[2], c[3]};
+        // the children's subtrees: the largest one of several on another thread
+        int32_t sub[4];
+        int ns = 0;
+        for (int j = 0; j < 4; ++j)
+            if (c[j] >= 0 && B.nodes[c[j]].left >= 0) sub[ns++] = c[j];
+        std::thread th;
+        int spawned = -1;
+        if (ns > 1) {
+            int big = 0;
+            for (int j = 1; j < ns; ++j)
+                if (B.nodes[sub[j]].n_tris > B.nodes[sub[big]].n_tris) big = j;
+            if (B.nodes[sub[big]].n_tris > kParallelCutoff && cthreads.fetch_add(1) < hw) {
+                spawned = big;
+                th = std::thread([&, s0 = sub[big]] { collapse(s0); });
+            } else if (B.nodes[sub[big]].n_tris > kParallelCutoff) {
+                cthreads.fetch_sub(1);
             }
         }
-        if (slot == 0) {
-            g.a[0] = b.lo[0]; g.a[1] = b.hi[0]; g.a[2] = b.lo[1]; g.a[3] = b.hi[1];
-            g.c[0] = b.lo[2]; g.c[1] = b.hi[2];
-        } else {
-            g.b[0] = b.lo[0]; g.b[1] = b.hi[0]; g.b[2] = b.lo[1]; g.b[3] = b.hi[1];
-            g.c[2] = b.lo[2]; g.c[3] = b.hi[2];
-        }
+        for (int j = 0; j < ns; ++j)
+            if (j != spawned) collapse(sub[j]);
+        if (spawned >= 0) { th.join(); cthreads.fetch_sub(1); }
+        uint32_t cnt = 1, dep = 0;
+        for (int j = 0; j < ns; ++j) { cnt += n4[sub[j]]; dep = std::max(dep, d4[sub[j]]); }
+        n4[n] = cnt;
+        d4[n] = dep + 1;
     };
+    std::atomic<uint32_t> leaves{0};
     auto leaf_ref = [&](const Node& n, uint32_t toff) -> int32_t {
         for (uint32_t i = 0; i < n.count; ++i) {
             const uint32_t t = prim[n.first + i].id;
@@ -397,45 +431,81 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
         leaves.fetch_add(1, std::memory_order_relaxed);
         return ~(int32_t)((toff << 3) | n.count);
     };
-    std::atomic<int> fthreads{1};
-    // interior node ni at GPU index gi, its leaf triangles from toff
-    std::function<void(uint32_t, uint32_t, uint32_t)> flat = [&](uint32_t ni, uint32_t gi, uint32_t toff) {
-        const Node& n = B.nodes[ni];
-        const Node& L = B.nodes[n.left];
-        const Node& R = B.nodes[n.right];
-        GpuNode& g = out.nodes[gi];
-        write_box(g, 0, L.box);
-        write_box(g, 1, R.box);
-        const uint32_t gl = gi + 1, gr = gi + 1 + L.n_inner;
-        const uint32_t tl = toff, tr = toff + L.n_tris;
-        g.d[0] = L.left < 0 ? leaf_ref(L, tl) : (int32_t)gl;
-        g.d[1] = R.left < 0 ? leaf_ref(R, tr) : (int32_t)gr;
-        g.d[2] = 0; g.d[3] = 0;
-        const bool lin = L.left >= 0, rin = R.left >= 0;
-        if (lin && rin && L.n_tris > kParallelCutoff && fthreads.fetch_add(1) < hw) {
-            std::thread t([&, gl, tl] { flat((uint32_t)n.left, gl, tl); });
-            flat((uint32_t)n.right, gr, tr);
-            t.join();
-            fthreads.fetch_sub(1);
-        } else {
-            if (lin && rin && L.n_tris > kParallelCutoff) fthreads.fetch_sub(1);
-            if (lin) flat((uint32_t)n.left, gl, tl);
-            if (rin) flat((uint32_t)n.right, gr, tr);
+    auto write_box = [](GpuNode& g, int j, const Box& bin) {
+        // one ulp outward: a ray lying exactly in a face plane of a box (zero direction
+        // component, origin on the face) still sees a non-empty slab interval
+        Box b = bin;
+        for (int k = 0; k < 3; ++k) {
+            if (b.lo[k] <= b.hi[k]) {
+                b.lo[k] = std::nextafter(b.lo[k], -INFINITY);
+                b.hi[k] = std::nextafter(b.hi[k], INFINITY);
+            }
         }
+        g.lox[j] = b.lo[0]; g.hix[j] = b.hi[0];
+        g.loy[j] = b.lo[1]; g.hiy[j] = b.hi[1];
+        g.loz[j] = b.lo[2]; g.hiz[j] = b.hi[2];
     };
+    auto empty_slot = [](GpuNode& g, int j) {
+        g.lox[j] = g.hix[j] = g.loy[j] = g.hiy[j] = g.loz[j] = g.hiz[j] = 0.0f;
+        g.child[j] = ~(int32_t)0;             // leaf of 0 triangles: never entered
+    };
+    std::atomic<int> fthreads{1};
+    // four-child node of binary node n at GPU index gi, its leaf triangles from toff
+    std::function<void(int32_t, uint32_t, uint32_t)> flat = [&](int32_t n, uint32_t gi, uint32_t toff) {
+        GpuNode& g = out.nodes[gi];
+        g.pad[0] = g.pad[1] = g.pad[2] = g.pad[3] = 0;
+        struct Sub { int32_t n; uint32_t gi, toff; };
+        Sub sub[4];
+        int ns = 0;
+        uint32_t gnext = gi + 1, t = toff;
+        for (int j = 0; j < 4; ++j) {
+            const int32_t c = kids[n][j];
+            if (c < 0) { empty_slot(g, j); continue; }
+            const Node& q = B.nodes[c];
+            write_box(g, j, q.box);
+            if (q.left >= 0) {
+                g.child[j] = (int32_t)gnext;
+                sub[ns++] = {c, gnext, t};
+                gnext += n4[c];
+            } else {
+                g.child[j] = leaf_ref(q, t);
+            }
+            t += q.n_tris;
+        }
+        std::thread th;
+        int spawned = -1;
+        if (ns > 1) {
+            int big = 0;
+            for (int j = 1; j < ns; ++j)
+                if (B.nodes[sub[j].n].n_tris > B.nodes[sub[big].n].n_tris) big = j;
+            if (B.nodes[sub[big].n].n_tris > kParallelCutoff && fthreads.fetch_add(1) < hw) {
+                spawned = big;
+                th = std::thread([&, sb = sub[big]] { flat(sb.n, sb.gi, sb.toff); });
+            } else if (B.nodes[sub[big].n].n_tris > kParallelCutoff) {
+                fthreads.fetch_sub(1);
+            }
+        }
+        for (int j = 0; j < ns; ++j)
+            if (j != spawned) flat(sub[j].n, sub[j].gi, sub[j].toff);
+        if (spawned >= 0) { th.join(); fthreads.fetch_sub(1); }
+    };
+    out.tris.resize(nt);
     if (root.left < 0) {
-        // single-leaf scene: a root whose second child is empty
-        Box emptybox; emptybox.empty();
+        // single-leaf scene: one node whose first child is the leaf
+        out.nodes.assign(1, GpuNode{});
         write_box(out.nodes[0], 0, root.box);
-        write_box(out.nodes[0], 1, emptybox);
-        out.nodes[0].d[0] = leaf_ref(root, 0);
-        out.nodes[0].d[1] = ~(int32_t)0;   // empty leaf (count 0)
-        out.nodes[0].d[2] = 0; out.nodes[0].d[3] = 0;
+        out.nodes[0].child[0] = leaf_ref(root, 0);
+        for (int j = 1; j < 4; ++j) empty_slot(out.nodes[0], j);
+        out.depth = 1;
     } else {
+        collapse(0);
+        out.nodes.resize(n4[0]);
         flat(0, 0, 0);
+        out.depth = d4[0];
     }
+    out.stack = 3 * out.depth + 1;
+    out.binary_depth = B.depth.load();
     out.leaves = leaves.load();
-    out.depth = B.depth.load();
     out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return true;
 }

@@ -6,15 +6,17 @@
 
 namespace trh {
 
-// 64-byte two-child node, read by the kernels as four 16-byte vector loads:
-//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
-//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)   d = (ref0, ref1, 0, 0)
-// ref >= 0: interior node index; ref < 0: leaf, ~ref = (first_triangle << 3) | count.
+// 128-byte four-child node, read by the kernels as eight 16-byte vector loads:
+//   q0..q5 = child bounds lo.x[4], hi.x[4], lo.y[4], hi.y[4], lo.z[4], hi.z[4]
+//   q6 = child refs[4], q7 = padding
+// ref >= 0: interior node index; ref < 0: leaf, ~ref = (first_triangle << 3) | count
+// (count 0: empty slot, never entered).
 struct alignas(16) GpuNode {
-    float a[4], b[4], c[4];
-    int32_t d[4];
+    float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
+    int32_t child[4];
+    int32_t pad[4];
 };
-static_assert(sizeof(GpuNode) == 64, "node must be 64 bytes");
+static_assert(sizeof(GpuNode) == 128, "node must be 128 bytes");
 
 // 48-byte triangle in leaf order: v0.xyz + triangle id (bits), v1.xyz, v2.xyz.
 struct alignas(16) GpuTri {
@@ -27,12 +29,15 @@ static_assert(sizeof(GpuTri) == 48, "triangle must be 48 bytes");
 struct BvhBuildResult {
     std::vector<GpuNode> nodes;
     std::vector<GpuTri> tris;
-    uint32_t depth = 0;
+    uint32_t depth = 0;          // four-child levels on the deepest path (root = 1)
+    uint32_t stack = 0;          // traversal stack entries a ray can need: 3 per level
+    uint32_t binary_depth = 0;   // depth of the binary SAH tree it was collapsed from
     uint32_t leaves = 0;
     double build_ms = 0.0;
 };
 
-// Binned SAH (32 bins over centroid bounds), leaves of at most `max_leaf` (<= 7) triangles.
+// Binned SAH (32 bins over centroid bounds), leaves of at most `max_leaf` (<= 7) triangles,
+// collapsed to four-child nodes (each node opens its largest-area interior children).
 // vertices [nv][3], triangles [nt][3].  Returns false (with msg) on bad input.
 bool build_bvh(const float* vertices, uint32_t nv, const uint32_t* triangles, uint32_t nt,
                uint32_t max_leaf, BvhBuildResult& out, std::string* msg);

@@ -515,14 +515,15 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             delete x;
             return fail(TR_ERR_INVALID_ARGUMENT, msg);
         }
-        if (bvh.depth + 1 >= (uint32_t)trk::kStack) {
+        if (bvh.stack > (uint32_t)trk::kStack) {
             delete x;
             return fail(TR_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
         }
         x->bvh_nodes = (uint32_t)bvh.nodes.size();
-        x->bvh_depth = bvh.depth;
+        x->bvh_depth = bvh.stack - 1;               // sizes the shared-memory traversal stack
+        x->bvh_levels = bvh.depth;
         x->bvh_ms = bvh.build_ms;
-        x->d_nodes = x->alloc<float4>(bvh.nodes.size() * 4);
+        x->d_nodes = x->alloc<float4>(bvh.nodes.size() * 8);
         upload(x->d_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode));
         x->d_tris = x->alloc<float4>(bvh.tris.size() * 3);
         upload(x->d_tris, bvh.tris.data(), bvh.tris.size() * sizeof(trh::GpuTri));
@@ -646,7 +647,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
 
         x->stats.bvh_build_ms = x->bvh_ms;
         x->stats.bvh_nodes = x->bvh_nodes;
-        x->stats.bvh_depth = x->bvh_depth;
+        x->stats.bvh_depth = x->bvh_levels;
     } catch (const CudaError& e) {
         x->release();
         delete x;

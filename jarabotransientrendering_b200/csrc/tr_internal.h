@@ -121,7 +121,7 @@ struct tr_ctx {
     float4* d_mats2 = nullptr;
     float4* d_lights = nullptr;
     trk::SceneDev scene{};
-    uint32_t nt = 0, bvh_nodes = 0, bvh_depth = 0;
+    uint32_t nt = 0, bvh_nodes = 0, bvh_depth = 0, bvh_levels = 0;   // bvh_depth: stack entries - 1
     double bvh_ms = 0.0;
 
     tr_camera cam{};

@@ -22,10 +22,31 @@ using namespace trd;
 
 
 // -----------------------------------------------------------------------------------------
-// BVH traversal: two-child 64-byte nodes, near-first, conservative slab test (Ize 2013),
-// watertight triangle test, per-thread stack in shared memory (strided by block size).
-// Closest hit: smallest t in (tnear, tfar], ties -> lower triangle id (order independent).
+// BVH traversal: four-child 128-byte nodes (one conservative slab test for the four children,
+// after Ize 2013), hit children visited nearest first (a five-exchange sorting network), the
+// others pushed on a per-thread stack in shared memory (strided by block size); watertight
+// triangle test.  Closest hit: smallest t in (tnear, tfar], ties -> lower triangle id (order
+// independent, so the result does not depend on the tree).
 // -----------------------------------------------------------------------------------------
+__device__ __forceinline__ void slab4(float lo_x, float hi_x, float lo_y, float hi_y, float lo_z, float hi_z, int ref,
+                                      float ox, float oy, float oz, float ix, float iy, float iz, float tnear,
+                                      float best, float& key) {
+    const float lx = (lo_x - ox) * ix, hx = (hi_x - ox) * ix;
+    const float ly = (lo_y - oy) * iy, hy = (hi_y - oy) * iy;
+    const float lz = (lo_z - oz) * iz, hz = (hi_z - oz) * iz;
+    const float tmin = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tnear));
+    const float tmax = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), best)) * 1.00000036f;
+    // empty slots are leaves of 0 triangles
+    const bool use = ref >= 0 || ((~ref) & 7) != 0;
+    key = (use && tmin <= tmax) ? tmin : __int_as_float(0x7f800000);
+}
+__device__ __forceinline__ void order2(float& ka, int& ra, float& kb, int& rb) {
+    if (kb < ka) {
+        const float tk = ka; ka = kb; kb = tk;
+        const int tr = ra; ra = rb; rb = tr;
+    }
+}
+
 template <bool kAnyHit>
 __device__ __forceinline__ uint32_t traverse(const SceneDev& sc, const WRay& r, float tfar,
                                              float& t_out, float& u_out, float& v_out,
@@ -37,36 +58,35 @@ __device__ __forceinline__ uint32_t traverse(const SceneDev& sc, const WRay& r, 
     int node = 0;
     const float ox = r.o.x, oy = r.o.y, oz = r.o.z;
     const float ix = r.inv.x, iy = r.inv.y, iz = r.inv.z;
+    const float kInf = __int_as_float(0x7f800000);
     for (;;) {
         while (node >= 0) {
-            const float4* np = sc.nodes + 4 * node;
-            const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-            const int4 d = __ldg(reinterpret_cast<const int4*>(np + 3));
-            float lx0 = (a.x - ox) * ix, hx0 = (a.y - ox) * ix;
-            float ly0 = (a.z - oy) * iy, hy0 = (a.w - oy) * iy;
-            float lz0 = (c.x - oz) * iz, hz0 = (c.y - oz) * iz;
-            float lx1 = (b.x - ox) * ix, hx1 = (b.y - ox) * ix;
-            float ly1 = (b.z - oy) * iy, hy1 = (b.w - oy) * iy;
-            float lz1 = (c.z - oz) * iz, hz1 = (c.w - oz) * iz;
-            float tmin0 = fmaxf(fmaxf(fminf(lx0, hx0), fminf(ly0, hy0)), fmaxf(fminf(lz0, hz0), r.tnear));
-            float tmax0 = fminf(fminf(fmaxf(lx0, hx0), fmaxf(ly0, hy0)), fminf(fmaxf(lz0, hz0), best)) * 1.00000036f;
-            float tmin1 = fmaxf(fmaxf(fminf(lx1, hx1), fminf(ly1, hy1)), fmaxf(fminf(lz1, hz1), r.tnear));
-            float tmax1 = fminf(fminf(fmaxf(lx1, hx1), fmaxf(ly1, hy1)), fminf(fmaxf(lz1, hz1), best)) * 1.00000036f;
-            const bool h0 = tmin0 <= tmax0, h1 = tmin1 <= tmax1;
-            if (h0 && h1) {
-                const bool first0 = tmin0 <= tmin1;
-                stack[sp * stride] = first0 ? d.y : d.x;
-                ++sp;
-                node = first0 ? d.x : d.y;
-            } else if (h0) {
-                node = d.x;
-            } else if (h1) {
-                node = d.y;
-            } else {
+            const float4* np = sc.nodes + 8 * node;
+            const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+            const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+            const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+            float k0, k1, k2, k3;
+            int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
+            slab4(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, c0, ox, oy, oz, ix, iy, iz, r.tnear, best, k0);
+            slab4(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, c1, ox, oy, oz, ix, iy, iz, r.tnear, best, k1);
+            slab4(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, c2, ox, oy, oz, ix, iy, iz, r.tnear, best, k2);
+            slab4(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, c3, ox, oy, oz, ix, iy, iz, r.tnear, best, k3);
+            order2(k0, c0, k1, c1);
+            order2(k2, c2, k3, c3);
+            order2(k0, c0, k2, c2);
+            order2(k1, c1, k3, c3);
+            order2(k1, c1, k2, c2);
+            if (k0 == kInf) {
                 if (sp == 0) goto done;
                 --sp;
                 node = stack[sp * stride];
+                continue;
             }
+            // farthest first, so the nearest of the others is popped next
+            if (k3 != kInf) { stack[sp * stride] = c3; ++sp; }
+            if (k2 != kInf) { stack[sp * stride] = c2; ++sp; }
+            if (k1 != kInf) { stack[sp * stride] = c1; ++sp; }
+            node = c0;
         }
         {
             const uint32_t ref = (uint32_t)(~node);

@@ -7,7 +7,7 @@
 
 namespace trk {
 
-constexpr int kStack = 64;          // max traversal stack entries per thread (BVH depth + 1)
+constexpr int kStack = 96;          // max traversal stack entries per thread (3 per four-child level + 1)
 constexpr int kTraceBlock = 128;    // threads per traversal block
 constexpr int kTraceMinBlocks = 8;  // register budget: 8 traversal blocks per SM
 constexpr int kSplatBlock = 512;    // threads per splat block
@@ -28,7 +28,7 @@ struct SceneDev {
     float lambda;             // free-flight rate: mean extinction avg(sigma_t), or 4 / (film
                               // duration) in time-sampling mode
     float g;
-    uint32_t bvh_depth;       // deepest leaf; the traversal stack holds bvh_depth + 1 entries
+    uint32_t bvh_depth;       // traversal stack entries - 1 (3 per four-child level)
     float bmin[3], binv[3];   // scene box (feature normalisation of the learned proposal)
 };
 

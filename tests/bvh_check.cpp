@@ -1,7 +1,8 @@
 // Host-only check of the product BVH builder (jarabotransientrendering_b200/csrc/bvh_build.cpp):
 // reads vertices/triangles from a raw file, builds, and verifies the invariants the GPU
 // traversal relies on: every triangle appears exactly once in leaf order, child boxes contain
-// their triangles, leaf refs and child indices are in range, depth is what was reported.
+// their triangles, leaf refs and child indices are in range, every node is reachable, the
+// four-child depth is what was reported and the reported stack covers it.
 // Usage: bvh_check FILE  (FILE: u32 nv, u32 nt, float[nv*3], u32[nt*3])
 #include <cstdio>
 #include <cstring>
@@ -36,15 +37,15 @@ int main(int argc, char** argv) {
         if (it.node < 0 || (size_t)it.node >= r.nodes.size()) { std::printf("bad node\n"); return 1; }
         ++visited;
         const trh::GpuNode& n = r.nodes[it.node];
-        for (int c = 0; c < 2; ++c) {
-            float lo[3] = {c ? n.b[0] : n.a[0], c ? n.b[2] : n.a[2], c ? n.c[2] : n.c[0]};
-            float hi[3] = {c ? n.b[1] : n.a[1], c ? n.b[3] : n.a[3], c ? n.c[3] : n.c[1]};
-            int32_t ref = n.d[c];
+        if (it.depth + 1 > maxd) maxd = it.depth + 1;          // four-child levels (root = 1)
+        for (int c = 0; c < 4; ++c) {
+            float lo[3] = {n.lox[c], n.loy[c], n.loz[c]};
+            float hi[3] = {n.hix[c], n.hiy[c], n.hiz[c]};
+            int32_t ref = n.child[c];
             if (ref >= 0) { st.push_back({ref, it.depth + 1}); continue; }
             uint32_t u = (uint32_t)(~ref), first = u >> 3, cnt = u & 7u;
             if (cnt == 0) continue;
             ++leaves;
-            if (it.depth + 1 > maxd) maxd = it.depth + 1;
             if (first + cnt > r.tris.size() || cnt > 4) { std::printf("bad leaf\n"); return 1; }
             for (uint32_t k = first; k < first + cnt; ++k) {
                 const float* q[3] = {r.tris[k].v0, r.tris[k].v1, r.tris[k].v2};
@@ -54,7 +55,9 @@ int main(int argc, char** argv) {
         }
     }
     if (visited != r.nodes.size()) { std::printf("unreachable nodes %u of %zu\n", visited, r.nodes.size()); return 1; }
-    std::printf("{\"nodes\": %zu, \"leaves\": %u, \"depth\": %u, \"walk_depth\": %u, \"build_ms\": %.1f}\n",
-                r.nodes.size(), leaves, r.depth, maxd, r.build_ms);
-    return maxd > r.depth + 1 ? 1 : 0;
+    std::printf("{\"nodes\": %zu, \"leaves\": %u, \"depth\": %u, \"walk_depth\": %u, \"stack\": %u, "
+                "\"binary_depth\": %u, \"build_ms\": %.1f}\n",
+                r.nodes.size(), leaves, r.depth, maxd, r.stack, r.binary_depth, r.build_ms);
+    // the traversal stack holds at most three siblings per level of the path being walked
+    return (maxd != r.depth || r.stack < 3 * maxd) ? 1 : 0;
 }
