@@ -108,8 +108,12 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     return TR_OK;
 }
 
-void upload(void* dst, const void* src, size_t bytes) {
-    TR_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+// Host-to-device copy ordered on `s`, the stream whose kernels read the data.  (A plain
+// cudaMemcpy runs on the legacy default stream, which does not order with the library's
+// non-blocking streams, and from pageable memory it may return before the data has landed.)
+void upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    TR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    TR_CUDA(cudaStreamSynchronize(s));        // the host buffer may be released after return
 }
 
 }  // namespace
@@ -203,7 +207,7 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = x->alloc<unsigned long long>(8);
-        TR_CUDA(cudaMemset(w.stats, 0, 8 * sizeof(unsigned long long)));
+        TR_CUDA(cudaMemsetAsync(w.stats, 0, 8 * sizeof(unsigned long long), x->s()));
     }
     w.capacity = capacity;
 }
@@ -524,9 +528,9 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         x->bvh_levels = bvh.depth;
         x->bvh_ms = bvh.build_ms;
         x->d_nodes = x->alloc<float4>(bvh.nodes.size() * 8);
-        upload(x->d_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode));
+        upload(x->d_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode), x->stream);
         x->d_tris = x->alloc<float4>(bvh.tris.size() * 3);
-        upload(x->d_tris, bvh.tris.data(), bvh.tris.size() * sizeof(trh::GpuTri));
+        upload(x->d_tris, bvh.tris.data(), bvh.tris.size() * sizeof(trh::GpuTri), x->stream);
 
         // per-triangle reference geometric normal normalize(cross(p2-p0, p1-p0)) (World.h:449)
         std::vector<float4> ng(s->num_triangles);
@@ -543,7 +547,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             ng[t] = make_float4(n.x, n.y, n.z, mf);
         }
         x->d_tri_ng = x->alloc<float4>(ng.size());
-        upload(x->d_tri_ng, ng.data(), ng.size() * sizeof(float4));
+        upload(x->d_tri_ng, ng.data(), ng.size() * sizeof(float4), x->stream);
 
         std::vector<float4> mats(s->num_materials), mats2(s->num_materials);
         for (uint32_t i = 0; i < s->num_materials; ++i) {
@@ -554,9 +558,9 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             mats2[i] = make_float4(m.alpha, 0.f, 0.f, 0.f);
         }
         x->d_mats = x->alloc<float4>(mats.size());
-        upload(x->d_mats, mats.data(), mats.size() * sizeof(float4));
+        upload(x->d_mats, mats.data(), mats.size() * sizeof(float4), x->stream);
         x->d_mats2 = x->alloc<float4>(mats2.size());
-        upload(x->d_mats2, mats2.data(), mats2.size() * sizeof(float4));
+        upload(x->d_mats2, mats2.data(), mats2.size() * sizeof(float4), x->stream);
 
         std::vector<float4> lights(5 * (size_t)s->num_lights);
         for (uint32_t i = 0; i < s->num_lights; ++i) {
@@ -570,7 +574,7 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             lights[5 * i + 4] = make_float4(L.normal[0], L.normal[1], L.normal[2], 0.f);
         }
         x->d_lights = x->alloc<float4>(lights.size());
-        upload(x->d_lights, lights.data(), lights.size() * sizeof(float4));
+        upload(x->d_lights, lights.data(), lights.size() * sizeof(float4), x->stream);
 
         trk::SceneDev& sc = x->scene;
         sc.nodes = x->d_nodes; sc.tris = x->d_tris; sc.tri_ng = x->d_tri_ng;
@@ -1071,11 +1075,12 @@ extern "C" tr_status tr_guide_create(int device, uint64_t seed, tr_guide** out) 
             const float a = l < 3 ? std::sqrt(6.0f / 64.0f) : 0.05f;
             for (int i = 0; i < 4096; ++i) p[(size_t)l * 4096 + i] = a * uni();
         }
-        TR_CUDA(cudaMemcpy(g->params, p.data(), sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyHostToDevice));
-        TR_CUDA(cudaMemset(g->m1, 0, sizeof(float) * TR_GUIDE_PARAMS));
-        TR_CUDA(cudaMemset(g->m2, 0, sizeof(float) * TR_GUIDE_PARAMS));
-        TR_CUDA(cudaMemset(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS));
-        TR_CUDA(cudaMemset(g->err, 0, sizeof(int)));
+        // everything ordered on the guide's stream (see upload)
+        TR_CUDA(cudaMemcpyAsync(g->params, p.data(), sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyHostToDevice, g->stream));
+        TR_CUDA(cudaMemsetAsync(g->m1, 0, sizeof(float) * TR_GUIDE_PARAMS, g->stream));
+        TR_CUDA(cudaMemsetAsync(g->m2, 0, sizeof(float) * TR_GUIDE_PARAMS, g->stream));
+        TR_CUDA(cudaMemsetAsync(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS, g->stream));
+        TR_CUDA(cudaMemsetAsync(g->err, 0, sizeof(int), g->stream));
         TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, g->stream));
         TR_CUDA(cudaStreamSynchronize(g->stream));
     } catch (const CudaError& e) {
@@ -1091,7 +1096,7 @@ extern "C" tr_status tr_guide_set_params(tr_guide* g, const float* params) {
     if (!g || !params) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
     try {
         TR_CUDA(cudaSetDevice(g->device));
-        TR_CUDA(cudaMemcpy(g->params, params, sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyHostToDevice));
+        TR_CUDA(cudaMemcpyAsync(g->params, params, sizeof(float) * TR_GUIDE_PARAMS, cudaMemcpyHostToDevice, g->stream));
         TR_CUDA(trg::pack_weights(g->params, g->w_fwd, g->w_bwd, g->stream));
         TR_CUDA(cudaStreamSynchronize(g->stream));
     } catch (const CudaError& e) {

@@ -177,7 +177,7 @@ void ensure_batch_wave(tr_batch* b, uint32_t capacity) {
     if (!w.counters) w.counters = b->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
         w.stats = b->alloc<unsigned long long>(8);
-        TR_CUDA(cudaMemset(w.stats, 0, 8 * sizeof(unsigned long long)));
+        TR_CUDA(cudaMemsetAsync(w.stats, 0, 8 * sizeof(unsigned long long), b->stream));
     }
     w.capacity = capacity;
 }
@@ -380,7 +380,10 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
             b->splat_auto.push_back((uint32_t)x->splat_g);
         }
         b->d_scenes = b->alloc<trk::SceneSlot>(n);
-        TR_CUDA(cudaMemcpy(b->d_scenes, slots.data(), n * sizeof(trk::SceneSlot), cudaMemcpyHostToDevice));
+        // ordered on the batch's stream (a plain cudaMemcpy from pageable memory may return
+        // before the data lands, on a stream that does not order with this one)
+        TR_CUDA(cudaMemcpyAsync(b->d_scenes, slots.data(), n * sizeof(trk::SceneSlot), cudaMemcpyHostToDevice, b->stream));
+        TR_CUDA(cudaStreamSynchronize(b->stream));
         b->d_cur = b->alloc<uint32_t>(1);
         b->trace_grid = trk::trace_grid_size(b->device, b->bvh_depth, true);
         b->stats.device_bytes = b->bytes;

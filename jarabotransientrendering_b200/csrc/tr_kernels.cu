@@ -47,71 +47,88 @@ __device__ __forceinline__ void order2(float& ka, int& ra, float& kb, int& rb) {
     }
 }
 
+// Traversal state of one ray between calls of trav_run: next node (or leaf ref), stack depth,
+// closest hit so far.
+struct Trav {
+    int node, sp;
+    float best, bu, bv;
+    uint32_t bid;
+};
+__device__ __forceinline__ void trav_init(Trav& st, float tfar) {
+    st.node = 0; st.sp = 0; st.best = tfar; st.bu = 0.f; st.bv = 0.f; st.bid = kInvalid;
+}
+
+// Runs at most `budget` node or leaf visits of the ray's traversal; returns true once the
+// traversal is complete (closest hit, or any hit with kAnyHit, in st).  The stack lives in
+// shared memory at stack[k * stride].
 template <bool kAnyHit>
-__device__ __forceinline__ uint32_t traverse(const SceneDev& sc, const WRay& r, float tfar,
-                                             float& t_out, float& u_out, float& v_out,
-                                             int* __restrict__ stack, int stride) {
-    float best = tfar;
-    uint32_t bid = kInvalid;
-    float bu = 0.f, bv = 0.f;
-    int sp = 0;
-    int node = 0;
+__device__ __forceinline__ bool trav_run(const SceneDev& sc, const WRay& r, Trav& st, int* __restrict__ stack,
+                                         int stride, int budget) {
     const float ox = r.o.x, oy = r.o.y, oz = r.o.z;
     const float ix = r.inv.x, iy = r.inv.y, iz = r.inv.z;
     const float kInf = __int_as_float(0x7f800000);
     for (;;) {
-        while (node >= 0) {
-            const float4* np = sc.nodes + 8 * node;
+        if (budget-- == 0) return false;
+        if (st.node >= 0) {
+            const float4* np = sc.nodes + 8 * st.node;
             const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
             const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
             const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
             float k0, k1, k2, k3;
             int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
-            slab4(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, c0, ox, oy, oz, ix, iy, iz, r.tnear, best, k0);
-            slab4(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, c1, ox, oy, oz, ix, iy, iz, r.tnear, best, k1);
-            slab4(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, c2, ox, oy, oz, ix, iy, iz, r.tnear, best, k2);
-            slab4(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, c3, ox, oy, oz, ix, iy, iz, r.tnear, best, k3);
+            slab4(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, c0, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k0);
+            slab4(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, c1, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k1);
+            slab4(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, c2, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k2);
+            slab4(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, c3, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k3);
             order2(k0, c0, k1, c1);
             order2(k2, c2, k3, c3);
             order2(k0, c0, k2, c2);
             order2(k1, c1, k3, c3);
             order2(k1, c1, k2, c2);
             if (k0 == kInf) {
-                if (sp == 0) goto done;
-                --sp;
-                node = stack[sp * stride];
+                if (st.sp == 0) return true;
+                --st.sp;
+                st.node = stack[st.sp * stride];
                 continue;
             }
             // farthest first, so the nearest of the others is popped next
-            if (k3 != kInf) { stack[sp * stride] = c3; ++sp; }
-            if (k2 != kInf) { stack[sp * stride] = c2; ++sp; }
-            if (k1 != kInf) { stack[sp * stride] = c1; ++sp; }
-            node = c0;
+            if (k3 != kInf) { stack[st.sp * stride] = c3; ++st.sp; }
+            if (k2 != kInf) { stack[st.sp * stride] = c2; ++st.sp; }
+            if (k1 != kInf) { stack[st.sp * stride] = c1; ++st.sp; }
+            st.node = c0;
+            continue;
         }
-        {
-            const uint32_t ref = (uint32_t)(~node);
-            const uint32_t first = ref >> 3, cnt = ref & 7u;
-            for (uint32_t k = 0; k < cnt; ++k) {
-                const float4* tp = sc.tris + 3 * (first + k);
-                const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
-                const uint32_t id = __float_as_uint(q0.w);
-                float t, u, v;
-                if (wt_hit(r, f3of(q0), f3of(q1), f3of(q2), best, t, u, v)) {
-                    if (t < best || bid == kInvalid || id < bid) {
-                        best = t; bid = id; bu = u; bv = v;
-                        if (kAnyHit) goto done;
-                    }
+        const uint32_t ref = (uint32_t)(~st.node);
+        const uint32_t first = ref >> 3, cnt = ref & 7u;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const float4* tp = sc.tris + 3 * (first + k);
+            const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
+            const uint32_t id = __float_as_uint(q0.w);
+            float t, u, v;
+            if (wt_hit(r, f3of(q0), f3of(q1), f3of(q2), st.best, t, u, v)) {
+                if (t < st.best || st.bid == kInvalid || id < st.bid) {
+                    st.best = t; st.bid = id; st.bu = u; st.bv = v;
+                    if (kAnyHit) return true;
                 }
             }
         }
-        if (sp == 0) break;
-        --sp;
-        node = stack[sp * stride];
+        if (st.sp == 0) return true;
+        --st.sp;
+        st.node = stack[st.sp * stride];
     }
-done:
-    t_out = bid == kInvalid ? tfar : best;
-    u_out = bu; v_out = bv;
-    return bid;
+}
+
+// Whole traversal in one call (used where one thread owns a fixed set of rays).
+template <bool kAnyHit>
+__device__ __forceinline__ uint32_t traverse(const SceneDev& sc, const WRay& r, float tfar,
+                                             float& t_out, float& u_out, float& v_out,
+                                             int* __restrict__ stack, int stride) {
+    Trav st;
+    trav_init(st, tfar);
+    trav_run<kAnyHit>(sc, r, st, stack, stride, 0x7fffffff);
+    t_out = st.bid == kInvalid ? tfar : st.best;
+    u_out = st.bu; v_out = st.bv;
+    return st.bid;
 }
 
 // -----------------------------------------------------------------------------------------
@@ -204,79 +221,112 @@ __global__ void __launch_bounds__(256) k_raygen(const __grid_constant__ Params p
 // -----------------------------------------------------------------------------------------
 // extend / shadow: persistent warps fetch 32 queue entries at a time.
 // -----------------------------------------------------------------------------------------
+// Node and leaf visits a lane makes between two refills of the warp's finished lanes.
+constexpr int kTravBudget = 8;
+
+// Warp-aggregated refill from a queue: every lane with busy == false takes the next entry
+// index (one atomic per warp); lanes left without an entry get idx >= n.  `drained` (warp
+// uniform) records that the queue is exhausted.
+__device__ __forceinline__ uint32_t refill(bool busy, uint32_t* cursor, uint32_t n, bool& drained) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned idle = __ballot_sync(kFull, !busy);
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(cursor, (uint32_t)__popc(idle));
+    base = __shfl_sync(kFull, base, 0);
+    if (base + (uint32_t)__popc(idle) >= n) drained = true;
+    return base + (uint32_t)__popc(idle & lanemask_lt());
+}
+
+// Closest hit of each queued ray.  Persistent warps; a lane whose ray is done takes the next
+// queued ray at the warp's next refill point, so the lanes stay busy while rays of very
+// different traversal lengths share a warp.
 template <bool kMulti>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(const __grid_constant__ Params p, int depth) {
-    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
+    extern __shared__ int stack[];     // [stack entries][kTraceBlock]
     uint32_t n0 = p.batch.n_slots;
     if constexpr (kMulti) n0 = cur_batch(p).n_slots;
     const uint32_t n = depth == 0 ? n0 : p.wave.counters[cnt_ext(depth)];
     const uint32_t* q = p.wave.q[depth & 1];
-    const unsigned lane = threadIdx.x & 31u;
     uint32_t* cursor = &p.wave.counters[cur_ext(depth)];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.wave.stats[0], (unsigned long long)n);
+    bool busy = false, drained = false;
+    uint32_t slot = 0;
+    float tfar = 0.f;
+    const SceneDev* sc = &p.scene;
+    WRay r;
+    Trav st;
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(cursor, 32u);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= n) break;
-        const uint32_t idx = base + lane;
-        if (idx < n) {
-            const uint32_t slot = depth == 0 ? idx : q[idx];
-            const SceneDev* sc = &p.scene;
-            const FilmDev* film = &p.film;
-            if constexpr (kMulti) {
-                const SceneSlot& S = p.multi.scenes[seg_of_slot(cur_batch(p), slot).scene];
-                sc = &S.scene;
-                film = &S.film;
+        if (!drained && __any_sync(kFull, !busy)) {
+            const uint32_t idx = refill(busy, cursor, n, drained);
+            if (!busy && idx < n) {
+                slot = depth == 0 ? idx : q[idx];
+                const FilmDev* film = &p.film;
+                if constexpr (kMulti) {
+                    const SceneSlot& S = p.multi.scenes[seg_of_slot(cur_batch(p), slot).scene];
+                    sc = &S.scene;
+                    film = &S.film;
+                }
+                const float4 o = p.wave.ray_o[slot];
+                const float4 d = p.wave.ray_d[slot];
+                wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
+                // camera unwarp and the film components need the camera ray's closest surface
+                // at any distance (World::Li's record, World.h:749-766); shade still decides
+                // surface vs medium event by comparing with the sampled distance (o.w)
+                tfar = depth == 0 && (film->unwarp || film->comps) ? __int_as_float(0x7f800000) : o.w;
+                trav_init(st, tfar);
+                busy = true;
             }
-            const float4 o = p.wave.ray_o[slot];
-            const float4 d = p.wave.ray_d[slot];
-            WRay r;
-            wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
-            float t, u, v;
-            // camera unwarp and the film components need the camera ray's closest surface at any
-            // distance (World::Li's record, World.h:749-766); shade still
-            // decides surface vs medium event by comparing with the sampled distance (o.w)
-            const float tfar = depth == 0 && (film->unwarp || film->comps) ? __int_as_float(0x7f800000) : o.w;
-            const uint32_t id = traverse<false>(*sc, r, tfar, t, u, v, stack + threadIdx.x, kTraceBlock);
-            p.wave.hit[slot] = make_float4(t, __uint_as_float(id), u, v);
+        }
+        if (!__any_sync(kFull, busy)) break;
+        if (busy && trav_run<false>(*sc, r, st, stack + threadIdx.x, kTraceBlock, kTravBudget)) {
+            const float t = st.bid == kInvalid ? tfar : st.best;
+            p.wave.hit[slot] = make_float4(t, __uint_as_float(st.bid), st.bu, st.bv);
+            busy = false;
         }
     }
 }
 
+// Any hit of each queued shadow ray; a record for the unoccluded ones.  Same lane refill as
+// k_extend.
 template <bool kMulti>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(const __grid_constant__ Params p, int depth) {
-    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
+    extern __shared__ int stack[];     // [stack entries][kTraceBlock]
     const uint32_t n = p.wave.counters[cnt_sh(depth)];
-    const unsigned lane = threadIdx.x & 31u;
     uint32_t* cursor = &p.wave.counters[cur_sh(depth)];
     const size_t rs = p.wave.capacity;          // record stride: records are [bounce][slot]
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.wave.stats[1], (unsigned long long)n);
     unsigned long long splats = 0;
+    bool busy = false, drained = false;
+    uint32_t idx = 0;
+    const SceneDev* sc = &p.scene;
+    WRay r;
+    Trav st;
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(cursor, 32u);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= n) break;
-        const uint32_t idx = base + lane;
-        if (idx < n) {
-            const float4 o = p.wave.sh_o[idx];
-            const float4 d = p.wave.sh_d[idx];
-            const SceneDev* sc = &p.scene;
-            if constexpr (kMulti)
-                sc = &p.multi.scenes[seg_of_slot(cur_batch(p), __float_as_uint(p.wave.sh_L[idx].w)).scene].scene;
-            WRay r;
-            wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
-            float t, u, v;
-            const uint32_t id = traverse<true>(*sc, r, o.w, t, u, v, stack + threadIdx.x, kTraceBlock);
-            if (id == kInvalid) {
+        if (!drained && __any_sync(kFull, !busy)) {
+            const uint32_t k = refill(busy, cursor, n, drained);
+            if (!busy && k < n) {
+                idx = k;
+                const float4 o = p.wave.sh_o[idx];
+                const float4 d = p.wave.sh_d[idx];
+                if constexpr (kMulti)
+                    sc = &p.multi.scenes[seg_of_slot(cur_batch(p), __float_as_uint(p.wave.sh_L[idx].w)).scene].scene;
+                wray_setup(r, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), kSigmaVis);
+                trav_init(st, o.w);
+                busy = true;
+            }
+        }
+        if (!__any_sync(kFull, busy)) break;
+        if (busy && trav_run<true>(*sc, r, st, stack + threadIdx.x, kTraceBlock, kTravBudget)) {
+            if (st.bid == kInvalid) {
                 const float4 L = p.wave.sh_L[idx];
+                const float4 d = p.wave.sh_d[idx];
                 const uint32_t slot = __float_as_uint(L.w);
-                const uint32_t k = p.wave.rec_n[slot];
-                p.wave.rec[(size_t)k * rs + slot] = make_float4(L.x, L.y, L.z, d.w);
-                p.wave.rec_n[slot] = (uint8_t)(k + 1);
+                const uint32_t kk = p.wave.rec_n[slot];
+                p.wave.rec[(size_t)kk * rs + slot] = make_float4(L.x, L.y, L.z, d.w);
+                p.wave.rec_n[slot] = (uint8_t)(kk + 1);
                 ++splats;
             }
+            busy = false;
         }
     }
     if (splats) atomicAdd(&p.wave.stats[2], splats);
