@@ -27,8 +27,11 @@ sys.path.insert(0, ROOT)
 # B = 48 B ray in/out + 64 B per two-child node visit + 48 B per triangle test.
 B_CLOSEST = 48 + 64 * 19.397909840536915 + 48 * 8.579641797558255     # 1701.3 B
 B_SHADOW = 48 + 64 * 16.98375084460311 + 48 * 6.767252594318216       # 1459.8 B
-# DRAM bytes per extend launch from one ncu capture (scaled to a full launch), or None.
-TRAFFIC_PER_EXTEND_LAUNCH = None
+# DRAM bytes per closest-hit query of k_extend, from one ncu capture of all eight k_extend
+# launches of the 2M-path icosphere case (same 2^21-slot batches as this workload):
+# (425,001,984 B read + 36,808,704 B written) / 4,550,499 queries -- the BVH stays in L2, DRAM
+# carries the ray records.  Scaled to this workload's mean launch for roofline.traffic.
+DRAM_BYTES_PER_CLOSEST_QUERY = (425001984 + 36808704) / 4550499
 
 WORKLOAD = "icosphere"
 # throughput (value, paths/s) plus the "convergence" object: time to 5% rel-L2, guided vs plain
@@ -399,7 +402,10 @@ def main():
     roofline = {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)" if dom != "shadow_ms" else
                 "k_shadow (any-hit traversal)", "dominant_by_time": dom,
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": TRAFFIC_PER_EXTEND_LAUNCH,
+                "peak_source": peak_kind,
+                "traffic": (DRAM_BYTES_PER_CLOSEST_QUERY * closest / ext_launches) if ext_launches else None,
+                "traffic_unit": "bytes per k_extend launch (ncu DRAM read + write per query x queries per launch)",
+                "algorithmic_bytes_per_launch": (closest * B_CLOSEST / ext_launches) if ext_launches else None,
                 "algorithmic_bytes_per_query": algo_bytes,
                 "kernel_ms_per_step": {k: v / args.steps for k, v in kern.items()},
                 "queries_per_step": {"closest": closest / args.steps, "shadow": shadow / args.steps}}
