@@ -51,6 +51,8 @@ def parse():
                     help="skip the time-to-5%%-rel-L2 comparison of guided and plain sampling")
     ap.add_argument("--convergence-ref-spp", type=int, default=131072,
                     help="samples per pixel of each of the two halves of the converged reference")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="skip the sampling-mode throughputs (time sampling, light subpaths)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the 16-scene batched (CUDA-graph) throughput and accuracy leg")
     return ap.parse_args()
@@ -216,6 +218,48 @@ def convergence(args, device):
     if plain["seconds"] and guided["seconds"]:
         res["speedup_guided_vs_plain"] = plain["seconds"] / guided["seconds"]
     return res
+
+
+def modes(args, device, reps=2):
+    """Throughput of the sampling modes beside the plain path tracer, from the device time of
+    tr_render (one warm-up render, then `reps` timed ones): time sampling in the medium workload
+    (256x256, 4096 bins x 0.002, 128 spp x 2 incoming paths, depth 12, homogeneous medium) and,
+    on the icosphere workload (327,714 triangles, 512x512, 2048 bins, depth 8, 32 spp), time
+    sampling alone and with light subpaths + eye-light vertex connections."""
+    import jarabotransientrendering_b200 as T
+    from jarabotransientrendering_b200 import scenes as S
+    cases = [("medium_plain", S.medium, 0, None),
+             ("medium_time_sampling", S.medium, S.FLAG_TIME_SAMPLING, None),
+             ("icosphere_plain", S.icosphere, 0, 32),
+             ("icosphere_time_sampling", S.icosphere, S.FLAG_TIME_SAMPLING, 32),
+             ("icosphere_bidirectional", S.icosphere, S.FLAG_TIME_SAMPLING | S.FLAG_BIDIRECTIONAL, 32)]
+    out = {}
+    for name, make, flags, spp in cases:
+        sc = make()
+        sc.flags |= flags
+        spp = spp or sc.spp
+        paths = sc.width * sc.height * spp * sc.incoming_samples
+        with T.Context(sc, device=device) as c:
+            T._abi.check(T._abi.lib().tr_set_profiling(c.h, 1))
+            c.render(0, spp)
+            ms, kern = 0.0, {"extend_ms": 0.0, "shade_ms": 0.0, "shadow_ms": 0.0, "splat_ms": 0.0}
+            st0 = c.stats()
+            for r in range(reps):
+                c.render((r + 1) * spp, spp)
+                st = c.stats()
+                ms += st["render_ms"]
+                for k in kern:
+                    kern[k] += st[k] / reps
+            st1 = c.stats()
+        out[name] = {"paths_per_s": paths * reps / (ms / 1e3), "ms_per_render": ms / reps, "paths_per_render": paths,
+                     "closest_rays_per_path": (st1["closest_rays"] - st0["closest_rays"]) / (paths * reps),
+                     "shadow_rays_per_path": (st1["shadow_rays"] - st0["shadow_rays"]) / (paths * reps),
+                     "kernel_ms_per_render": kern,
+                     "scene": f"{sc.name} {sc.width}x{sc.height}, {sc.time_bins} bins, {spp} spp x "
+                              f"{sc.incoming_samples}, depth {sc.max_bounces}, flags {sc.flags}"}
+    out["note"] = ("shadow_ms includes the connection kernel (one any-hit ray per eye-light vertex pair, "
+                   "counted in shadow_rays) in bidirectional mode")
+    return out
 
 
 def batched(args, device, frames=2):
@@ -487,6 +531,11 @@ def main():
             out["batched"] = batched(args, local)
         except Exception as e:            # reported, not fatal: the throughput line stands
             out["batched"] = {"error": f"{type(e).__name__}: {e}"}
+    if rank == 0 and world == 1 and not args.no_modes:
+        try:
+            out["modes"] = modes(args, local)
+        except Exception as e:            # reported, not fatal: the throughput line stands
+            out["modes"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and not args.no_convergence:
         try:
             out["convergence"] = convergence(args, local)
