@@ -203,6 +203,13 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
         bd.nl = x->alloc<uint8_t>(capacity);
         bd.ne = x->alloc<uint8_t>(capacity);
         bd.L0 = x->alloc<float4>(capacity);
+        // connection queue of one eye depth (up to nvert rays per slot) and the record flags
+        drop(bd.co_o); drop(bd.co_d); drop(bd.co_L); drop(bd.valid);
+        bd.co_o = x->alloc<float4>(nv * capacity);
+        bd.co_d = x->alloc<float4>(nv * capacity);
+        bd.co_L = x->alloc<float4>(nv * capacity);
+        bd.ncand = x->integ.max_bounces * (std::max<uint32_t>(1u, x->integ.max_bounces) - 1u) / 2u;
+        bd.valid = x->alloc<uint8_t>(R * capacity);
     }
     if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
     if (!w.stats) {
@@ -380,8 +387,23 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 launches += 2;
             }
             if (bidir && x->bd.nvert) {
-                timed(3, [&] { return trk::launch_connect(p, x->connect_grid, strm); });
-                launches += 1;
+                // eye-light vertex connections, one eye depth at a time: rays with their samples
+                // into the connection queue, traced by k_shadow (records on blocked pairs),
+                // then compacted after the next-event records
+                const size_t R = (size_t)x->integ.max_bounces + x->bd.ncand;
+                TR_CUDA(cudaMemsetAsync(x->bd.valid, 0, R * x->wave.capacity, strm));
+                trk::Params pc = p;
+                pc.wave.sh_o = x->bd.co_o;
+                pc.wave.sh_d = x->bd.co_d;
+                pc.wave.sh_L = x->bd.co_L;
+                for (uint32_t ie = 0; ie < x->bd.nvert; ++ie) {
+                    timed(3, [&] { return trk::launch_connect_gen(p, (int)ie, strm); });
+                    const int dq = (int)(x->integ.max_bounces + ie);
+                    timed(3, [&] { return trk::launch_shadow(pc, dq, x->trace_grid, strm); });
+                }
+                timed(3, [&] { return trk::launch_connect_compact(p, strm); });
+                launches += 1 + 2ull * x->bd.nvert;
+                sh_l += x->bd.nvert;
             }
             timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm); });
             for (uint32_t b = 0; b < x->film.bounce_films; ++b)
@@ -643,7 +665,6 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         }
 
         x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);
-        if (it->flags & TR_FLAG_BIDIRECTIONAL) x->connect_grid = trk::connect_grid_size(device, x->bvh_depth);
         int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
         x->splat_g = std::max(1, std::min(g, 16));
         x->d_cursor = x->alloc<uint32_t>(1);

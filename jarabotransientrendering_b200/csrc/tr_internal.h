@@ -144,7 +144,6 @@ struct tr_ctx {
     trk::Wave lwave{};                      // light subpaths (TR_FLAG_BIDIRECTIONAL)
     trk::BidirWave bd{};
     uint32_t* d_lcounters = nullptr;
-    int connect_grid = 0;
     // film streaming (tr_render_film)
     cudaStream_t copy_stream = nullptr;
     float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows

@@ -317,9 +317,20 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(const _
         }
         if (!__any_sync(kFull, busy)) break;
         if (busy && trav_run<true>(*sc, r, st, stack + threadIdx.x, kTraceBlock, kTravBudget)) {
-            if (st.bid == kInvalid) {
+            const float4 d = p.wave.sh_d[idx];
+            const uint32_t dw = __float_as_uint(d.w);
+            if (dw & kConnRay) {
+                // eye-light vertex connection: the reference records it when the segment is
+                // blocked (World::intersects returns true on a hit); fixed record index
+                if (st.bid != kInvalid && !(dw & kConnNoRecord)) {
+                    const float4 L = p.wave.sh_L[idx];
+                    const uint32_t lw = __float_as_uint(L.w);
+                    const uint32_t slot = lw & 0xffffffu, kk = lw >> 24;
+                    p.wave.rec[(size_t)kk * rs + slot] = make_float4(L.x, L.y, L.z, __uint_as_float(dw & 0x1fffffffu));
+                    p.bd.valid[(size_t)kk * rs + slot] = 1;
+                }
+            } else if (st.bid == kInvalid) {
                 const float4 L = p.wave.sh_L[idx];
-                const float4 d = p.wave.sh_d[idx];
                 const uint32_t slot = __float_as_uint(L.w);
                 const uint32_t kk = p.wave.rec_n[slot];
                 p.wave.rec[(size_t)kk * rs + slot] = make_float4(L.x, L.y, L.z, d.w);
@@ -606,7 +617,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
                     }
                     if constexpr (kTimeSampling) {
                         // ---- bidirectional connections: keep the eye vertex (value, pdf,
-                        // delay) for k_connect (connect_paths, BidirectionalPathTracing.h:
+                        // delay) for the connection passes (connect_paths, BidirectionalPathTracing.h:
                         // 1018-1041); scenes without a medium, so every vertex is a surface ----
                         if ((flags & kFlagBidirectional) && surface && (uint32_t)depth + 2u <= max_bounces) {
                             const size_t cap = p.wave.capacity;
@@ -971,7 +982,9 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_user(Sce
 // point (as for time sampling); k_light_raygen emits the light subpath from it on the light
 // wave (its own rays, queues, counters and PCG32 stream); k_extend + k_light_shade walk it,
 // storing its vertices; the eye walk (k_extend / k_shade / k_shadow) stores the eye vertices
-// next to its next-event estimates; k_connect connects them and appends splat records.
+// next to its next-event estimates; per eye depth k_connect_gen queues the connection rays,
+// k_shadow traces them and records the pairs the reference connects, and k_connect_compact
+// appends those records after the slot's next-event records.
 // -----------------------------------------------------------------------------------------
 
 // slot -> (pixel, camera sample, incoming sample) of a single-scene batch
@@ -1197,74 +1210,124 @@ __device__ float mis_quantity(const Params& p, uint32_t slot, uint32_t t, uint32
     return (float)(1.0 / (double)iw);
 }
 
-// Eye-light vertex connections of one path slot per thread (transient connect_paths,
-// BidirectionalPathTracing.h:1018-1041; connect_vertices' shadow connection, :840-871): pairs
-// with ie + il + 2 <= max_bounces whose delays fit the film; the pair counts when
-// World::intersects reports a blocker between the two vertices (the query returns true on a
-// hit, World.h:617-639 / 693-697, and the reference connects on true); value
-// fe * (fv * (f_l * L0)) / w, time = distance + both delays, bounce ie + il + 1.  Records go
-// after the slot's next-event records, for k_splat.
-__global__ void __launch_bounds__(kTraceBlock, 4) k_connect(const __grid_constant__ Params p) {
-    extern __shared__ int stack[];     // [bvh depth + 1][kTraceBlock]
-    const SceneDev& sc = p.scene;
+// Eye-light vertex connections of eye depth ie (transient connect_paths,
+// BidirectionalPathTracing.h:1018-1041; connect_vertices' shadow connection, :840-871): for every
+// slot, the pairs (ie, il) with ie + il + 2 <= max_bounces whose delays fit the film each get a
+// connection ray from the light vertex to the eye vertex in the connection queue, with the
+// sample the pair contributes -- value fe * (fv * (f_l * L0)) / w, time = distance + both
+// delays, bounce ie + il + 1 -- and its fixed record index (after the slot's next-event
+// records, in (ie, il) order).  k_shadow then records the pairs whose segment is blocked (the
+// reference connects when World::intersects returns true, World.h:617-639 / 693-697).
+// One slot per thread; the warp appends its rays with one atomic.
+__global__ void __launch_bounds__(256) k_connect_gen(const __grid_constant__ Params p, int ie) {
     const FilmDev& film = p.film;
     const size_t cap = p.wave.capacity;
     const float total_time = (float)film.T * film.exposure + film.offset;
     const float inv_inc = 1.0f / (float)p.batch.ninc;
-    unsigned long long rays = 0, splats = 0;
-    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < p.batch.n_slots;
-         slot += gridDim.x * blockDim.x) {
-        const uint32_t ne = p.bd.ne[slot], nl = p.bd.nl[slot];
-        if (ne == 0 || nl == 0) continue;
-        const float4 L0 = p.bd.L0[slot];
-        const float cam_d = film.unwarp ? p.wave.cam_dist[slot] : 0.0f;
-        uint32_t k = p.wave.rec_n[slot];
-        for (uint32_t ie = 0; ie < ne; ++ie) {
-            const BVert E = load_vert(p.bd.evert, ie, cap, slot);
-            const float4 e_npdf = make_float4(E.n.x, E.n.y, E.n.z, E.pdf);
+    const uint32_t maxb = p.max_bounces;
+    const uint32_t uie = (uint32_t)ie;
+    const uint32_t off = uie * (maxb - 1u) - uie * (uie - 1u) / 2u;      // records of eye depths < ie
+    uint32_t* counter = &p.wave.counters[cnt_sh((int)maxb + ie)];
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < p.batch.n_slots; base += gridDim.x * blockDim.x) {
+        const uint32_t slot = base + threadIdx.x;
+        const bool have = slot < p.batch.n_slots && uie < p.bd.ne[slot] && p.bd.nl[slot] > 0;
+        uint32_t nl = 0;
+        BVert E;
+        if (have) {
+            nl = p.bd.nl[slot];
+            E = load_vert(p.bd.evert, uie, cap, slot);
+        }
+        // the pairs that get a ray (the reference's delay tests, :1020-1024 and :705-711)
+        auto traced = [&](uint32_t il, f3& l2e, float& dd) -> int {        // 1 ray, 0 skip, -1 stop
+            if (uie + il + 2u > maxb) return -1;
+            const float4 a = p.bd.lvert[(size_t)il * 4 * cap + slot];
+            if (E.time + a.w > total_time) return -1;
+            l2e = E.pos - mk(a.x, a.y, a.z);
+            dd = sqrtf(dot(l2e, l2e));
+            l2e = divs(l2e, dd);
+            return ((dd + E.time) + a.w > total_time) ? 0 : 1;
+        };
+        uint32_t cnt = 0;
+        if (have) {
             for (uint32_t il = 0; il < nl; ++il) {
-                if (ie + il + 2u > p.max_bounces) break;
-                const BVert Lv = load_vert(p.bd.lvert, il, cap, slot);
-                if (E.time + Lv.time > total_time) break;
-                f3 l2e = E.pos - Lv.pos;
-                const float dd = sqrtf(dot(l2e, l2e));
-                l2e = divs(l2e, dd);
-                if ((dd + E.time) + Lv.time > total_time) continue;
-                WRay r;
-                wray_setup(r, Lv.pos, l2e, kSigmaVis);
-                float th, tu, tv;
-                ++rays;
-                const uint32_t hid = traverse<true>(sc, r, dd - kSigmaVis, th, tu, tv, stack + threadIdx.x, kTraceBlock);
-                if (hid == kInvalid) continue;
-                float ce = -dot(l2e, E.n), cl = dot(l2e, Lv.n);
-                ce = ce > 0.0f ? ce : 0.0f;
-                cl = cl > 0.0f ? cl : 0.0f;
-                const f3 fe = mk((E.kd.x * kInvPi) * ce, (E.kd.y * kInvPi) * ce, (E.kd.z * kInvPi) * ce);
-                const f3 fl = mk((Lv.kd.x * kInvPi) * cl, (Lv.kd.y * kInvPi) * cl, (Lv.kd.z * kInvPi) * cl);
-                const float att = 1.0f / (dd * dd);
-                const f3 fv = mk((fe.x * fl.x) * att, (fe.y * fl.y) * att, (fe.z * fl.z) * att);
-                const float w = mis_quantity(p, slot, ie, il, E.pos, e_npdf, Lv.pos,
-                                             make_float4(Lv.n.x, Lv.n.y, Lv.n.z, Lv.pdf));
-                const float Lr = ((E.f.x * (fv.x * (Lv.f.x * L0.x))) / w) * inv_inc;
-                const float Lg = ((E.f.y * (fv.y * (Lv.f.y * L0.y))) / w) * inv_inc;
-                const float Lb = ((E.f.z * (fv.z * (Lv.f.z * L0.z))) / w) * inv_inc;
-                const float tt = dd + (E.time + Lv.time);
-                const float tc = film.unwarp ? tt - cam_d : tt;
-                const float ps = (tc - film.offset) / film.exposure;
-                const bool inside = ps < (float)film.T && ps >= 0.0f;
-                if (!(inside || film.nbounce)) continue;
-                const bool fin = finite3(Lr, Lg, Lb);
-                const uint32_t bin = inside ? (uint32_t)floorf(ps) : kBinOutside;
-                const uint32_t bounce = ie + il + 1u;
-                p.wave.rec[(size_t)k * cap + slot] = fin ? make_float4(Lr, Lg, Lb, __uint_as_float(bin | (bounce << 24)))
-                                                         : make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(bin | (bounce << 24)));
-                ++k;
-                ++splats;
+                f3 l2e; float dd;
+                const int t = traced(il, l2e, dd);
+                if (t < 0) break;
+                cnt += (uint32_t)t;
             }
         }
-        p.wave.rec_n[slot] = (uint8_t)k;
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= (unsigned)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        uint32_t wbase = 0;
+        if (lane == 0 && total) wbase = atomicAdd(counter, total);
+        wbase = __shfl_sync(kFull, wbase, 0);
+        if (!have || cnt == 0) continue;
+        uint32_t q = wbase + incl - cnt;
+        const uint32_t n0 = p.wave.rec_n[slot];
+        const float4 L0 = p.bd.L0[slot];
+        const float cam_d = film.unwarp ? p.wave.cam_dist[slot] : 0.0f;
+        const float4 e_npdf = make_float4(E.n.x, E.n.y, E.n.z, E.pdf);
+        for (uint32_t il = 0; il < nl; ++il) {
+            f3 l2e; float dd;
+            const int t = traced(il, l2e, dd);
+            if (t < 0) break;
+            if (t == 0) continue;
+            const BVert Lv = load_vert(p.bd.lvert, il, cap, slot);
+            float ce = -dot(l2e, E.n), cl = dot(l2e, Lv.n);
+            ce = ce > 0.0f ? ce : 0.0f;
+            cl = cl > 0.0f ? cl : 0.0f;
+            const f3 fe = mk((E.kd.x * kInvPi) * ce, (E.kd.y * kInvPi) * ce, (E.kd.z * kInvPi) * ce);
+            const f3 fl = mk((Lv.kd.x * kInvPi) * cl, (Lv.kd.y * kInvPi) * cl, (Lv.kd.z * kInvPi) * cl);
+            const float att = 1.0f / (dd * dd);
+            const f3 fv = mk((fe.x * fl.x) * att, (fe.y * fl.y) * att, (fe.z * fl.z) * att);
+            const float w = mis_quantity(p, slot, uie, il, E.pos, e_npdf, Lv.pos,
+                                         make_float4(Lv.n.x, Lv.n.y, Lv.n.z, Lv.pdf));
+            const float Lr = ((E.f.x * (fv.x * (Lv.f.x * L0.x))) / w) * inv_inc;
+            const float Lg = ((E.f.y * (fv.y * (Lv.f.y * L0.y))) / w) * inv_inc;
+            const float Lb = ((E.f.z * (fv.z * (Lv.f.z * L0.z))) / w) * inv_inc;
+            const float tt = dd + (E.time + Lv.time);
+            const float tc = film.unwarp ? tt - cam_d : tt;
+            const float ps = (tc - film.offset) / film.exposure;
+            const bool inside = ps < (float)film.T && ps >= 0.0f;
+            const bool fin = finite3(Lr, Lg, Lb);
+            const uint32_t bin = inside ? (uint32_t)floorf(ps) : kBinOutside;
+            const uint32_t bounce = uie + il + 1u;
+            uint32_t bw = bin | (bounce << 24) | kConnRay;
+            if (!(inside || film.nbounce)) bw |= kConnNoRecord;
+            const uint32_t k = n0 + off + il;
+            p.bd.co_o[q] = make_float4(Lv.pos.x, Lv.pos.y, Lv.pos.z, dd - kSigmaVis);
+            p.bd.co_d[q] = make_float4(l2e.x, l2e.y, l2e.z, __uint_as_float(bw));
+            p.bd.co_L[q] = fin ? make_float4(Lr, Lg, Lb, __uint_as_float(slot | (k << 24)))
+                               : make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(slot | (k << 24)));
+            ++q;
+        }
     }
-    if (rays) atomicAdd(&p.wave.stats[1], rays);
+}
+
+// After the connection passes: a slot's recorded connections moved, in (ie, il) order, right
+// after its next-event records, for k_splat.
+__global__ void __launch_bounds__(256) k_connect_compact(const __grid_constant__ Params p) {
+    const size_t cap = p.wave.capacity;
+    unsigned long long splats = 0;
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < p.batch.n_slots;
+         slot += gridDim.x * blockDim.x) {
+        const uint32_t n0 = p.wave.rec_n[slot];
+        uint32_t j = n0;
+        for (uint32_t c = 0; c < p.bd.ncand; ++c) {
+            const size_t k = (size_t)(n0 + c) * cap + slot;
+            if (!p.bd.valid[k]) continue;
+            if (j != n0 + c) p.wave.rec[(size_t)j * cap + slot] = p.wave.rec[k];
+            ++j;
+        }
+        splats += j - n0;
+        p.wave.rec_n[slot] = (uint8_t)j;
+    }
     if (splats) atomicAdd(&p.wave.stats[2], splats);
 }
 
@@ -1383,16 +1446,14 @@ cudaError_t launch_light_shade(const Params& pl, int depth, cudaStream_t s) {
     k_light_shade<<<std::max(1, grid), 256, 0, s>>>(pl, depth);
     return cudaGetLastError();
 }
-int connect_grid_size(int device, uint32_t bvh_depth) {
-    int sms = 0, per_sm = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_connect, kTraceBlock, trace_smem_bytes(bvh_depth));
-    return std::max(1, sms * std::max(1, per_sm));
+cudaError_t launch_connect_gen(const Params& p, int ie, cudaStream_t s) {
+    const uint32_t n = p.batch.n_slots;
+    k_connect_gen<<<std::max(1u, std::min(4096u, (n + 255) / 256)), 256, 0, s>>>(p, ie);
+    return cudaGetLastError();
 }
-cudaError_t launch_connect(const Params& p, int grid, cudaStream_t s) {
-    const uint32_t need = (p.batch.n_slots + kTraceBlock - 1) / kTraceBlock;
-    if ((uint32_t)grid > need) grid = (int)need;
-    k_connect<<<std::max(1, grid), kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p);
+cudaError_t launch_connect_compact(const Params& p, cudaStream_t s) {
+    const uint32_t n = p.batch.n_slots;
+    k_connect_compact<<<std::max(1u, std::min(4096u, (n + 255) / 256)), 256, 0, s>>>(p);
     return cudaGetLastError();
 }
 

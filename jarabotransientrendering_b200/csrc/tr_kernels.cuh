@@ -47,7 +47,18 @@ struct BidirWave {
     uint8_t* ne;              // eye vertices per slot
     float4* L0;               // light subpath value (emitted intensity, times cos for a rectangle)
     uint32_t nvert;           // vertices kept per subpath: max_bounces - 1
+    // connection rays of one eye depth (a shadow queue, up to nvert per slot): origin + tfar,
+    // direction + (bin | bounce << 24 | kConnRay | kConnNoRecord), contribution + (slot | record << 24)
+    float4* co_o;
+    float4* co_d;
+    float4* co_L;
+    uint8_t* valid;           // [record][slot]: 1 when the connection's record was written
+    uint32_t ncand;           // connection records a slot can have: max_bounces (max_bounces - 1) / 2
 };
+// flags in a shadow-queue entry's bin word: a connection ray (record when the segment is
+// blocked, at the record index carried with the slot), and one whose sample has no record
+constexpr uint32_t kConnRay = 1u << 31;
+constexpr uint32_t kConnNoRecord = 1u << 30;
 // state of the light subpath stream (another PCG32 state and increment than the eye walk's)
 constexpr unsigned long long kLightStateSalt = 0xD1B54A32D192ED03ULL;
 constexpr unsigned long long kLightSeqSalt = 0x3C6EF372FE94F82AULL;
@@ -220,8 +231,10 @@ cudaError_t launch_bounce_weights(const Params& p, cudaStream_t s);
 // queues and counters; target, stats and vertex arrays shared), then the connections
 cudaError_t launch_light_raygen(const Params& pl, cudaStream_t s);
 cudaError_t launch_light_shade(const Params& pl, int depth, cudaStream_t s);
-cudaError_t launch_connect(const Params& p, int grid, cudaStream_t s);
-int connect_grid_size(int device, uint32_t bvh_depth);      // resident k_connect blocks
+// connection rays of eye depth ie into the connection queue (counter cnt_sh(max_bounces + ie)),
+// then, after k_shadow has traced them, the slot's connection records compacted in order
+cudaError_t launch_connect_gen(const Params& p, int ie, cudaStream_t s);
+cudaError_t launch_connect_compact(const Params& p, cudaStream_t s);
 // FP64 film sums -> FP32 (film streaming)
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
