@@ -176,15 +176,19 @@ class GpuTransientRenderer : public TransientRenderer<D, Radiance, RadianceAtten
 public:
     // time_sampling: the reference's TransientRenderer(f_log, time_sampling) argument
     // (TransientRenderer.h:61-62, "-time-sampling"), i.e. TR_FLAG_TIME_SAMPLING.
+    // path_tracing_only: what the caller passed to BidirectionalPathTracing::set_path_tracing_only
+    // (BidirectionalPathTracing.h:214-217); false adds light subpaths and vertex connections
+    // (TR_FLAG_BIDIRECTIONAL, defined with time sampling in scenes without a medium).
     GpuTransientRenderer(FILE* f_log, const SceneCapture& scene, const tr_camera& camera, unsigned max_bounces,
                          unsigned sqrt_spp, unsigned incoming_samples, uint64_t seed, int device = 0,
-                         bool time_sampling = false)
+                         bool time_sampling = false, bool path_tracing_only = true)
         : Base(f_log, time_sampling), m_scene(scene), m_camera(camera), m_integrator{}, m_device(device) {
         m_integrator.max_bounces = max_bounces;
         m_integrator.sqrt_spp = sqrt_spp;
         m_integrator.incoming_samples = incoming_samples;
         m_integrator.seed = seed;
         if (time_sampling) m_integrator.flags |= TR_FLAG_TIME_SAMPLING;
+        if (!path_tracing_only) m_integrator.flags |= TR_FLAG_BIDIRECTIONAL;
     }
 
     void render(const char* name, World<D, Radiance>& world, Integrator<D, Radiance, RadianceAttenuation>* integrator,
