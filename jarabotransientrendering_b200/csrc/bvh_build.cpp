@@ -295,7 +295,7 @@ struct Builder {
 }  // namespace
 
 bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, uint32_t max_leaf,
-               BvhBuildResult& out, std::string* msg) {
+               BvhBuildResult& out, std::string* msg, bool write_tris) {
     auto t0 = std::chrono::steady_clock::now();
     if (nt == 0) { if (msg) *msg = "scene has no triangles"; return false; }
     if (nt >= (1u << 28)) { if (msg) *msg = "too many triangles"; return false; }
@@ -421,6 +421,8 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
     auto leaf_ref = [&](const Node& n, uint32_t toff) -> int32_t {
         for (uint32_t i = 0; i < n.count; ++i) {
             const uint32_t t = prim[n.first + i].id;
+            out.order[toff + i] = t;
+            if (!write_tris) continue;
             GpuTri& g = out.tris[toff + i];
             const uint32_t* ti = &tri[3 * (size_t)t];
             std::memcpy(g.v0, &v[3 * (size_t)ti[0]], 12);
@@ -489,7 +491,9 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
             if (j != spawned) flat(sub[j].n, sub[j].gi, sub[j].toff);
         if (spawned >= 0) { th.join(); fthreads.fetch_sub(1); }
     };
-    out.tris.resize(nt);
+    out.order.resize(nt);
+    if (write_tris) out.tris.resize(nt);
+    else out.tris.clear();
     if (root.left < 0) {
         // single-leaf scene: one node whose first child is the leaf
         out.nodes.assign(1, GpuNode{});

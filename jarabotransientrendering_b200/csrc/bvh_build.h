@@ -28,7 +28,8 @@ static_assert(sizeof(GpuTri) == 48, "triangle must be 48 bytes");
 
 struct BvhBuildResult {
     std::vector<GpuNode> nodes;
-    std::vector<GpuTri> tris;
+    std::vector<uint32_t> order;  // triangle ids in leaf order (leaf refs index this order)
+    std::vector<GpuTri> tris;     // the triangles in that order (only when write_tris)
     uint32_t depth = 0;          // four-child levels on the deepest path (root = 1)
     uint32_t stack = 0;          // traversal stack entries a ray can need: 3 per level
     uint32_t binary_depth = 0;   // depth of the binary SAH tree it was collapsed from
@@ -39,7 +40,9 @@ struct BvhBuildResult {
 // Binned SAH (32 bins over centroid bounds), leaves of at most `max_leaf` (<= 7) triangles,
 // collapsed to four-child nodes (each node opens its largest-area interior children).
 // vertices [nv][3], triangles [nt][3].  Returns false (with msg) on bad input.
+// write_tris = false leaves `tris` empty: the caller gathers the triangle records from `order`
+// (the CUDA path does it on the device).
 bool build_bvh(const float* vertices, uint32_t nv, const uint32_t* triangles, uint32_t nt,
-               uint32_t max_leaf, BvhBuildResult& out, std::string* msg);
+               uint32_t max_leaf, BvhBuildResult& out, std::string* msg, bool write_tris = true);
 
 }  // namespace trh

@@ -534,14 +534,31 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         x->cam = *c; x->film = *f; x->integ = *it;
         x->nt = s->num_triangles;
 
+        // the scene's own arrays go to the device first (from page-locked memory the copies
+        // overlap the BVH build)
+        const size_t ntri = s->num_triangles;
+        float* d_v = x->alloc<float>(3 * (size_t)s->num_vertices);
+        uint32_t* d_t = x->alloc<uint32_t>(3 * ntri);
+        uint32_t* d_m = x->alloc<uint32_t>(ntri);
+        uint32_t* d_o = x->alloc<uint32_t>(ntri);
+        TR_CUDA(cudaMemcpyAsync(d_v, s->vertices, sizeof(float) * 3 * (size_t)s->num_vertices,
+                                cudaMemcpyHostToDevice, x->stream));
+        TR_CUDA(cudaMemcpyAsync(d_t, s->triangles, sizeof(uint32_t) * 3 * ntri, cudaMemcpyHostToDevice, x->stream));
+        TR_CUDA(cudaMemcpyAsync(d_m, s->triangle_material, sizeof(uint32_t) * ntri, cudaMemcpyHostToDevice, x->stream));
+
         // BVH (replaces World::freeze -> rtcCommit)
         trh::BvhBuildResult bvh;
         std::string msg;
-        if (!trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg)) {
+        if (!trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg,
+                            /*write_tris*/ false)) {
+            cudaStreamSynchronize(x->stream);
+            x->release();
             delete x;
             return fail(TR_ERR_INVALID_ARGUMENT, msg);
         }
         if (bvh.stack > (uint32_t)trk::kStack) {
+            cudaStreamSynchronize(x->stream);
+            x->release();
             delete x;
             return fail(TR_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
         }
@@ -551,25 +568,13 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         x->bvh_ms = bvh.build_ms;
         x->d_nodes = x->alloc<float4>(bvh.nodes.size() * 8);
         upload(x->d_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode), x->stream);
-        x->d_tris = x->alloc<float4>(bvh.tris.size() * 3);
-        upload(x->d_tris, bvh.tris.data(), bvh.tris.size() * sizeof(trh::GpuTri), x->stream);
-
-        // per-triangle reference geometric normal normalize(cross(p2-p0, p1-p0)) (World.h:449)
-        std::vector<float4> ng(s->num_triangles);
-        for (uint32_t t = 0; t < s->num_triangles; ++t) {
-            const uint32_t* tri = &s->triangles[3 * (size_t)t];
-            const float* a = &s->vertices[3 * (size_t)tri[0]];
-            const float* b = &s->vertices[3 * (size_t)tri[1]];
-            const float* cc = &s->vertices[3 * (size_t)tri[2]];
-            trd::f3 p0 = trd::mk(a[0], a[1], a[2]), p1 = trd::mk(b[0], b[1], b[2]), p2 = trd::mk(cc[0], cc[1], cc[2]);
-            trd::f3 n = trd::normalize(trd::cross(p2 - p0, p1 - p0));
-            uint32_t mi = s->triangle_material[t];
-            float mf;
-            std::memcpy(&mf, &mi, 4);
-            ng[t] = make_float4(n.x, n.y, n.z, mf);
-        }
-        x->d_tri_ng = x->alloc<float4>(ng.size());
-        upload(x->d_tri_ng, ng.data(), ng.size() * sizeof(float4), x->stream);
+        // the leaf-ordered triangle records and the per-triangle normals, built on the device
+        // (World.h:449 normals, the same IEEE operations as a host evaluation)
+        TR_CUDA(cudaMemcpyAsync(d_o, bvh.order.data(), sizeof(uint32_t) * ntri, cudaMemcpyHostToDevice, x->stream));
+        x->d_tris = x->alloc<float4>(ntri * 3);
+        x->d_tri_ng = x->alloc<float4>(ntri);
+        TR_CUDA(trk::launch_build_tris(d_v, d_t, d_m, d_o, (uint32_t)ntri, x->d_tris, x->d_tri_ng, x->stream));
+        TR_CUDA(cudaStreamSynchronize(x->stream));      // bvh.order is released on return
 
         std::vector<float4> mats(s->num_materials), mats2(s->num_materials);
         for (uint32_t i = 0; i < s->num_materials; ++i) {

@@ -1457,6 +1457,29 @@ cudaError_t launch_connect_compact(const Params& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+__global__ void __launch_bounds__(256) k_build_tris(const float* __restrict__ v, const uint32_t* __restrict__ t,
+                                                    const uint32_t* __restrict__ mat, const uint32_t* __restrict__ order,
+                                                    uint32_t nt, float4* __restrict__ tris, float4* __restrict__ tri_ng) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+        const uint32_t id = order[i];
+        const uint32_t a = t[3 * (size_t)id], b = t[3 * (size_t)id + 1], c = t[3 * (size_t)id + 2];
+        const f3 p0 = mk(v[3 * (size_t)a], v[3 * (size_t)a + 1], v[3 * (size_t)a + 2]);
+        const f3 p1 = mk(v[3 * (size_t)b], v[3 * (size_t)b + 1], v[3 * (size_t)b + 2]);
+        const f3 p2 = mk(v[3 * (size_t)c], v[3 * (size_t)c + 1], v[3 * (size_t)c + 2]);
+        tris[3 * (size_t)i] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(id));
+        tris[3 * (size_t)i + 1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
+        tris[3 * (size_t)i + 2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
+        const f3 n = normalize(cross(p2 - p0, p1 - p0));
+        tri_ng[id] = make_float4(n.x, n.y, n.z, __uint_as_float(mat[id]));
+    }
+}
+cudaError_t launch_build_tris(const float* vertices, const uint32_t* triangles, const uint32_t* material,
+                              const uint32_t* order, uint32_t nt, float4* tris, float4* tri_ng, cudaStream_t s) {
+    k_build_tris<<<std::max(1u, std::min(8192u, (nt + 255) / 256)), 256, 0, s>>>(vertices, triangles, material,
+                                                                                   order, nt, tris, tri_ng);
+    return cudaGetLastError();
+}
+
 // FP64 film sums to FP32 (round to nearest); grid-stride, streaming loads
 __global__ void __launch_bounds__(256) k_to_f32(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)

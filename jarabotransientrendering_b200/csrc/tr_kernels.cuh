@@ -235,6 +235,11 @@ cudaError_t launch_light_shade(const Params& pl, int depth, cudaStream_t s);
 // then, after k_shadow has traced them, the slot's connection records compacted in order
 cudaError_t launch_connect_gen(const Params& p, int ie, cudaStream_t s);
 cudaError_t launch_connect_compact(const Params& p, cudaStream_t s);
+// Scene set-up on the device: the leaf-ordered triangle records (v0 + id, v1, v2) from the
+// builder's order, and per triangle id the reference geometric normal
+// normalize(cross(p2 - p0, p1 - p0)) (World.h:449) with the material index.
+cudaError_t launch_build_tris(const float* vertices, const uint32_t* triangles, const uint32_t* material,
+                              const uint32_t* order, uint32_t nt, float4* tris, float4* tri_ng, cudaStream_t s);
 // FP64 film sums -> FP32 (film streaming)
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
 cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
