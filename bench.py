@@ -157,6 +157,22 @@ def cpu_reference(scene, rows_per_proc, procs):
                       f"render loop time of the slowest process"}
 
 
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest of a per-rank number over all ranks: the job takes as long as its slowest
+    rank (every rank must call it, in the same order)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, seconds):
+    """Whole-job throughput: the units every rank processed over the slowest rank's time."""
+    return units_per_rank * world / seconds
+
+
 def run_reference(args, rank, world):
     from jarabotransientrendering_b200 import scenes as S
     if rank != 0:
@@ -427,12 +443,8 @@ def main():
     st1 = ctx.stats()
     closest = st1["closest_rays"] - st0["closest_rays"]
     shadow = st1["shadow_rays"] - st0["shadow_rays"]
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    total_paths = paths_per_step * args.steps * world
-    value = total_paths / (ms / 1e3)
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = whole_job_rate(paths_per_step * args.steps, world, ms / 1e3)
 
     # roofline of the dominant kernel (largest device time)
     peak, peak_kind = peaks()
@@ -509,13 +521,15 @@ def main():
         et64, ph64 = e2e_run(f64, 1)
         d2h64 = sum(a.nbytes for a in f64)
         del f64
-        out["e2e"] = {"value": paths_per_step * world / et, "unit": "paths/s",
+        et = max_over_ranks(et, dist, "cuda")
+        et64 = max_over_ranks(et64, dist, "cuda")
+        out["e2e"] = {"value": whole_job_rate(paths_per_step, world, et), "unit": "paths/s",
                       "h2d_bytes_per_step": int(pv.nbytes + pt.nbytes + pm.nbytes),
                       "d2h_bytes_per_step": int(d2h),
                       "ms_per_step": et * 1e3,
                       "film": "FP32 sums (the reference's film precision)",
                       "phases_per_step": ph,
-                      "fp64_film": {"value": paths_per_step * world / et64, "d2h_bytes_per_step": int(d2h64),
+                      "fp64_film": {"value": whole_job_rate(paths_per_step, world, et64), "d2h_bytes_per_step": int(d2h64),
                                     "ms_per_step": et64 * 1e3, "phases": ph64},
                       "includes": "tr_create (scene H2D from pinned memory + host BVH build + film alloc), "
                                   "tr_render_film (render with the film streamed into pinned host memory as "
