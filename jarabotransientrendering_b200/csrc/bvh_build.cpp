@@ -33,12 +33,17 @@ struct Box {
     }
 };
 
-struct Node {                         // filled by Builder::build (no initialisers: the array is
-    Box box;                          // allocated for 2 nt nodes and only the used ones are written)
-    int32_t left, right;
-    uint32_t first, count;
-    uint32_t n_inner, n_tris;         // interior nodes and triangles in the subtree
-};
+// Builder::build fills BinNodes (no initialisers: the array is allocated for all node slots and
+// only the used ones are written).
+using Node = BinNode;
+inline Box box_of(const BinNode& n) {
+    Box b;
+    for (int k = 0; k < 3; ++k) { b.lo[k] = n.lo[k]; b.hi[k] = n.hi[k]; }
+    return b;
+}
+inline void set_box(BinNode& n, const Box& b) {
+    for (int k = 0; k < 3; ++k) { n.lo[k] = b.lo[k]; n.hi[k] = b.hi[k]; }
+}
 
 constexpr int kBins = 32;
 
@@ -195,10 +200,10 @@ struct Builder {
         }
         const Box& nb = B.nb;
         const Box& cb = B.cb;
-        nd.box = nb;
+        set_box(nd, nb);
         auto make_leaf = [&]() {
             nd.first = first; nd.count = count;
-            nd.n_inner = 0; nd.n_tris = count;
+            nd.n_tris = count;
             return me;
         };
         // SAH leaf test: keep as a leaf when small enough
@@ -286,7 +291,6 @@ struct Builder {
             r = (int32_t)build(mid, first + count - mid, d + 1, sl, rb, rc2);
         }
         nd.left = l; nd.right = r; nd.count = 0;
-        nd.n_inner = 1 + nodes[l].n_inner + nodes[r].n_inner;
         nd.n_tris = nodes[l].n_tris + nodes[r].n_tris;
         return me;
     }
@@ -359,32 +363,40 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
     B.max_threads = hw;
     B.build(0, nt, 0);
 
-    // Collapse to four-child nodes: a node starts with its binary children and repeatedly
-    // opens the interior child of largest surface area (the first on ties) while it has fewer
-    // than four.  Pass 1 records each four-child node's binary children and its subtree's
-    // node count and depth; pass 2 writes every subtree at its own offsets (depth-first
-    // preorder, children in left-to-right order, leaf triangles in the same order), large
-    // subtrees on their own threads.
-    const Node& root = B.nodes[0];
-    const size_t cap = Builder::capacity(nt);
+    std::vector<uint32_t> ids(nt);
+    parallel_for(nt, [&](uint32_t a, uint32_t b) { for (uint32_t i = a; i < b; ++i) ids[i] = prim[i].id; });
+    const bool ok = finish_bvh(B.nodes.get(), Builder::capacity(nt), ids.data(), nt, B.depth.load(), v, tri, write_tris, out);
+    out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return ok;
+}
+
+// Collapse to four-child nodes: a node starts with its binary children and repeatedly opens the
+// interior child of largest surface area (the first on ties) while it has fewer than four.
+// Pass 1 records each four-child node's binary children and its subtree's node count and depth;
+// pass 2 writes every subtree at its own offsets (depth-first preorder, children in left-to-right
+// order, leaf triangles in the same order), large subtrees on their own threads.
+bool finish_bvh(const BinNode* nodes, size_t cap, const uint32_t* ids, uint32_t nt, uint32_t binary_depth,
+                const float* v, const uint32_t* tri, bool write_tris, BvhBuildResult& out) {
+    const int hw = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const Node& root = nodes[0];
     std::unique_ptr<std::array<int32_t, 4>[]> kids(new std::array<int32_t, 4>[cap]);
     std::unique_ptr<uint32_t[]> n4(new uint32_t[cap]);
     std::unique_ptr<uint32_t[]> d4(new uint32_t[cap]);
     std::atomic<int> cthreads{1};
     std::function<void(int32_t)> collapse = [&](int32_t n) {
-        int32_t c[4] = {B.nodes[n].left, B.nodes[n].right, -1, -1};
+        int32_t c[4] = {nodes[n].left, nodes[n].right, -1, -1};
         int k = 2;
         while (k < 4) {
             int best = -1;
             float ba = -1.0f;
             for (int j = 0; j < k; ++j) {
-                const Node& q = B.nodes[c[j]];
+                const Node& q = nodes[c[j]];
                 if (q.left < 0) continue;
-                const float a = q.box.area();
+                const float a = box_of(q).area();
                 if (a > ba) { ba = a; best = j; }
             }
             if (best < 0) break;
-            const Node& q = B.nodes[c[best]];
+            const Node& q = nodes[c[best]];
             for (int j = k; j > best + 1; --j) c[j] = c[j - 1];
             c[best] = q.left;
             c[best + 1] = q.right;
@@ -395,17 +407,17 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
         int32_t sub[4];
         int ns = 0;
         for (int j = 0; j < 4; ++j)
-            if (c[j] >= 0 && B.nodes[c[j]].left >= 0) sub[ns++] = c[j];
+            if (c[j] >= 0 && nodes[c[j]].left >= 0) sub[ns++] = c[j];
         std::thread th;
         int spawned = -1;
         if (ns > 1) {
             int big = 0;
             for (int j = 1; j < ns; ++j)
-                if (B.nodes[sub[j]].n_tris > B.nodes[sub[big]].n_tris) big = j;
-            if (B.nodes[sub[big]].n_tris > kParallelCutoff && cthreads.fetch_add(1) < hw) {
+                if (nodes[sub[j]].n_tris > nodes[sub[big]].n_tris) big = j;
+            if (nodes[sub[big]].n_tris > kParallelCutoff && cthreads.fetch_add(1) < hw) {
                 spawned = big;
                 th = std::thread([&, s0 = sub[big]] { collapse(s0); });
-            } else if (B.nodes[sub[big]].n_tris > kParallelCutoff) {
+            } else if (nodes[sub[big]].n_tris > kParallelCutoff) {
                 cthreads.fetch_sub(1);
             }
         }
@@ -420,7 +432,7 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
     std::atomic<uint32_t> leaves{0};
     auto leaf_ref = [&](const Node& n, uint32_t toff) -> int32_t {
         for (uint32_t i = 0; i < n.count; ++i) {
-            const uint32_t t = prim[n.first + i].id;
+            const uint32_t t = ids[n.first + i];
             out.order[toff + i] = t;
             if (!write_tris) continue;
             GpuTri& g = out.tris[toff + i];
@@ -463,8 +475,8 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
         for (int j = 0; j < 4; ++j) {
             const int32_t c = kids[n][j];
             if (c < 0) { empty_slot(g, j); continue; }
-            const Node& q = B.nodes[c];
-            write_box(g, j, q.box);
+            const Node& q = nodes[c];
+            write_box(g, j, box_of(q));
             if (q.left >= 0) {
                 g.child[j] = (int32_t)gnext;
                 sub[ns++] = {c, gnext, t};
@@ -479,11 +491,11 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
         if (ns > 1) {
             int big = 0;
             for (int j = 1; j < ns; ++j)
-                if (B.nodes[sub[j].n].n_tris > B.nodes[sub[big].n].n_tris) big = j;
-            if (B.nodes[sub[big].n].n_tris > kParallelCutoff && fthreads.fetch_add(1) < hw) {
+                if (nodes[sub[j].n].n_tris > nodes[sub[big].n].n_tris) big = j;
+            if (nodes[sub[big].n].n_tris > kParallelCutoff && fthreads.fetch_add(1) < hw) {
                 spawned = big;
                 th = std::thread([&, sb = sub[big]] { flat(sb.n, sb.gi, sb.toff); });
-            } else if (B.nodes[sub[big].n].n_tris > kParallelCutoff) {
+            } else if (nodes[sub[big].n].n_tris > kParallelCutoff) {
                 fthreads.fetch_sub(1);
             }
         }
@@ -497,7 +509,7 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
     if (root.left < 0) {
         // single-leaf scene: one node whose first child is the leaf
         out.nodes.assign(1, GpuNode{});
-        write_box(out.nodes[0], 0, root.box);
+        write_box(out.nodes[0], 0, box_of(root));
         out.nodes[0].child[0] = leaf_ref(root, 0);
         for (int j = 1; j < 4; ++j) empty_slot(out.nodes[0], j);
         out.depth = 1;
@@ -508,9 +520,8 @@ bool build_bvh(const float* v, uint32_t nv, const uint32_t* tri, uint32_t nt, ui
         out.depth = d4[0];
     }
     out.stack = 3 * out.depth + 1;
-    out.binary_depth = B.depth.load();
+    out.binary_depth = binary_depth;
     out.leaves = leaves.load();
-    out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return true;
 }
 

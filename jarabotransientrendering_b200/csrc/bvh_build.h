@@ -26,6 +26,14 @@ struct alignas(16) GpuTri {
 };
 static_assert(sizeof(GpuTri) == 48, "triangle must be 48 bytes");
 
+// Binary SAH tree node (output of the binned builders, input of the four-child collapse).
+struct BinNode {
+    float lo[3], hi[3];          // bounds of the node's triangles
+    int32_t left, right;         // children; left < 0: leaf
+    uint32_t first, count;       // leaf: its triangles, [first, first + count) of the id order
+    uint32_t n_tris;             // triangles in the subtree
+};
+
 struct BvhBuildResult {
     std::vector<GpuNode> nodes;
     std::vector<uint32_t> order;  // triangle ids in leaf order (leaf refs index this order)
@@ -44,5 +52,11 @@ struct BvhBuildResult {
 // (the CUDA path does it on the device).
 bool build_bvh(const float* vertices, uint32_t nv, const uint32_t* triangles, uint32_t nt,
                uint32_t max_leaf, BvhBuildResult& out, std::string* msg, bool write_tris = true);
+
+// Collapses a binary tree (root at index 0 of nodes[0, cap), leaves indexing `ids`, the triangle
+// ids in leaf order) to four-child nodes and fills out (nodes, order, stack, depths; tris when
+// write_tris).  Shared by the host builder and the device builder.
+bool finish_bvh(const BinNode* nodes, size_t cap, const uint32_t* ids, uint32_t nt, uint32_t binary_depth,
+                const float* vertices, const uint32_t* triangles, bool write_tris, BvhBuildResult& out);
 
 }  // namespace trh

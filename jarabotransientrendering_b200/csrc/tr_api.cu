@@ -534,8 +534,46 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         x->cam = *c; x->film = *f; x->integ = *it;
         x->nt = s->num_triangles;
 
-        // the scene's own arrays go to the device first (from page-locked memory the copies
-        // overlap the BVH build)
+        // film: [H][W][T][3] + steady + weights, double precision, zeroed.  Allocated first, so
+        // the largest block is taken from the memory pool before any scratch (a film freed by an
+        // earlier context is reused whole instead of mapped again)
+        const size_t nstreak = (size_t)f->width * f->height * f->time_bins * 3u;
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        free_b += tri::pool_idle_bytes(device);      // kept by the pool for reuse
+        const size_t nb = f->bounce_films;
+        if ((1 + nb) * nstreak * sizeof(double) + ((size_t)2 << 30) > free_b) {
+            x->release();
+            delete x;
+            return fail(TR_ERR_OUT_OF_MEMORY, "streak film of " + std::to_string(nstreak * 8 >> 20) +
+                                                  " MiB does not fit in free device memory");
+        }
+        x->d_streak = x->alloc<double>(nstreak);
+        x->d_steady = x->alloc<double>((size_t)f->width * f->height * 3u);
+        x->d_weight = x->alloc<double>((size_t)f->width * f->height);
+        TR_CUDA(cudaMemsetAsync(x->d_streak, 0, nstreak * sizeof(double), x->stream));
+        TR_CUDA(cudaMemsetAsync(x->d_steady, 0, (size_t)f->width * f->height * 3u * sizeof(double), x->stream));
+        TR_CUDA(cudaMemsetAsync(x->d_weight, 0, (size_t)f->width * f->height * sizeof(double), x->stream));
+        if (nb) {
+            const size_t npix = (size_t)f->width * f->height;
+            x->d_bstreak = x->alloc<double>(nb * nstreak);
+            x->d_bsteady = x->alloc<double>(nb * npix * 3u);
+            x->d_bweight = x->alloc<double>(nb * npix);
+            TR_CUDA(cudaMemsetAsync(x->d_bstreak, 0, nb * nstreak * sizeof(double), x->stream));
+            TR_CUDA(cudaMemsetAsync(x->d_bsteady, 0, nb * npix * 3u * sizeof(double), x->stream));
+            TR_CUDA(cudaMemsetAsync(x->d_bweight, 0, nb * npix * sizeof(double), x->stream));
+        }
+        {
+            const size_t npix = (size_t)f->width * f->height;
+            if (f->components & TR_COMP_DEPTH) x->d_cdepth = x->alloc<double>(npix);
+            if (f->components & TR_COMP_POSITIONS) x->d_cpos = x->alloc<double>(npix * 3u);
+            if (f->components & TR_COMP_NORMALS) x->d_cnorm = x->alloc<double>(npix * 3u);
+            if (x->d_cdepth) TR_CUDA(cudaMemsetAsync(x->d_cdepth, 0, npix * sizeof(double), x->stream));
+            if (x->d_cpos) TR_CUDA(cudaMemsetAsync(x->d_cpos, 0, npix * 3u * sizeof(double), x->stream));
+            if (x->d_cnorm) TR_CUDA(cudaMemsetAsync(x->d_cnorm, 0, npix * 3u * sizeof(double), x->stream));
+        }
+
+        // the scene's own arrays go to the device first (the BVH is built there from them)
         const size_t ntri = s->num_triangles;
         float* d_v = x->alloc<float>(3 * (size_t)s->num_vertices);
         uint32_t* d_t = x->alloc<uint32_t>(3 * ntri);
@@ -546,10 +584,12 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         TR_CUDA(cudaMemcpyAsync(d_t, s->triangles, sizeof(uint32_t) * 3 * ntri, cudaMemcpyHostToDevice, x->stream));
         TR_CUDA(cudaMemcpyAsync(d_m, s->triangle_material, sizeof(uint32_t) * ntri, cudaMemcpyHostToDevice, x->stream));
 
-        // BVH (replaces World::freeze -> rtcCommit)
+        // BVH (replaces World::freeze -> rtcCommit): built on the device from the uploaded arrays;
+        // on invalid input the host builder names the offending index or vertex
         trh::BvhBuildResult bvh;
         std::string msg;
-        if (!trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg,
+        if (!trh::build_bvh_device(d_v, s->num_vertices, d_t, s->num_triangles, 4, x->stream, bvh) &&
+            !trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg,
                             /*write_tris*/ false)) {
             cudaStreamSynchronize(x->stream);
             x->release();
@@ -630,43 +670,6 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             // duration (BidirectionalPathTracing.h:189-206, :240-307)
             if (it->flags & TR_FLAG_TIME_SAMPLING) sc.lambda = 4.0f / ((float)f->time_bins * f->exposure);
             sc.g = s->medium.g;
-        }
-
-        // film: [H][W][T][3] + steady + weights, double precision, zeroed
-        const size_t nstreak = (size_t)f->width * f->height * f->time_bins * 3u;
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
-        free_b += tri::pool_idle_bytes(device);      // kept by the pool for reuse
-        const size_t nb = f->bounce_films;
-        if ((1 + nb) * nstreak * sizeof(double) + ((size_t)2 << 30) > free_b) {
-            x->release();
-            delete x;
-            return fail(TR_ERR_OUT_OF_MEMORY, "streak film of " + std::to_string(nstreak * 8 >> 20) +
-                                                  " MiB does not fit in free device memory");
-        }
-        x->d_streak = x->alloc<double>(nstreak);
-        x->d_steady = x->alloc<double>((size_t)f->width * f->height * 3u);
-        x->d_weight = x->alloc<double>((size_t)f->width * f->height);
-        TR_CUDA(cudaMemsetAsync(x->d_streak, 0, nstreak * sizeof(double), x->stream));
-        TR_CUDA(cudaMemsetAsync(x->d_steady, 0, (size_t)f->width * f->height * 3u * sizeof(double), x->stream));
-        TR_CUDA(cudaMemsetAsync(x->d_weight, 0, (size_t)f->width * f->height * sizeof(double), x->stream));
-        if (nb) {
-            const size_t npix = (size_t)f->width * f->height;
-            x->d_bstreak = x->alloc<double>(nb * nstreak);
-            x->d_bsteady = x->alloc<double>(nb * npix * 3u);
-            x->d_bweight = x->alloc<double>(nb * npix);
-            TR_CUDA(cudaMemsetAsync(x->d_bstreak, 0, nb * nstreak * sizeof(double), x->stream));
-            TR_CUDA(cudaMemsetAsync(x->d_bsteady, 0, nb * npix * 3u * sizeof(double), x->stream));
-            TR_CUDA(cudaMemsetAsync(x->d_bweight, 0, nb * npix * sizeof(double), x->stream));
-        }
-        {
-            const size_t npix = (size_t)f->width * f->height;
-            if (f->components & TR_COMP_DEPTH) x->d_cdepth = x->alloc<double>(npix);
-            if (f->components & TR_COMP_POSITIONS) x->d_cpos = x->alloc<double>(npix * 3u);
-            if (f->components & TR_COMP_NORMALS) x->d_cnorm = x->alloc<double>(npix * 3u);
-            if (x->d_cdepth) TR_CUDA(cudaMemsetAsync(x->d_cdepth, 0, npix * sizeof(double), x->stream));
-            if (x->d_cpos) TR_CUDA(cudaMemsetAsync(x->d_cpos, 0, npix * 3u * sizeof(double), x->stream));
-            if (x->d_cnorm) TR_CUDA(cudaMemsetAsync(x->d_cnorm, 0, npix * 3u * sizeof(double), x->stream));
         }
 
         x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);

@@ -209,3 +209,12 @@ tr_status train_on_pool(tr_guide* g, const trk::GuideWave& gw, const uint32_t* p
                         float lr, cudaStream_t s, tr_stats& stats);
 
 }  // namespace tri
+
+namespace trh {
+struct BvhBuildResult;
+// Binned-SAH build on the device (bvh_gpu.cu) from device-resident vertices [nv][3] and
+// triangles [nt][3], collapsed to four-child nodes like build_bvh; false on invalid input (the
+// host builder then reports which index or vertex).
+bool build_bvh_device(const float* d_vertices, uint32_t nv, const uint32_t* d_triangles, uint32_t nt,
+                      uint32_t max_leaf, cudaStream_t s, BvhBuildResult& out);
+}  // namespace trh

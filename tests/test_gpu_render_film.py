@@ -117,3 +117,30 @@ def test_device_memory_is_kept_for_reuse_and_released_on_request(gpu):
     free3 = torch.cuda.mem_get_info()[0]
     assert free3 - free2 >= film_bytes
     assert _abi.lib().tr_release_cached_memory(99) == 1
+
+
+@pytest.mark.parametrize("workload", ["cornell", "icosphere"])
+def test_device_bvh_build_matches_the_host_builder(gpu, tmp_path, workload):
+    """tr_create builds the BVH on the device with the host builder's split rules: the same
+    four-child tree (node count and depth) as csrc/bvh_build.cpp on the same mesh."""
+    import json
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    csrc = os.path.join(root, "jarabotransientrendering_b200", "csrc")
+    exe = tmp_path / "bvh_check"
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-pthread", "-ffp-contract=off", f"-I{csrc}",
+                           os.path.join(root, "tests", "bvh_check.cpp"), os.path.join(csrc, "bvh_build.cpp"),
+                           "-o", str(exe)])
+    sc = S.WORKLOADS[workload]()
+    v, t, _ = sc.flatten()
+    raw = tmp_path / "mesh.bin"
+    with open(raw, "wb") as fh:
+        fh.write(np.array([len(v), len(t)], np.uint32).tobytes())
+        fh.write(v.tobytes())
+        fh.write(t.tobytes())
+    host = json.loads(subprocess.run([str(exe), str(raw)], capture_output=True, text=True, check=True).stdout)
+    small = S.WORKLOADS[workload](width=8, height=8, time_bins=16)
+    with gpu.Context(small) as c:
+        st = c.stats()
+    assert st["bvh_nodes"] == host["nodes"] and st["bvh_depth"] == host["depth"], (st, host)
