@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -394,6 +395,101 @@ __global__ void k_small(Dev d, int cur, uint32_t ns) {
     atomicMax(&d.counters[3], maxd);
 }
 
+// ---- four-child collapse on the device (the rules of finish_bvh in bvh_build.cpp) ----
+
+// each four-child root of this level picks its children: start from the binary children and
+// open the interior child of largest area (the first on ties) while fewer than four; interior
+// children become the next level's roots
+__global__ void k_collapse(const BinNode* __restrict__ nodes, uint32_t* q, uint32_t lo, uint32_t n,
+                           uint32_t* next, int4* kids) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t nd = q[lo + i];
+    int32_t c[4] = {nodes[nd].left, nodes[nd].right, -1, -1};
+    int k = 2;
+    while (k < 4) {
+        int best = -1;
+        float ba = -1.0f;
+        for (int j = 0; j < k; ++j) {
+            const BinNode& b = nodes[c[j]];
+            if (b.left < 0) continue;
+            const float a = area(b.lo, b.hi);
+            if (a > ba) { ba = a; best = j; }
+        }
+        if (best < 0) break;
+        const BinNode& b = nodes[c[best]];
+        for (int j = k; j > best + 1; --j) c[j] = c[j - 1];
+        c[best] = b.left;
+        c[best + 1] = b.right;
+        ++k;
+    }
+    kids[nd] = make_int4(c[0], c[1], c[2], c[3]);
+    for (int j = 0; j < 4; ++j)
+        if (c[j] >= 0 && nodes[c[j]].left >= 0) q[atomicAdd(next, 1u)] = (uint32_t)c[j];
+}
+
+// four-child nodes in each subtree (deepest level first)
+__global__ void k_count4(const BinNode* __restrict__ nodes, const uint32_t* q, uint32_t lo, uint32_t n,
+                         const int4* kids, uint32_t* n4) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t nd = q[lo + i];
+    const int4 c4 = kids[nd];
+    const int32_t c[4] = {c4.x, c4.y, c4.z, c4.w};
+    uint32_t cnt = 1;
+    for (int j = 0; j < 4; ++j)
+        if (c[j] >= 0 && nodes[c[j]].left >= 0) cnt += n4[c[j]];
+    n4[nd] = cnt;
+}
+
+// the node at its depth-first preorder index (children in order, leaf triangles in the same
+// order; boxes one ulp outward), its children's indices and triangle offsets for the next level
+__global__ void k_place4(const BinNode* __restrict__ nodes, const uint32_t* __restrict__ ids, const uint32_t* q,
+                         uint32_t lo, uint32_t n, const int4* kids, const uint32_t* n4, uint32_t* gidx, uint32_t* toff,
+                         GpuNode* out, uint32_t* order, uint32_t* leaves) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t nd = q[lo + i];
+    const int4 c4 = kids[nd];
+    const int32_t c[4] = {c4.x, c4.y, c4.z, c4.w};
+    GpuNode g;
+    uint32_t gnext = gidx[nd] + 1, t = toff[nd];
+    for (int j = 0; j < 4; ++j) {
+        if (c[j] < 0) {
+            g.lox[j] = g.hix[j] = g.loy[j] = g.hiy[j] = g.loz[j] = g.hiz[j] = 0.0f;
+            g.child[j] = ~(int32_t)0;           // leaf of 0 triangles: never entered
+            continue;
+        }
+        const BinNode& b = nodes[c[j]];
+        float blo[3] = {b.lo[0], b.lo[1], b.lo[2]}, bhi[3] = {b.hi[0], b.hi[1], b.hi[2]};
+        for (int k = 0; k < 3; ++k) {
+            if (blo[k] <= bhi[k]) {
+                blo[k] = nextafterf(blo[k], -INFINITY);
+                bhi[k] = nextafterf(bhi[k], INFINITY);
+            }
+        }
+        g.lox[j] = blo[0]; g.hix[j] = bhi[0];
+        g.loy[j] = blo[1]; g.hiy[j] = bhi[1];
+        g.loz[j] = blo[2]; g.hiz[j] = bhi[2];
+        if (b.left >= 0) {
+            g.child[j] = (int32_t)gnext;
+            gidx[c[j]] = gnext;
+            toff[c[j]] = t;
+            gnext += n4[c[j]];
+        } else {
+            for (uint32_t k = 0; k < b.count; ++k) order[t + k] = ids[b.first + k];
+            g.child[j] = ~(int32_t)((t << 3) | b.count);
+            atomicAdd(leaves, 1u);
+        }
+        t += b.n_tris;
+    }
+    g.pad[0] = g.pad[1] = g.pad[2] = g.pad[3] = 0;
+    const float4* src = reinterpret_cast<const float4*>(&g);
+    float4* dst = reinterpret_cast<float4*>(out + gidx[nd]);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dst[k] = src[k];
+}
+
 template <class T>
 T* pool_alloc(size_t count, cudaStream_t s, std::vector<void*>& held) {
     int dev = 0;
@@ -410,7 +506,8 @@ T* pool_alloc(size_t count, cudaStream_t s, std::vector<void*>& held) {
 // false when the input is invalid (out-of-range index or non-finite vertex: the caller's host
 // builder reports which).  Throws tri::CudaError on CUDA failures.
 bool build_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_t, uint32_t nt, uint32_t max_leaf,
-                      cudaStream_t s, BvhBuildResult& out) {
+                      cudaStream_t s, const std::function<GpuNode*(size_t)>& alloc_nodes, uint32_t* d_order,
+                      DeviceBvh& out) {
     const auto t0 = std::chrono::steady_clock::now();
     if (nt == 0 || nt >= (1u << 28)) return false;
     if (max_leaf < 1 || max_leaf > 7) max_leaf = 4;
@@ -487,14 +584,57 @@ bool build_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_t, uint32
     TR_CUDA(cudaStreamSynchronize(s));
     if (h[4]) return false;
     const uint32_t nnodes = h[0];
-    std::vector<BinNode> nodes(nnodes);
-    std::vector<uint32_t> ids(nt);
-    TR_CUDA(cudaMemcpyAsync(nodes.data(), d.nodes, sizeof(BinNode) * nnodes, cudaMemcpyDeviceToHost, s));
-    TR_CUDA(cudaMemcpyAsync(ids.data(), d.ids[cur], sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, s));
+    BinNode top;
+    TR_CUDA(cudaMemcpyAsync(&top, d.nodes, sizeof(top), cudaMemcpyDeviceToHost, s));
     TR_CUDA(cudaStreamSynchronize(s));
-    const bool ok = finish_bvh(nodes.data(), nnodes, ids.data(), nt, h[3], nullptr, nullptr, false, out);
+    if (top.left < 0) return false;                 // a one-leaf scene: the host builder takes it
+
+    // collapse to four-child nodes, level by level from the root
+    uint32_t* q = pool_alloc<uint32_t>(nnodes, s, held);
+    int4* kids = pool_alloc<int4>(nnodes, s, held);
+    uint32_t* n4 = pool_alloc<uint32_t>(nnodes, s, held);
+    uint32_t* gidx = pool_alloc<uint32_t>(nnodes, s, held);
+    uint32_t* toff = pool_alloc<uint32_t>(nnodes, s, held);
+    const uint32_t zero = 0;
+    TR_CUDA(cudaMemcpyAsync(q, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
+    TR_CUDA(cudaMemcpyAsync(gidx, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
+    TR_CUDA(cudaMemcpyAsync(toff, &zero, sizeof(zero), cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> lvl_lo{0}, lvl_n{1};
+    while (true) {
+        const uint32_t lo = lvl_lo.back(), n = lvl_n.back();
+        const uint32_t next0 = lo + n;
+        TR_CUDA(cudaMemcpyAsync(d.counters + 5, &next0, sizeof(next0), cudaMemcpyHostToDevice, s));
+        k_collapse<<<(n + 127) / 128, 128, 0, s>>>(d.nodes, q, lo, n, d.counters + 5, kids);
+        TR_CUDA(cudaGetLastError());
+        uint32_t next = 0;
+        TR_CUDA(cudaMemcpyAsync(&next, d.counters + 5, sizeof(next), cudaMemcpyDeviceToHost, s));
+        TR_CUDA(cudaStreamSynchronize(s));
+        if (next == next0) break;
+        lvl_lo.push_back(next0);
+        lvl_n.push_back(next - next0);
+    }
+    const int levels = (int)lvl_lo.size();
+    for (int L = levels - 1; L >= 0; --L)
+        k_count4<<<(lvl_n[L] + 127) / 128, 128, 0, s>>>(d.nodes, q, lvl_lo[L], lvl_n[L], kids, n4);
+    uint32_t n4root = 0;
+    TR_CUDA(cudaMemcpyAsync(&n4root, n4, sizeof(n4root), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(cudaStreamSynchronize(s));
+    GpuNode* dn = alloc_nodes(n4root);
+    TR_CUDA(cudaMemsetAsync(d.counters + 6, 0, sizeof(uint32_t), s));
+    for (int L = 0; L < levels; ++L)
+        k_place4<<<(lvl_n[L] + 127) / 128, 128, 0, s>>>(d.nodes, d.ids[cur], q, lvl_lo[L], lvl_n[L], kids, n4,
+                                                          gidx, toff, dn, d_order, d.counters + 6);
+    TR_CUDA(cudaGetLastError());
+    uint32_t leaves = 0;
+    TR_CUDA(cudaMemcpyAsync(&leaves, d.counters + 6, sizeof(leaves), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(cudaStreamSynchronize(s));
+    out.nodes = n4root;
+    out.depth = (uint32_t)levels;
+    out.stack = 3 * out.depth + 1;
+    out.binary_depth = h[3];
+    out.leaves = leaves;
     out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    return ok;
+    return true;
 }
 
 }  // namespace trh

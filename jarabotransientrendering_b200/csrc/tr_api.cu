@@ -584,33 +584,46 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         TR_CUDA(cudaMemcpyAsync(d_t, s->triangles, sizeof(uint32_t) * 3 * ntri, cudaMemcpyHostToDevice, x->stream));
         TR_CUDA(cudaMemcpyAsync(d_m, s->triangle_material, sizeof(uint32_t) * ntri, cudaMemcpyHostToDevice, x->stream));
 
-        // BVH (replaces World::freeze -> rtcCommit): built on the device from the uploaded arrays;
-        // on invalid input the host builder names the offending index or vertex
+        // BVH (replaces World::freeze -> rtcCommit): built on the device from the uploaded arrays,
+        // nodes and leaf order left there; the host builder takes one-leaf scenes and names the
+        // offending index or vertex of invalid input
+        trh::DeviceBvh dbv;
+        float4* dnodes = nullptr;
+        const bool on_device = trh::build_bvh_device(
+            d_v, s->num_vertices, d_t, s->num_triangles, 4, x->stream,
+            [&](size_t n) { dnodes = x->alloc<float4>(n * 8); return reinterpret_cast<trh::GpuNode*>(dnodes); },
+            d_o, dbv);
         trh::BvhBuildResult bvh;
-        std::string msg;
-        if (!trh::build_bvh_device(d_v, s->num_vertices, d_t, s->num_triangles, 4, x->stream, bvh) &&
-            !trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg,
-                            /*write_tris*/ false)) {
-            cudaStreamSynchronize(x->stream);
-            x->release();
-            delete x;
-            return fail(TR_ERR_INVALID_ARGUMENT, msg);
+        if (!on_device) {
+            std::string msg;
+            if (!trh::build_bvh(s->vertices, s->num_vertices, s->triangles, s->num_triangles, 4, bvh, &msg,
+                                /*write_tris*/ false)) {
+                cudaStreamSynchronize(x->stream);
+                x->release();
+                delete x;
+                return fail(TR_ERR_INVALID_ARGUMENT, msg);
+            }
+            dbv.nodes = (uint32_t)bvh.nodes.size();
+            dbv.depth = bvh.depth;
+            dbv.stack = bvh.stack;
+            dbv.build_ms = bvh.build_ms;
+            dnodes = x->alloc<float4>(bvh.nodes.size() * 8);
+            upload(dnodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode), x->stream);
+            TR_CUDA(cudaMemcpyAsync(d_o, bvh.order.data(), sizeof(uint32_t) * ntri, cudaMemcpyHostToDevice, x->stream));
         }
-        if (bvh.stack > (uint32_t)trk::kStack) {
+        if (dbv.stack > (uint32_t)trk::kStack) {
             cudaStreamSynchronize(x->stream);
             x->release();
             delete x;
             return fail(TR_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
         }
-        x->bvh_nodes = (uint32_t)bvh.nodes.size();
-        x->bvh_depth = bvh.stack - 1;               // sizes the shared-memory traversal stack
-        x->bvh_levels = bvh.depth;
-        x->bvh_ms = bvh.build_ms;
-        x->d_nodes = x->alloc<float4>(bvh.nodes.size() * 8);
-        upload(x->d_nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(trh::GpuNode), x->stream);
+        x->bvh_nodes = dbv.nodes;
+        x->bvh_depth = dbv.stack - 1;               // sizes the shared-memory traversal stack
+        x->bvh_levels = dbv.depth;
+        x->bvh_ms = dbv.build_ms;
+        x->d_nodes = dnodes;
         // the leaf-ordered triangle records and the per-triangle normals, built on the device
         // (World.h:449 normals, the same IEEE operations as a host evaluation)
-        TR_CUDA(cudaMemcpyAsync(d_o, bvh.order.data(), sizeof(uint32_t) * ntri, cudaMemcpyHostToDevice, x->stream));
         x->d_tris = x->alloc<float4>(ntri * 3);
         x->d_tri_ng = x->alloc<float4>(ntri);
         TR_CUDA(trk::launch_build_tris(d_v, d_t, d_m, d_o, (uint32_t)ntri, x->d_tris, x->d_tri_ng, x->stream));

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "tr_guide.cuh"
@@ -211,10 +212,21 @@ tr_status train_on_pool(tr_guide* g, const trk::GuideWave& gw, const uint32_t* p
 }  // namespace tri
 
 namespace trh {
-struct BvhBuildResult;
+struct GpuNode;
+// Figures of a device build (its nodes and leaf order stay on the device).
+struct DeviceBvh {
+    uint32_t nodes = 0;          // four-child nodes
+    uint32_t depth = 0;          // four-child levels on the deepest path
+    uint32_t stack = 0;          // traversal stack entries a ray can need
+    uint32_t binary_depth = 0;
+    uint32_t leaves = 0;
+    double build_ms = 0.0;
+};
 // Binned-SAH build on the device (bvh_gpu.cu) from device-resident vertices [nv][3] and
-// triangles [nt][3], collapsed to four-child nodes like build_bvh; false on invalid input (the
-// host builder then reports which index or vertex).
+// triangles [nt][3], collapsed to four-child nodes as build_bvh does: the nodes go to
+// alloc_nodes(count), the triangle ids in leaf order to d_order [nt].  False on invalid input or
+// a one-leaf scene (the host builder then builds, or reports which index or vertex is wrong).
 bool build_bvh_device(const float* d_vertices, uint32_t nv, const uint32_t* d_triangles, uint32_t nt,
-                      uint32_t max_leaf, cudaStream_t s, BvhBuildResult& out);
+                      uint32_t max_leaf, cudaStream_t s, const std::function<GpuNode*(size_t)>& alloc_nodes,
+                      uint32_t* d_order, DeviceBvh& out);
 }  // namespace trh
