@@ -80,22 +80,38 @@ __device__ __forceinline__ bool trav_run(const SceneDev& sc, const WRay& r, Trav
             slab4(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, c1, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k1);
             slab4(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, c2, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k2);
             slab4(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, c3, ox, oy, oz, ix, iy, iz, r.tnear, st.best, k3);
-            order2(k0, c0, k1, c1);
-            order2(k2, c2, k3, c3);
-            order2(k0, c0, k2, c2);
-            order2(k1, c1, k3, c3);
-            order2(k1, c1, k2, c2);
-            if (k0 == kInf) {
-                if (st.sp == 0) return true;
-                --st.sp;
-                st.node = stack[st.sp * stride];
-                continue;
+            if constexpr (!kAnyHit) {
+                order2(k0, c0, k1, c1);
+                order2(k2, c2, k3, c3);
+                order2(k0, c0, k2, c2);
+                order2(k1, c1, k3, c3);
+                order2(k1, c1, k2, c2);
+                if (k0 == kInf) {
+                    if (st.sp == 0) return true;
+                    --st.sp;
+                    st.node = stack[st.sp * stride];
+                    continue;
+                }
+                // farthest first, so the nearest of the others is popped next
+                if (k3 != kInf) { stack[st.sp * stride] = c3; ++st.sp; }
+                if (k2 != kInf) { stack[st.sp * stride] = c2; ++st.sp; }
+                if (k1 != kInf) { stack[st.sp * stride] = c1; ++st.sp; }
+                st.node = c0;
+            } else {
+                // any hit ends the query: children in slot order, no sorting
+                int next = -1;
+                if (k3 != kInf) { next = c3; }
+                if (k2 != kInf) { if (next != -1) { stack[st.sp * stride] = next; ++st.sp; } next = c2; }
+                if (k1 != kInf) { if (next != -1) { stack[st.sp * stride] = next; ++st.sp; } next = c1; }
+                if (k0 != kInf) { if (next != -1) { stack[st.sp * stride] = next; ++st.sp; } next = c0; }
+                if (next == -1) {
+                    if (st.sp == 0) return true;
+                    --st.sp;
+                    st.node = stack[st.sp * stride];
+                    continue;
+                }
+                st.node = next;
             }
-            // farthest first, so the nearest of the others is popped next
-            if (k3 != kInf) { stack[st.sp * stride] = c3; ++st.sp; }
-            if (k2 != kInf) { stack[st.sp * stride] = c2; ++st.sp; }
-            if (k1 != kInf) { stack[st.sp * stride] = c1; ++st.sp; }
-            st.node = c0;
             continue;
         }
         const uint32_t ref = (uint32_t)(~st.node);
