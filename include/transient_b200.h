@@ -358,7 +358,8 @@ typedef struct tr_batch tr_batch;
 typedef struct tr_batch_config {
     uint32_t capacity;       /* path slots per wavefront batch (queue size), 65,536 .. 8,388,608 */
     uint32_t shade_block;    /* threads per shade block: 128 or 256 */
-    uint32_t splat_div;      /* film tile width = each scene's automatic width / splat_div (1, 2, 4, ...) */
+    uint32_t splat_div;      /* pixels per splat block = the automatic count (whole pixels filling
+                              * one 512-thread block) / splat_div (1, 2, 4, ...)                  */
     uint32_t use_graph;      /* 1: replay the batch launches from a captured CUDA graph; 0: launch directly */
 } tr_batch_config;
 
@@ -368,8 +369,8 @@ tr_status tr_batch_get_config(tr_batch* b, tr_batch_config* cfg);
 /* Adds camera samples [sample_begin[i], sample_begin[i] + sample_count[i]) of every pixel of
  * scene i to context i's film (a count of 0 skips the scene).                               */
 tr_status tr_batch_render(tr_batch* b, const uint64_t* sample_begin, const uint32_t* sample_count);
-/* Project autotuner: times candidate configurations (queue capacity, shade block, film tile
- * width), trial k rendering samples [sample_begin[i] + k*trial_samples[i], +trial_samples[i])
+/* Project autotuner: times candidate configurations (queue capacity, shade block, pixels per
+ * splat block), trial k rendering samples [sample_begin[i] + k*trial_samples[i], +trial_samples[i])
  * of scene i, keeps the fastest configuration and returns it in best.  The trial renders add
  * to the films like any render; *trials_run = number of trials.                              */
 tr_status tr_batch_autotune(tr_batch* b, const uint64_t* sample_begin, const uint32_t* trial_samples,

@@ -83,8 +83,8 @@ tr_status validate(const tr_scene* s, const tr_camera* c, const tr_film* f, cons
     if (f->bounce_films > 32) return fail(TR_ERR_INVALID_ARGUMENT, "at most 32 bounce films");
     if (f->components & ~(TR_COMP_DEPTH | TR_COMP_POSITIONS | TR_COMP_NORMALS))
         return fail(TR_ERR_INVALID_ARGUMENT, "unknown film component bits");
-    if (trk::splat_smem_bytes(f->time_bins, 1) > 220 * 1024)
-        return fail(TR_ERR_NOT_SUPPORTED, "time_bins too large for one shared-memory pixel tile");
+    if (f->time_bins >= trk::kBinOutside)     // bin indices are 24-bit fields of the splat records
+        return fail(TR_ERR_INVALID_ARGUMENT, "time_bins must be below 16777215");
     if (it->sqrt_spp == 0 || it->incoming_samples == 0)
         return fail(TR_ERR_INVALID_ARGUMENT, "sqrt_spp and incoming_samples must be >= 1");
     if (it->max_bounces > kMaxBounces) return fail(TR_ERR_INVALID_ARGUMENT, "max_bounces must be <= 63");
@@ -405,9 +405,9 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 launches += 1 + 2ull * x->bd.nvert;
                 sh_l += x->bd.nvert;
             }
-            timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm); });
+            timed(4, [&] { return trk::launch_splat(p, strm); });
             for (uint32_t b = 0; b < x->film.bounce_films; ++b)
-                timed(4, [&] { return trk::launch_splat(p, x->splat_g, strm, (int)b); });
+                timed(4, [&] { return trk::launch_splat(p, strm, (int)b); });
             if (x->film.bounce_films) {
                 timed(4, [&] { return trk::launch_bounce_weights(p, strm); });
                 launches += 1ull + x->film.bounce_films;
@@ -686,8 +686,6 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
         }
 
         x->trace_grid = trk::trace_grid_size(device, x->bvh_depth);
-        int g = (int)(kSplatSmemBudget / trk::splat_smem_bytes(f->time_bins, 1));
-        x->splat_g = std::max(1, std::min(g, 16));
         x->d_cursor = x->alloc<uint32_t>(1);
         TR_CUDA(cudaStreamSynchronize(x->stream));
 
@@ -1048,8 +1046,8 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
             TR_CUDA(trk::launch_shade(p, (int)d, strm));
             TR_CUDA(trk::launch_shadow(p, (int)d, x->trace_grid, strm));
         }
-        TR_CUDA(trk::launch_splat(p, x->splat_g, strm));
-        for (uint32_t b = 0; b < x->film.bounce_films; ++b) TR_CUDA(trk::launch_splat(p, x->splat_g, strm, (int)b));
+        TR_CUDA(trk::launch_splat(p, strm));
+        for (uint32_t b = 0; b < x->film.bounce_films; ++b) TR_CUDA(trk::launch_splat(p, strm, (int)b));
         if (x->film.bounce_films) TR_CUDA(trk::launch_bounce_weights(p, strm));
         x->stats.paths += paths;
         x->stats.camera_samples += npix * ns;

@@ -33,7 +33,6 @@ struct tr_batch {
     trk::Wave wave{};
     uint32_t max_bounces = 1, bvh_depth = 0;
     int trace_grid = 0;
-    std::vector<uint32_t> splat_auto;       // automatic film tile width of each scene
     tr_batch_config cfg{1u << 21, 256, 1, 1};
 
     // learned proposal
@@ -46,11 +45,11 @@ struct tr_batch {
 
     // captured graph and the launch shape it replays
     struct Shape {
-        uint32_t capacity = 0, shade_block = 0, max_blocks = 0, smem = 0, guided = 0, pool = 0;
+        uint32_t capacity = 0, shade_block = 0, max_blocks = 0, guided = 0, pool = 0;
         float mix = 0.f, keep = 0.f;
         bool operator==(const Shape& o) const {
             return capacity == o.capacity && shade_block == o.shade_block && max_blocks == o.max_blocks &&
-                   smem == o.smem && guided == o.guided && pool == o.pool && mix == o.mix && keep == o.keep;
+                   guided == o.guided && pool == o.pool && mix == o.mix && keep == o.keep;
         }
     };
     cudaGraph_t graph = nullptr;
@@ -83,13 +82,14 @@ namespace {
 struct Plan {
     std::vector<trk::BatchDesc> batches;
     uint32_t max_blocks = 0;
-    size_t smem = 0;
     uint64_t slots = 0;
     std::vector<uint64_t> scene_slots;      // per scene
 };
 
-uint32_t splat_width(const tr_batch* b, uint32_t scene) {
-    return std::max<uint32_t>(1u, b->splat_auto[scene] / std::max<uint32_t>(1u, b->cfg.splat_div));
+// pixels per splat block of a segment: the automatic width (whole pixels filling one block)
+// divided by the configuration's splat_div
+uint32_t splat_width(const tr_batch* b, uint32_t per_pix) {
+    return std::max<uint32_t>(1u, trk::splat_pixels_per_block(per_pix) / std::max<uint32_t>(1u, b->cfg.splat_div));
 }
 
 Plan make_plan(const tr_batch* b, const uint64_t* s_begin, const uint32_t* s_count) {
@@ -112,12 +112,11 @@ Plan make_plan(const tr_batch* b, const uint64_t* s_begin, const uint32_t* s_cou
         const uint32_t ninc = x->integ.incoming_samples;
         const uint32_t W = x->film.width, H = x->film.height;
         const uint32_t npix_total = W * H;
-        const uint32_t G = splat_width(b, i);
-        pl.smem = std::max(pl.smem, trk::splat_smem_bytes(x->film.time_bins, (int)G));
         const uint32_t ns_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(count, cap / ninc));
         for (uint32_t sb = 0; sb < count; sb += ns_chunk) {
             const uint32_t ns = std::min(ns_chunk, count - sb);
             const uint32_t per_pix = ns * ninc;
+            const uint32_t G = splat_width(b, per_pix);
             uint32_t pix = 0;
             while (pix < npix_total) {
                 const uint32_t free = cap - used;
@@ -208,7 +207,6 @@ trk::Params batch_params(const tr_batch* b, const Plan& pl) {
     p.multi.cur = b->d_cur;
     p.multi.nscenes = (uint32_t)b->ctx.size();
     p.multi.max_splat_blocks = std::max<uint32_t>(1u, pl.max_blocks);
-    p.multi.splat_smem = (uint32_t)pl.smem;
     p.multi.shade_block = b->cfg.shade_block;
     if (b->guide) {
         p.guide = b->gw;
@@ -231,7 +229,7 @@ void enqueue_batch(const tr_batch* b, const trk::Params& p, cudaStream_t s, uint
         count += 3;
     }
     if (guided && b->pool) { TR_CUDA(trk::launch_train_gather(p, b->pool_state, s)); count += 2; }
-    TR_CUDA(trk::launch_splat(p, 0, s));
+    TR_CUDA(trk::launch_splat(p, s));
     TR_CUDA(trk::launch_advance(b->d_cur, s));
     count += 3;
 }
@@ -270,7 +268,6 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
     shape.capacity = b->cfg.capacity;
     shape.shade_block = b->cfg.shade_block;
     shape.max_blocks = p.multi.max_splat_blocks;
-    shape.smem = p.multi.splat_smem;
     shape.guided = guided ? 1u : 0u;
     shape.pool = b->pool;
     shape.mix = guided ? b->gw.mix_prob : 0.f;
@@ -377,7 +374,6 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
             S.flags = px.flags;
             b->max_bounces = std::max(b->max_bounces, x->integ.max_bounces);
             b->bvh_depth = std::max(b->bvh_depth, x->bvh_depth);
-            b->splat_auto.push_back((uint32_t)x->splat_g);
         }
         b->d_scenes = b->alloc<trk::SceneSlot>(n);
         // ordered on the batch's stream (a plain cudaMemcpy from pageable memory may return

@@ -54,7 +54,6 @@ T* dalloc(size_t count, size_t& total) {
 
 constexpr uint32_t kMaxBounces = 63;            // counters hold 64 depths
 constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batch
-constexpr size_t kSplatSmemBudget = 56 * 1024;   // four 512-thread splat CTAs per SM
 
 }  // namespace tri
 
@@ -150,7 +149,6 @@ struct tr_ctx {
     float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows
     size_t stage_floats = 0;
     int trace_grid = 0;
-    int splat_g = 1;
 
     // ray-batch scratch
     float* d_rays = nullptr;

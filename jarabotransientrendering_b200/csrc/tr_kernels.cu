@@ -804,14 +804,38 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p,
 // splat: StreakCameraFilm::add_samples / add_temporal_sample (StreakCameraFilm.h:139-192,
 // 279-315) with the box filter of size 1: bin = floor((t - offset) / exposure) (computed in
 // shade), streak(pixel, bin) += L, steady(pixel) += L, weight(pixel) += 1 per camera sample.
-// A CTA owns `G` whole pixels of the batch, accumulates their records in an FP32 shared-memory
-// tile (warp-aggregated atomics on equal (pixel, bin) keys) and adds the tile to the FP64 film.
+// A CTA owns `G` whole pixels of the batch.  A warp reads one record per lane and step; lanes
+// holding the same (pixel, bin) sum their radiance with shuffles and the group's lowest lane
+// adds the sum to the FP64 film with native double atomics (resolved in L2, so the film cells
+// of a pixel's hot bins stay on chip while its warps add to them).  Steady sums are kept per
+// lane and added the same way once per pass over the slots.
 // -----------------------------------------------------------------------------------------
+
+// Sum (x, y, z) over the lanes of `peers` (the calling lane's group, all lanes active); the
+// group's lowest lane receives the total.  Tree over the group's ranks: at step s the member of
+// rank r (r a multiple of 2s) adds the partial sum of rank r + s.  Each lane keeps the lane
+// index of the member s ranks above it (32: none) and doubles that distance per step by
+// pointer jumping.  `steps_to` is the largest group size that has to be summed.
+__device__ __forceinline__ void group_sum3(unsigned peers, unsigned lane, uint32_t steps_to, float& x, float& y,
+                                          float& z) {
+    const int rank = __popc(peers & lanemask_lt());
+    const unsigned above = peers & ~((2u << lane) - 1u);      // lane 31: 2u << 31 == 0
+    int up = above ? __ffs(above) - 1 : 32;
+    for (int step = 1; step < (int)steps_to; step <<= 1) {
+        const int src = up < 32 ? up : (int)lane;
+        const float ox = __shfl_sync(kFull, x, src);
+        const float oy = __shfl_sync(kFull, y, src);
+        const float oz = __shfl_sync(kFull, z, src);
+        const int up2 = __shfl_sync(kFull, up, src);
+        if ((rank & (2 * step - 1)) == 0 && up < 32) { x += ox; y += oy; z += oz; }
+        up = up < 32 ? up2 : 32;
+    }
+}
+
 template <bool kMulti>
 __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ Params p, int G_launch, int bsel) {
-    extern __shared__ __align__(16) float tile[];
     // the block's segment and film: the launch's own in single-scene mode; in multi-scene mode
-    // from the current batch's block table, each segment with its own film-tile width
+    // from the current batch's block table, each segment with its own pixels per block
     const Batch* Bp = &p.batch;
     const FilmDev* Fp = &p.film;
     uint32_t G = (uint32_t)G_launch, blk = blockIdx.x;
@@ -838,99 +862,62 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
     double* out_steady = bsel < 0 ? film.steady : film.bsteady + (size_t)bsel * npix_film * 3u;
     const bool steady_all = bsel < 0 && film.nbounce > 0;
     const uint32_t nb_last = film.nbounce ? film.nbounce - 1u : 0u;
-    float* steady = tile + (size_t)G * TT;
-    {
-        float4* t4 = reinterpret_cast<float4*>(tile);
-        const uint32_t n4 = ((uint32_t)G * TT + 3u * G + 3u) / 4u;
-        for (uint32_t e = threadIdx.x; e < n4; e += blockDim.x) t4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    __syncthreads();
+    // film pixel of the block's pixel `pl`
+    auto film_pixel = [&](uint32_t pl) {
+        const uint32_t wpix = B.pix_begin + pix0 + pl;
+        return (size_t)(B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
+    };
     const uint32_t per_pix = B.ns * B.ninc;
     const uint32_t nslots = gp * per_pix;
     const uint32_t slot0 = B.slot_begin + pix0 * per_pix;
     const size_t rs = p.wave.capacity;           // records are [bounce][slot]
     const unsigned lane = threadIdx.x & 31u;
-    const unsigned lt = lanemask_lt();
-    // per-lane running steady-image sums, flushed when the lane moves to another pixel
-    uint32_t acc_pl = 0xffffffffu;
-    float ax = 0.f, ay = 0.f, az = 0.f;
     for (uint32_t base = (threadIdx.x & ~31u); base < nslots; base += blockDim.x) {
         const uint32_t ls = base + lane;
         const bool act = ls < nslots;
         const uint32_t slot = slot0 + (act ? ls : 0u);
         const uint32_t cnt = act ? (uint32_t)p.wave.rec_n[slot] : 0u;
         const uint32_t pl = act ? ls / per_pix : 0u;
-        if (act && pl != acc_pl) {
-            if (acc_pl != 0xffffffffu) {
-                float* sd = steady + acc_pl * 3u;
-                atomicAdd(sd, ax); atomicAdd(sd + 1, ay); atomicAdd(sd + 2, az);
-            }
-            acc_pl = pl; ax = ay = az = 0.f;
-        }
+        // a warp's 32 slots span at most 32 pixels: keys (pixel - the warp's first) * T + bin
+        // stay below 32 * 2^24 and never reach the out-of-window key
+        const uint32_t pl_rel = pl - __shfl_sync(kFull, pl, 0);
+        float ax = 0.f, ay = 0.f, az = 0.f;              // this lane's steady-image sum
         const uint32_t kmax = __reduce_max_sync(kFull, cnt);
+        // records are streamed (read once); the next one is in flight while this one is summed
+        float4 next = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (cnt > 0u) next = __ldcs(&p.wave.rec[slot]);
         for (uint32_t k = 0; k < kmax; ++k) {
             const bool valid = k < cnt;
-            float4 rc = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (valid) rc = __ldcs(&p.wave.rec[(size_t)k * rs + slot]);     // streamed, read once
+            const float4 rc = next;
+            if (k + 1u < cnt) next = __ldcs(&p.wave.rec[(size_t)(k + 1u) * rs + slot]);
             const uint32_t bin = __float_as_uint(rc.w) & 0x00ffffffu;
             const uint32_t rdepth = __float_as_uint(rc.w) >> 24;
             const bool mine = valid && (bsel < 0 || min(rdepth, nb_last) == (uint32_t)bsel);
             const bool inwin = mine && bin != kBinOutside;
-            const uint32_t key = inwin ? pl * T + bin : 0xffffffffu;
-            // lanes holding the same (pixel, bin) are summed with shuffles; the group's
-            // lowest lane issues one shared-memory atomic per channel
+            const uint32_t key = inwin ? pl_rel * T + bin : 0xffffffffu;
             const unsigned peers = __match_any_sync(kFull, key);
-            const int rank = __popc(peers & lt);
-            const int gsize = __popc(peers);
+            const uint32_t maxg = __reduce_max_sync(kFull, inwin ? (uint32_t)__popc(peers) : 1u);
             float vx = rc.x, vy = rc.y, vz = rc.z;
-            const uint32_t maxg = __reduce_max_sync(kFull, inwin ? (uint32_t)gsize : 1u);
-            for (int step = 1; step < (int)maxg; step <<= 1) {
-                const int src_rank = rank + step;
-                const int src = src_rank < gsize ? (int)__fns(peers, 0, src_rank + 1) : (int)lane;
-                const float ox = __shfl_sync(kFull, vx, src);
-                const float oy = __shfl_sync(kFull, vy, src);
-                const float oz = __shfl_sync(kFull, vz, src);
-                if ((rank & (2 * step - 1)) == 0 && src_rank < gsize) { vx += ox; vy += oy; vz += oz; }
-            }
-            if (inwin && rank == 0) {
-                float* cell = tile + (size_t)key * 3u;
-                atomicAdd(cell, vx); atomicAdd(cell + 1, vy); atomicAdd(cell + 2, vz);
+            group_sum3(peers, lane, maxg, vx, vy, vz);
+            if (inwin && (peers & lanemask_lt()) == 0u) {
+                double* cell = out_streak + film_pixel(pl) * TT + (size_t)bin * 3u;
+                atomicAdd(cell, (double)vx); atomicAdd(cell + 1, (double)vy); atomicAdd(cell + 2, (double)vz);
             }
             if (inwin || (steady_all && valid)) { ax += rc.x; ay += rc.y; az += rc.z; }
         }
-    }
-    if (acc_pl != 0xffffffffu) {
-        float* sd = steady + acc_pl * 3u;
-        atomicAdd(sd, ax); atomicAdd(sd + 1, ay); atomicAdd(sd + 2, az);
-    }
-    __syncthreads();
-    // flush: FP64 read-add-write of the touched bins (the film starts zeroed); four
-    // independent loads in flight per thread
-    for (uint32_t pl = 0; pl < gp; ++pl) {
-        const uint32_t wpix = B.pix_begin + pix0 + pl;
-        const size_t pixel = (size_t)(B.win_y0 + wpix / B.win_w) * film.W + (B.win_x0 + wpix % B.win_w);
-        double* dst = out_streak + pixel * TT;
-        const float* src = tile + (size_t)pl * TT;
-        for (uint32_t e0 = threadIdx.x; e0 < TT; e0 += 4u * blockDim.x) {
-            float v[4];
-            double o[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint32_t e = e0 + (uint32_t)u * blockDim.x;
-                v[u] = e < TT ? src[e] : 0.0f;
-                o[u] = v[u] != 0.0f ? dst[e] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint32_t e = e0 + (uint32_t)u * blockDim.x;
-                if (v[u] != 0.0f) dst[e] = o[u] + (double)v[u];
-            }
-        }
-        if (threadIdx.x == 0) {
-            if (bsel < 0) film.weight[pixel] += (double)B.ns;
-            for (int c = 0; c < 3; ++c) out_steady[pixel * 3 + c] += (double)steady[pl * 3 + c];
+        // steady image: lanes of the same pixel sum, the group's lowest lane adds
+        const bool has = act && (ax != 0.f || ay != 0.f || az != 0.f);
+        const unsigned peers = __match_any_sync(kFull, has ? pl_rel : 0xffffffffu);
+        const uint32_t maxg = __reduce_max_sync(kFull, has ? (uint32_t)__popc(peers) : 1u);
+        group_sum3(peers, lane, maxg, ax, ay, az);
+        if (has && (peers & lanemask_lt()) == 0u) {
+            double* sd = out_steady + film_pixel(pl) * 3u;
+            atomicAdd(sd, (double)ax); atomicAdd(sd + 1, (double)ay); atomicAdd(sd + 2, (double)az);
         }
     }
+    // weight: one per camera sample; the block owns its pixels, so a plain update
+    if (bsel < 0)
+        for (uint32_t pl = threadIdx.x; pl < gp; pl += blockDim.x) film.weight[film_pixel(pl)] += (double)B.ns;
 }
 
 // Per-bounce film weights (MultibounceStreakCameraFilm.h:151-171 with StreakCameraFilm.h:139-160):
@@ -1367,9 +1354,9 @@ int trace_grid_size(int device, uint32_t bvh_depth, bool multi) {
     return sms * per_sm;
 }
 
-size_t splat_smem_bytes(uint32_t T, int G) {
-    // tile [G][T][3] + steady [G][3] floats, rounded up to whole float4 (zeroed as float4)
-    return (((size_t)G * T * 3u + 3u * (size_t)G) * sizeof(float) + 15u) & ~size_t(15);
+uint32_t splat_pixels_per_block(uint32_t per_pix) {
+    // whole pixels that fill one splat block with one slot per thread
+    return per_pix >= (uint32_t)kSplatBlock ? 1u : (uint32_t)kSplatBlock / (per_pix ? per_pix : 1u);
 }
 
 // Kernel variants: multi-scene when the parameters carry a scene table (tr_batch), else the
@@ -1425,19 +1412,13 @@ cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s) 
     else k_shadow<false><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
 }
-cudaError_t launch_splat(const Params& p, int G, cudaStream_t s, int bsel) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_splat<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(k_splat<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr_set = true;
-    }
+cudaError_t launch_splat(const Params& p, cudaStream_t s, int bsel) {
     if (p.multi.scenes) {
-        k_splat<true><<<p.multi.max_splat_blocks, kSplatBlock, p.multi.splat_smem, s>>>(p, 0, bsel);
+        k_splat<true><<<p.multi.max_splat_blocks, kSplatBlock, 0, s>>>(p, 0, bsel);
     } else {
-        const size_t smem = splat_smem_bytes(p.film.T, G);
-        const uint32_t blocks = (p.batch.npix + (uint32_t)G - 1) / (uint32_t)G;
-        k_splat<false><<<blocks, kSplatBlock, smem, s>>>(p, G, bsel);
+        const uint32_t G = splat_pixels_per_block(p.batch.ns * p.batch.ninc);
+        const uint32_t blocks = (p.batch.npix + G - 1) / G;
+        k_splat<false><<<blocks, kSplatBlock, 0, s>>>(p, (int)G, bsel);
     }
     return cudaGetLastError();
 }

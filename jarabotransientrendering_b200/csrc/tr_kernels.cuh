@@ -98,7 +98,7 @@ struct Batch {
     uint32_t slot_begin;                // first slot (0 in single-scene mode)
     uint32_t scene;                     // index into MultiDev::scenes (0 in single-scene mode)
     uint32_t blk_begin;                 // first splat block of this segment
-    uint32_t splat_g;                   // pixels per splat block (film tile width)
+    uint32_t splat_g;                   // pixels per splat block
 };
 
 // Multi-scene rendering (tr_batch): per-scene data and the batch descriptors live in device
@@ -164,7 +164,6 @@ struct MultiDev {
     uint32_t nscenes;
     // launch shapes (host side): grids cover the largest batch of the plan
     uint32_t max_splat_blocks;
-    uint32_t splat_smem;         // bytes: largest film tile of the plan
     uint32_t shade_block;        // threads per shade block (128 or 256)
 };
 
@@ -224,7 +223,9 @@ cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s);
 cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s);
 cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s);
 // bsel < 0: the film itself; bsel = b: per-bounce film b (records of bounce min(depth, N-1) == b)
-cudaError_t launch_splat(const Params& p, int pixels_per_cta, cudaStream_t s, int bsel = -1);
+// pixels per splat block: automatic (whole pixels filling one block) in single-scene mode,
+// each segment's splat_g in multi-scene mode
+cudaError_t launch_splat(const Params& p, cudaStream_t s, int bsel = -1);
 // per-bounce film weights: +1 per camera sample with a record of that bounce film
 cudaError_t launch_bounce_weights(const Params& p, cudaStream_t s);
 // bidirectional connections: light subpath generation on the light wave `pl` (its own rays,
@@ -250,6 +251,6 @@ cudaError_t launch_guide(const Params& p, int depth, uint32_t* pool_state, cudaS
 cudaError_t launch_train_gather(const Params& p, uint32_t* pool_state, cudaStream_t s);
 int trace_grid_size(int device, uint32_t bvh_depth, bool multi = false);
 size_t trace_smem_bytes(uint32_t bvh_depth);
-size_t splat_smem_bytes(uint32_t T, int pixels_per_cta);
+uint32_t splat_pixels_per_block(uint32_t slots_per_pixel);
 
 }  // namespace trk

@@ -1,8 +1,8 @@
 """GPU tests of multi-scene batches (tr_batch_*): several contexts rendered in shared wavefront
 batches replayed from a captured CUDA graph.  Each scene's film must equal the film of rendering
 that context alone over the same sample range (same per-path random streams; sums differ only by
-the order of FP32 shared-memory additions), whatever the queue capacity, shade block, film tile
-width or graph use; the autotuner must return a valid configuration; a learned proposal shared by
+the grouping of FP32 warp sums and the order of FP64 film additions), whatever the queue
+capacity, shade block, pixels per splat block or graph use; the autotuner must return a valid configuration; a learned proposal shared by
 the batch must leave every scene's estimate unbiased."""
 import numpy as np
 import pytest

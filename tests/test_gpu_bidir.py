@@ -2,8 +2,8 @@
 vertex connections, BidirectionalPathTracing with set_path_tracing_only(false), in time-sampling
 mode) against the CPU oracle, which is pinned to the reference's own renderer in
 tests/test_oracle.py.  GPU and oracle replay the same eye walks, light subpaths (their own
-random stream) and connections, so the films agree per bin up to the order of FP32
-shared-memory additions."""
+random stream) and connections, so the films agree per bin up to the FP32 rounding of
+warp-group sums."""
 import numpy as np
 import pytest
 

@@ -1,7 +1,7 @@
 """GPU tests of the film options against the CPU oracle (which is pinned to the reference's own
 integrator for them in tests/test_oracle.py): camera unwarp (StreakCameraFilm.h:167) and
 per-bounce films (MultibounceStreakCameraFilm.h:151-171).  GPU and oracle replay the same
-random walks, so the films agree per bin up to the order of FP32 shared-memory additions."""
+random walks, so the films agree per bin up to the FP32 rounding of warp-group sums."""
 import os
 
 import numpy as np
@@ -66,7 +66,7 @@ def test_bounce_films_match_oracle(gpu, oracle_lib, name, nb, unwarp):
         _same(b[k]["steady"], o["bsteady"][k])
         assert (b[k]["weight"] == o["bweight"][k]).all()
     # the bounce films partition the in-window samples of the film (each film sums its records in
-    # its own FP32 shared-memory tiles, hence the FP32 tolerance)
+    # its own FP32 warp groups, hence the FP32 tolerance)
     assert np.allclose(sum(x["streak"] for x in b), f["streak"], rtol=RTOL, atol=1e-12)
 
 

@@ -5,7 +5,7 @@ golden films.
   watertight test, same fixed operation order), occlusion booleans identical;
 * renders: per-path random walks are bit-identical (same PCG32 streams, same IEEE operation
   sequence), so every (pixel, bin) sum agrees with the oracle up to the FP32 rounding of the
-  shared-memory tile (relative 2e-5);
+  warp-group sums added to the FP64 film (relative 2e-5);
 * statistics against the reference renderer's own films (tests/golden): per-bin z-scores and
   total energy;
 * size-independent properties at the full benchmark sizes: weight = samples per pixel,
@@ -20,7 +20,7 @@ from jarabotransientrendering_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
 
-RTOL_TILE = 2e-5     # FP32 shared-memory tile sums vs FP64 oracle sums of the same records
+RTOL_TILE = 2e-5     # FP32 warp-group sums vs FP64 oracle sums of the same records
 
 
 def small(name):

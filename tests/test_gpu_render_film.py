@@ -11,7 +11,7 @@ from jarabotransientrendering_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 2e-5          # FP32 shared-memory tile sums, as in the other film comparisons
+RTOL = 2e-5          # FP32 warp-group sums, as in the other film comparisons
 
 
 def _arrays(sc, dtype, pinned):
@@ -80,7 +80,7 @@ def test_render_film_over_several_sample_chunks(gpu):
     with gpu.Context(sc) as c:
         c.render_film(0, n, st, sd, wt)
     assert (wt == n).all()
-    # 2.5 M samples summed in FP32 shared-memory tiles, in launch-dependent order
+    # 2.5 M samples: FP32 warp-group sums added to the FP64 film in launch-dependent order
     _close(st, f["streak"], rtol=1e-3)
 
 

@@ -3,7 +3,7 @@ BidirectionalPathTracing::set_mode(SamplingMode::Transient)) against the CPU ora
 pinned to the reference's own renderer in tests/test_oracle.py.  GPU and oracle replay the same
 random walks: per-path light point, time-based free flights, no Russian roulette, time-angular
 directions in the medium (including the reference's rare tiny densities), so the films agree per
-bin up to the order of FP32 shared-memory additions."""
+bin up to the FP32 rounding of warp-group sums."""
 import numpy as np
 import pytest
 

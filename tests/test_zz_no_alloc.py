@@ -17,7 +17,7 @@ from jarabotransientrendering_b200 import _abi, scenes as S
 
 pytestmark = pytest.mark.gpu
 
-RTOL_TILE = 2e-5     # same tolerance as the other GPU film comparisons (FP32 tile sums)
+RTOL_TILE = 2e-5     # same tolerance as the other GPU film comparisons (FP32 warp-group sums)
 
 
 def _noalloc(ctx, window, s0, n, stream=None):
