@@ -102,7 +102,7 @@ typedef struct tr_camera {
 } tr_camera;
 
 /* Streak film (src/Film/StreakCameraFilm.h:91-121): width x height pixels, time_bins bins of
- * `exposure` path-length units starting at `offset`.
+ * `exposure` path-length units starting at `offset`; time_bins < 16777215 (24-bit bin field).
  * camera_unwarp ("-camera-unwarp"): bin every sample by its path time minus the distance from
  *   the camera to the first surface along its camera ray (StreakCameraFilm.h:167, World.h:749-766).
  * bounce_films ("-multibounce-streak N"): N > 0 adds N per-bounce streak films as

@@ -104,6 +104,30 @@ def test_render_matches_oracle_per_path(gpu, oracle_lib, name):
     assert st["closest_rays"] == fo["stats"]["closest_rays"]
 
 
+@pytest.mark.parametrize("sqrt_spp", [1, 4])
+def test_long_film_matches_oracle(gpu, oracle_lib, sqrt_spp):
+    # 65,536 time bins (a pixel's streak row is 1.5 MiB of FP64); one sample per pixel puts 32
+    # pixels in each warp's records, 16 samples two pixels
+    sc = S.cornell(width=16, height=12, time_bins=65536, exposure=0.0002, sqrt_spp=sqrt_spp, max_bounces=6)
+    with gpu.Context(sc) as ctx:
+        ctx.render(0, sc.spp)
+        fg = ctx.film()
+        st = ctx.stats()
+    fo = oracle_lib.Oracle(sc).render(sample_count=sc.spp, nthreads=8)
+    assert (fg["weight"] == fo["weight"]).all()
+    assert ((fg["streak"] != 0) == (fo["streak"] != 0)).all()
+    assert np.allclose(fg["streak"], fo["streak"], rtol=RTOL_TILE, atol=1e-12)
+    assert np.allclose(fg["steady"], fo["steady"], rtol=RTOL_TILE, atol=1e-12)
+    assert st["splats"] == fo["stats"]["splats"] > 0
+
+
+def test_time_bins_beyond_the_bin_field_are_refused(gpu):
+    sc = S.cornell(width=1, height=1, time_bins=(1 << 24) - 1, exposure=1e-6, sqrt_spp=1)
+    with pytest.raises(gpu.TransientError, match="time_bins") as ei:
+        gpu.Context(sc)
+    assert ei.value.status == 1
+
+
 def test_render_region_and_progressive_additivity(gpu, oracle_lib):
     sc = small("cornell")
     with gpu.Context(sc) as ctx:
