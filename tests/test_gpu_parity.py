@@ -121,6 +121,26 @@ def test_long_film_matches_oracle(gpu, oracle_lib, sqrt_spp):
     assert st["splats"] == fo["stats"]["splats"] > 0
 
 
+@pytest.mark.parametrize("flags", [0, S.FLAG_TIME_SAMPLING])
+def test_batches_on_two_wave_lanes_match_oracle(gpu, oracle_lib, flags):
+    # 48 x 48 pixels x 1024 samples = 2.36 M paths: two pixel batches of the 2^21-slot wave,
+    # rendered on alternating wave buffers and streams
+    sc = S.cornell(width=48, height=48, time_bins=128, exposure=0.04, sqrt_spp=32, max_bounces=4)
+    sc.flags |= flags
+    with gpu.Context(sc) as ctx:
+        ctx.render(0, sc.spp)
+        fg = ctx.film()
+        st = ctx.stats()
+    fo = oracle_lib.Oracle(sc).render(sample_count=sc.spp, nthreads=8)
+    assert (fg["weight"] == fo["weight"]).all()
+    assert ((fg["streak"] != 0) == (fo["streak"] != 0)).all()
+    assert np.allclose(fg["streak"], fo["streak"], rtol=RTOL_TILE, atol=1e-12)
+    assert np.allclose(fg["steady"], fo["steady"], rtol=RTOL_TILE, atol=1e-12)
+    assert st["splats"] == fo["stats"]["splats"]
+    assert st["shadow_rays"] == fo["stats"]["shadow_rays"]
+    assert st["closest_rays"] == fo["stats"]["closest_rays"]
+
+
 def test_time_bins_beyond_the_bin_field_are_refused(gpu):
     sc = S.cornell(width=1, height=1, time_bins=(1 << 24) - 1, exposure=1e-6, sqrt_spp=1)
     with pytest.raises(gpu.TransientError, match="time_bins") as ei:
