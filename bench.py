@@ -341,7 +341,10 @@ def batched(args, device, frames=2):
         res["plain_batched"] = {"paths_per_s": paths_frame * frames / sum(wall), "ms_per_frame": 1e3 * sum(wall) / frames,
                                 "graph_kernel_launches_per_frame": st["kernel_launches"]}
         B.close()
-        # one context after another (plain), same frame
+        # one context after another (plain), same frame; one untimed render per context first
+        # (its first own render allocates its wave buffers)
+        for c, k, a in zip(ctxs, spp, nxt):
+            c.render(a, k)
         for c in ctxs:
             c.clear()
         torch.cuda.synchronize(device)

@@ -219,10 +219,10 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.capacity = capacity;
 }
 
-// The second lane's buffers: the per-slot arrays of the first wave at its capacity, its own
-// queue counters, the first wave's statistics counters.
-void ensure_wave2(tr_ctx* x) {
-    trk::Wave& w = x->wave2;
+// Lane k + 1's buffers: the per-slot arrays of the first wave at its capacity, its own queue
+// counters, the first wave's statistics counters.
+void ensure_lane_wave(tr_ctx* x, int k) {
+    trk::Wave& w = x->lane_wave[k];
     const uint32_t capacity = x->wave.capacity;
     if (w.capacity >= capacity && w.counters) return;
     auto drop = [&](void* p) {
@@ -385,7 +385,13 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     const uint32_t T = x->film.time_bins;
     const bool f32 = sink && sink->type == TR_FILM_F32;
     if (sink) {
-        if (!x->copy_stream) TR_CUDA(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
+        if (!x->copy_stream) {
+            // highest priority: its FP32 conversions get SMs as soon as a traversal launch's
+            // blocks retire, so the host copies start without waiting behind the other lanes
+            int lo = 0, hi = 0;
+            TR_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            TR_CUDA(cudaStreamCreateWithPriority(&x->copy_stream, cudaStreamNonBlocking, hi));
+        }
         const uint32_t per_pix_max = std::min<uint32_t>(ns_total, std::max<uint32_t>(1u, cap / ninc)) * ninc;
         const size_t ppb_max = std::max<uint32_t>(1u, cap / per_pix_max);
         const size_t stage = ppb_max * ((size_t)T * 3u + 4u);
@@ -394,23 +400,24 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             x->stage_floats = stage;
         }
     }
-    // Two wave lanes: with more than one pixel batch and each pixel in one batch only (a single
-    // sample chunk), consecutive batches alternate between two sets of wave buffers and two
+    // Wave lanes: with more than one pixel batch and each pixel in one batch only (a single
+    // sample chunk), consecutive batches alternate between kWaveLanes sets of wave buffers and
     // pairs of streams, so one batch's last, nearly empty depths run beside the next batch's
     // first ones.  The batches share no pixels; the learned proposal (shared training pool)
     // and light subpaths (one light wave) keep a single lane.
     const uint64_t n_pix_batches = (win_pix + std::max<uint32_t>(1u, cap / (ns_chunk * ninc)) - 1) /
                                    std::max<uint32_t>(1u, cap / (ns_chunk * ninc));
-    const bool two_lanes = !guided && !bidir && ns_chunk >= ns_total && n_pix_batches > 1;
+    const int lanes = (!guided && !bidir && ns_chunk >= ns_total)
+                          ? (int)std::min<uint64_t>((uint64_t)kWaveLanes, n_pix_batches) : 1;
     uint32_t batch_no = 0;
-    if (two_lanes) {
-        ensure_wave2(x);
-        if (!x->lane_stream) TR_CUDA(cudaStreamCreateWithFlags(&x->lane_stream, cudaStreamNonBlocking));
-        if (!x->lane_shadow_stream)
-            TR_CUDA(cudaStreamCreateWithFlags(&x->lane_shadow_stream, cudaStreamNonBlocking));
+    for (int k = 0; k + 1 < lanes; ++k) {
+        ensure_lane_wave(x, k);
+        if (!x->lane_stream[k]) TR_CUDA(cudaStreamCreateWithFlags(&x->lane_stream[k], cudaStreamNonBlocking));
+        if (!x->lane_shadow_stream[k])
+            TR_CUDA(cudaStreamCreateWithFlags(&x->lane_shadow_stream[k], cudaStreamNonBlocking));
     }
     TR_CUDA(cudaEventRecord(x->ev0, strm));
-    if (two_lanes) TR_CUDA(order(strm, x->lane_stream));
+    for (int k = 0; k + 1 < lanes; ++k) TR_CUDA(order(strm, x->lane_stream[k]));
     for (uint64_t sb = 0; sb < ns_total; sb += ns_chunk) {
         const uint32_t ns = (uint32_t)std::min<uint64_t>(ns_chunk, ns_total - sb);
         const uint32_t per_pix = ns * ninc;
@@ -418,10 +425,10 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         for (uint64_t pb = 0; pb < win_pix; pb += ppb) {
             const uint32_t npix = (uint32_t)std::min<uint64_t>(ppb, win_pix - pb);
             trk::Params p = make_params(x);
-            const int lane = two_lanes ? (int)(batch_no++ & 1u) : 0;
-            const cudaStream_t ls = lane ? x->lane_stream : strm;
-            const cudaStream_t lsh = lane ? x->lane_shadow_stream : s_sh;
-            if (lane) p.wave = x->wave2;
+            const int lane = (int)(batch_no++ % (uint32_t)lanes);
+            const cudaStream_t ls = lane ? x->lane_stream[lane - 1] : strm;
+            const cudaStream_t lsh = lane ? x->lane_shadow_stream[lane - 1] : s_sh;
+            if (lane) p.wave = x->lane_wave[lane - 1];
             auto tl = [&](int kind, auto&& launch) { timed_on(kind, ls, launch); };
             p.batch.win_x0 = x0; p.batch.win_y0 = y0; p.batch.win_w = win_w;
             p.batch.pix_begin = (uint32_t)pb; p.batch.npix = npix;
@@ -530,7 +537,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             }
         }
     }
-    if (two_lanes) TR_CUDA(order(x->lane_stream, strm));
+    for (int k = 0; k + 1 < lanes; ++k) TR_CUDA(order(x->lane_stream[k], strm));
     if (sink) TR_CUDA(cudaStreamSynchronize(x->copy_stream));
     TR_CUDA(cudaEventRecord(x->ev1, strm));
     TR_CUDA(cudaEventSynchronize(x->ev1));

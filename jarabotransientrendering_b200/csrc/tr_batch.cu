@@ -21,6 +21,9 @@ using namespace tri;
 struct tr_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t shadow_stream = nullptr;   // shadow launches beside the next depth's extend
+    cudaEvent_t dep[4] = {};                // ordering events between the two, used in turn
+    uint32_t next_dep = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<tr_ctx*> ctx;
     std::vector<void*> allocs;
@@ -216,18 +219,31 @@ trk::Params batch_params(const tr_batch* b, const Plan& pl) {
     return p;
 }
 
-// the launches of one batch; `count` is incremented by the number of kernels
-void enqueue_batch(const tr_batch* b, const trk::Params& p, cudaStream_t s, uint64_t& count) {
+// `to` waits for the work enqueued on `from` so far (inside a capture: a graph dependency)
+void order(tr_batch* b, cudaStream_t from, cudaStream_t to) {
+    cudaEvent_t e = b->dep[b->next_dep++ % 4u];
+    TR_CUDA(cudaEventRecord(e, from));
+    TR_CUDA(cudaStreamWaitEvent(to, e, 0));
+}
+
+// the launches of one batch; `count` is incremented by the number of kernels.  The shadow
+// launch of depth d runs on the second stream beside the closest-hit launch of depth d + 1
+// (both only read what shade(d) wrote); shade(d + 1) refills the shadow queue and waits for it.
+void enqueue_batch(tr_batch* b, const trk::Params& p, cudaStream_t s, uint64_t& count) {
     const bool guided = b->guide != nullptr;
+    const cudaStream_t sh = b->shadow_stream;
     TR_CUDA(cudaMemsetAsync(b->wave.counters, 0, trk::kCounters * sizeof(uint32_t), s));
     TR_CUDA(trk::launch_raygen(p, s));
     for (uint32_t d = 0; d < b->max_bounces; ++d) {
         TR_CUDA(trk::launch_extend(p, (int)d, b->trace_grid, s));
+        if (d > 0) order(b, sh, s);
         TR_CUDA(trk::launch_shade(p, (int)d, s));
         if (guided) { TR_CUDA(trk::launch_guide(p, (int)d, b->pool_state, s)); ++count; }
-        TR_CUDA(trk::launch_shadow(p, (int)d, b->trace_grid, s));
+        order(b, s, sh);
+        TR_CUDA(trk::launch_shadow(p, (int)d, b->trace_grid, sh));
         count += 3;
     }
+    if (b->max_bounces) order(b, sh, s);
     if (guided && b->pool) { TR_CUDA(trk::launch_train_gather(p, b->pool_state, s)); count += 2; }
     TR_CUDA(trk::launch_splat(p, s));
     TR_CUDA(trk::launch_advance(b->d_cur, s));
@@ -357,6 +373,8 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         b->device = contexts[0]->device;
         TR_CUDA(cudaSetDevice(b->device));
         TR_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        TR_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : b->dep) TR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         TR_CUDA(cudaEventCreate(&b->ev0));
         TR_CUDA(cudaEventCreate(&b->ev1));
         std::vector<trk::SceneSlot> slots(n);
@@ -385,6 +403,9 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         b->stats.device_bytes = b->bytes;
     } catch (const CudaError& e) {
         for (void* p : b->allocs) cudaFree(p);
+        for (cudaEvent_t e : b->dep)
+            if (e) cudaEventDestroy(e);
+        if (b->shadow_stream) cudaStreamDestroy(b->shadow_stream);
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
@@ -519,6 +540,9 @@ tr_status tr_batch_destroy(tr_batch* b) {
     for (void* p : b->allocs) cudaFree(p);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    for (cudaEvent_t e : b->dep)
+        if (e) cudaEventDestroy(e);
+    if (b->shadow_stream) cudaStreamDestroy(b->shadow_stream);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return TR_OK;

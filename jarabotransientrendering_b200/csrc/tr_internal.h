@@ -54,6 +54,10 @@ T* dalloc(size_t count, size_t& total) {
 
 constexpr uint32_t kMaxBounces = 63;            // counters hold 64 depths
 constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batch
+#ifndef TR_WAVE_LANES
+#define TR_WAVE_LANES 4
+#endif
+constexpr int kWaveLanes = TR_WAVE_LANES;        // wave buffer sets batches alternate between
 
 }  // namespace tri
 
@@ -141,7 +145,7 @@ struct tr_ctx {
 
     // wavefront state
     trk::Wave wave{};
-    trk::Wave wave2{};                      // second lane of batches (shares wave.stats)
+    trk::Wave lane_wave[tri::kWaveLanes - 1]{};  // further lanes of batches (share wave.stats)
     trk::Wave lwave{};                      // light subpaths (TR_FLAG_BIDIRECTIONAL)
     trk::BidirWave bd{};
     uint32_t* d_lcounters = nullptr;
@@ -149,7 +153,7 @@ struct tr_ctx {
     cudaStream_t copy_stream = nullptr;
     // shadow rays of one depth beside the closest-hit rays of the next (tr_render_region)
     cudaStream_t shadow_stream = nullptr;
-    cudaStream_t lane_stream = nullptr, lane_shadow_stream = nullptr;   // second lane
+    cudaStream_t lane_stream[tri::kWaveLanes - 1]{}, lane_shadow_stream[tri::kWaveLanes - 1]{};
     std::vector<cudaEvent_t> dep_events;    // ordering events (no timing), reused in turn
     size_t next_dep = 0;
     float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows
@@ -189,9 +193,12 @@ struct tr_ctx {
         for (cudaEvent_t e : dep_events) cudaEventDestroy(e);
         dep_events.clear();
         if (shadow_stream) cudaStreamDestroy(shadow_stream);
-        if (lane_stream) cudaStreamDestroy(lane_stream);
-        if (lane_shadow_stream) cudaStreamDestroy(lane_shadow_stream);
-        shadow_stream = lane_stream = lane_shadow_stream = nullptr;
+        for (int k = 0; k < tri::kWaveLanes - 1; ++k) {
+            if (lane_stream[k]) cudaStreamDestroy(lane_stream[k]);
+            if (lane_shadow_stream[k]) cudaStreamDestroy(lane_shadow_stream[k]);
+            lane_stream[k] = lane_shadow_stream[k] = nullptr;
+        }
+        shadow_stream = nullptr;
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         if (ev0) cudaEventDestroy(ev0);
@@ -207,7 +214,7 @@ struct tr_ctx {
 namespace tri {
 
 void ensure_wave(tr_ctx* x, uint32_t capacity);
-void ensure_wave2(tr_ctx* x);
+void ensure_lane_wave(tr_ctx* x, int k);
 void ensure_guided(tr_ctx* x, uint32_t capacity);
 trk::Params make_params(tr_ctx* x);
 trg::GuideDev guide_dev(tr_guide* g);

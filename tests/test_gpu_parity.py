@@ -122,10 +122,10 @@ def test_long_film_matches_oracle(gpu, oracle_lib, sqrt_spp):
 
 
 @pytest.mark.parametrize("flags", [0, S.FLAG_TIME_SAMPLING])
-def test_batches_on_two_wave_lanes_match_oracle(gpu, oracle_lib, flags):
-    # 48 x 48 pixels x 1024 samples = 2.36 M paths: two pixel batches of the 2^21-slot wave,
-    # rendered on alternating wave buffers and streams
-    sc = S.cornell(width=48, height=48, time_bins=128, exposure=0.04, sqrt_spp=32, max_bounces=4)
+def test_batches_on_wave_lanes_match_oracle(gpu, oracle_lib, flags):
+    # 96 x 96 pixels x 1024 samples = 9.4 M paths: five pixel batches of the 2^21-slot wave,
+    # dealt in turn to the wave lanes (buffers and streams), so one lane takes two batches
+    sc = S.cornell(width=96, height=96, time_bins=128, exposure=0.04, sqrt_spp=32, max_bounces=4)
     sc.flags |= flags
     with gpu.Context(sc) as ctx:
         ctx.render(0, sc.spp)
