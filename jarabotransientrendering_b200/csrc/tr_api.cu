@@ -252,6 +252,19 @@ void ensure_lane_wave(tr_ctx* x, int k) {
     w.capacity = capacity;
 }
 
+// Lane k + 1's guided-vertex records (the training pool and its counters are shared: the
+// batches of all lanes fill it, each entry tagged with its batch).
+void ensure_lane_guided(tr_ctx* x, int k) {
+    const uint32_t capacity = x->wave.capacity;
+    if (x->lane_vrec_cap[k] >= capacity && x->lane_vrec[k]) return;
+    if (x->lane_vrec[k]) {
+        cudaFree(x->lane_vrec[k]);
+        x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), (void*)x->lane_vrec[k]), x->allocs.end());
+    }
+    x->lane_vrec[k] = x->alloc<uint4>((size_t)capacity * 5);
+    x->lane_vrec_cap[k] = capacity;
+}
+
 void ensure_guided(tr_ctx* x, uint32_t capacity) {
     if (x->gw_capacity >= capacity && x->gw.pool_cap == x->guide_pool && x->pool_state) return;
     auto drop = [&](void* p) {
@@ -403,15 +416,17 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     // Wave lanes: with more than one pixel batch and each pixel in one batch only (a single
     // sample chunk), consecutive batches alternate between kWaveLanes sets of wave buffers and
     // pairs of streams, so one batch's last, nearly empty depths run beside the next batch's
-    // first ones.  The batches share no pixels; the learned proposal (shared training pool)
-    // and light subpaths (one light wave) keep a single lane.
+    // first ones.  The batches share no pixels; with the learned proposal they share the
+    // training pool (entries tagged by batch).  Light subpaths (one light wave) keep a single
+    // lane.
     const uint64_t n_pix_batches = (win_pix + std::max<uint32_t>(1u, cap / (ns_chunk * ninc)) - 1) /
                                    std::max<uint32_t>(1u, cap / (ns_chunk * ninc));
-    const int lanes = (!guided && !bidir && ns_chunk >= ns_total)
+    const int lanes = (!bidir && ns_chunk >= ns_total)
                           ? (int)std::min<uint64_t>((uint64_t)kWaveLanes, n_pix_batches) : 1;
     uint32_t batch_no = 0;
     for (int k = 0; k + 1 < lanes; ++k) {
         ensure_lane_wave(x, k);
+        if (guided) ensure_lane_guided(x, k);
         if (!x->lane_stream[k]) TR_CUDA(cudaStreamCreateWithFlags(&x->lane_stream[k], cudaStreamNonBlocking));
         if (!x->lane_shadow_stream[k])
             TR_CUDA(cudaStreamCreateWithFlags(&x->lane_shadow_stream[k], cudaStreamNonBlocking));
@@ -429,6 +444,12 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             const cudaStream_t ls = lane ? x->lane_stream[lane - 1] : strm;
             const cudaStream_t lsh = lane ? x->lane_shadow_stream[lane - 1] : s_sh;
             if (lane) p.wave = x->lane_wave[lane - 1];
+            if (guided && lanes > 1) {
+                // several batches fill the training pool at once: each tags its entries
+                if (++x->guide_tag == 0) ++x->guide_tag;
+                p.guide.tag = x->guide_tag;
+                if (lane) p.guide.vrec = x->lane_vrec[lane - 1];
+            }
             auto tl = [&](int kind, auto&& launch) { timed_on(kind, ls, launch); };
             p.batch.win_x0 = x0; p.batch.win_y0 = y0; p.batch.win_w = win_w;
             p.batch.pix_begin = (uint32_t)pb; p.batch.npix = npix;

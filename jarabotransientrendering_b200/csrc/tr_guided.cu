@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params
                             G.pool_dir[3 * (size_t)k] = wi.x;
                             G.pool_dir[3 * (size_t)k + 1] = wi.y;
                             G.pool_dir[3 * (size_t)k + 2] = wi.z;
-                            G.pool_meta[k] = make_uint4(slot, (uint32_t)depth, __float_as_uint(avg3(f)), 0u);
+                            G.pool_meta[k] = make_uint4(slot, (uint32_t)depth, __float_as_uint(avg3(f)), G.tag);
                         }
                     }
                 }
@@ -316,14 +316,17 @@ __global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params
 // Training targets of this batch's pool entries: the luminance reaching the film through the
 // rest of the path (splat records of later bounces) relative to the throughput at the vertex,
 // i.e. an estimate of (incident radiance x f cos / sampling pdf) along the sampled direction.
-// pool_state[0] = entries filled, pool_state[1] = entries already given a target.
+// pool_state[0] = entries filled, pool_state[1] = entries already given a target.  A tagged
+// batch (batches in flight on several wave lanes fill the pool interleaved) scans every
+// filled entry and takes those carrying its tag.
 __global__ void k_train_gather(Params p, const uint32_t* pool_state) {
     const GuideWave& G = p.guide;
     const uint32_t end = min(pool_state[0], G.pool_cap);
-    const uint32_t begin = pool_state[1];
+    const uint32_t begin = G.tag ? 0u : pool_state[1];
     const size_t rs = p.wave.capacity;
     for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const uint4 meta = G.pool_meta[i];
+        if (meta.w != G.tag) continue;
         const uint32_t slot = meta.x, d = meta.y;
         const float lumf = __uint_as_float(meta.z);
         const uint32_t cnt = p.wave.rec_n[slot];
@@ -368,7 +371,7 @@ cudaError_t launch_guide(const Params& p, int depth, uint32_t* pool_state, cudaS
 
 cudaError_t launch_train_gather(const Params& p, uint32_t* pool_state, cudaStream_t s) {
     k_train_gather<<<256, 256, 0, s>>>(p, pool_state);
-    k_train_mark<<<1, 1, 0, s>>>(pool_state, p.guide.pool_cap);
+    if (!p.guide.tag) k_train_mark<<<1, 1, 0, s>>>(pool_state, p.guide.pool_cap);
     return cudaGetLastError();
 }
 

@@ -146,6 +146,9 @@ struct tr_ctx {
     // wavefront state
     trk::Wave wave{};
     trk::Wave lane_wave[tri::kWaveLanes - 1]{};  // further lanes of batches (share wave.stats)
+    uint4* lane_vrec[tri::kWaveLanes - 1]{};      // their guided-vertex records (learned proposal)
+    uint32_t lane_vrec_cap[tri::kWaveLanes - 1]{};
+    uint32_t guide_tag = 0;                       // last training-pool batch tag handed out
     trk::Wave lwave{};                      // light subpaths (TR_FLAG_BIDIRECTIONAL)
     trk::BidirWave bd{};
     uint32_t* d_lcounters = nullptr;
@@ -215,6 +218,7 @@ namespace tri {
 
 void ensure_wave(tr_ctx* x, uint32_t capacity);
 void ensure_lane_wave(tr_ctx* x, int k);
+void ensure_lane_guided(tr_ctx* x, int k);
 void ensure_guided(tr_ctx* x, uint32_t capacity);
 trk::Params make_params(tr_ctx* x);
 trg::GuideDev guide_dev(tr_guide* g);

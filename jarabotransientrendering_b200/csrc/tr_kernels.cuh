@@ -79,6 +79,9 @@ struct GuideWave {
     uint4* pool_meta;         // [pool_cap] slot, depth, throughput luminance (bits), unused
     uint32_t pool_cap;
     float keep_prob;          // probability that a guided vertex becomes a training sample
+    // batch tag written into pool_meta[k].w (0: untagged; the batch's entries are then the
+    // pool range filled since the previous gather)
+    uint32_t tag;
 };
 
 struct CameraDev {

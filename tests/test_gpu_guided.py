@@ -86,6 +86,23 @@ def test_guided_render_is_unbiased(gpu, train):
         assert st["train_steps"] >= 1 and np.isfinite(st["train_loss"])
 
 
+def test_guided_render_on_wave_lanes_is_unbiased_and_trains(gpu):
+    # 96 x 96 pixels x 1024 samples per render: five pixel batches dealt to the wave lanes,
+    # several of them filling the training pool at once (entries tagged by batch)
+    sc = guided_scene(96, 96, 128, 0.04)
+    K = 20
+    plain, _ = _films(gpu, sc, K, 1024)
+    g = gpu.Guide(seed=7)
+    try:
+        guided, st = _films(gpu, sc, K, 1024, guide=g, train_pool=65536)
+    finally:
+        g.close()
+    r = _compare(guided, plain, tile=16, window=16)
+    assert abs(r["energy_z"]) < 4.0 and abs(r["energy_rel"]) < 0.02, r
+    assert r["tile_max_z"] < 4.5 and r["window_max_z"] < 4.5, r
+    assert st["train_steps"] >= 1 and np.isfinite(st["train_loss"])
+
+
 def test_guided_training_updates_the_network(gpu):
     sc = guided_scene(64, 64, 128, 0.04)
     g = gpu.Guide(seed=9)
