@@ -469,6 +469,10 @@ def main():
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
                 "peak_source": peak_kind,
+                # the same algorithmic bytes over the whole timed step (shading, splat and gaps
+                # included): the survey's (N_closest B_closest + N_shadow B_shadow) / wall
+                "achieved_over_step": algo / (ms / 1e3) / 1e9,
+                "frac_over_step": algo / (ms / 1e3) / 1e9 / peak,
                 "traffic": ((DRAM_BYTES_PER_CLOSEST_QUERY * closest + DRAM_BYTES_PER_SHADOW_QUERY * shadow) / pairs)
                 if pairs else None,
                 "traffic_unit": "bytes per extend + shadow launch pair (ncu DRAM read + write per query x queries)",
