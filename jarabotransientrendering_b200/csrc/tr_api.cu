@@ -458,17 +458,23 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             TR_CUDA(cudaMemsetAsync(p.wave.counters, 0, trk::kCounters * sizeof(uint32_t), ls));
             tl(0, [&] { return trk::launch_raygen(p, ls); });
             if (bidir) {
-                // the light subpaths, on the light wave, from the light points raygen drew
+                // the light subpaths, on the light wave, from the light points raygen drew.
+                // They share nothing with the eye walks until the connections (own rays,
+                // queues, counters and vertex store), so they run on a third stream beside
+                // them; the connection passes wait for both.
+                if (!x->light_stream) TR_CUDA(cudaStreamCreateWithFlags(&x->light_stream, cudaStreamNonBlocking));
+                const cudaStream_t slt = x->light_stream;
+                TR_CUDA(order(ls, slt));
                 trk::Params pl = p;
                 pl.wave = x->lwave;
                 pl.wave.target = x->wave.target;
                 pl.wave.stats = x->wave.stats;
                 pl.wave.capacity = x->wave.capacity;
-                TR_CUDA(cudaMemsetAsync(pl.wave.counters, 0, trk::kCounters * sizeof(uint32_t), ls));
-                tl(0, [&] { return trk::launch_light_raygen(pl, ls); });
+                TR_CUDA(cudaMemsetAsync(pl.wave.counters, 0, trk::kCounters * sizeof(uint32_t), slt));
+                timed_on(0, slt, [&] { return trk::launch_light_raygen(pl, slt); });
                 for (uint32_t d = 0; d < x->bd.nvert; ++d) {
-                    tl(1, [&] { return trk::launch_extend(pl, (int)d, x->trace_grid, ls); });
-                    tl(2, [&] { return trk::launch_light_shade(pl, (int)d, ls); });
+                    timed_on(1, slt, [&] { return trk::launch_extend(pl, (int)d, x->trace_grid, slt); });
+                    timed_on(2, slt, [&] { return trk::launch_light_shade(pl, (int)d, slt); });
                 }
                 launches += 1 + 2ull * x->bd.nvert;
                 ext_l += x->bd.nvert;
@@ -489,6 +495,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 TR_CUDA(trk::launch_train_gather(p, x->pool_state, ls));
                 launches += 2;
             }
+            if (bidir) TR_CUDA(order(x->light_stream, ls));
             if (bidir && x->bd.nvert) {
                 // eye-light vertex connections, one eye depth at a time: rays with their samples
                 // into the connection queue, traced by k_shadow (records on blocked pairs),

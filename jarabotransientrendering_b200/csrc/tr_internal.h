@@ -157,6 +157,7 @@ struct tr_ctx {
     // shadow rays of one depth beside the closest-hit rays of the next (tr_render_region)
     cudaStream_t shadow_stream = nullptr;
     cudaStream_t lane_stream[tri::kWaveLanes - 1]{}, lane_shadow_stream[tri::kWaveLanes - 1]{};
+    cudaStream_t light_stream = nullptr;    // light subpaths beside the eye walks (bidirectional)
     std::vector<cudaEvent_t> dep_events;    // ordering events (no timing), reused in turn
     size_t next_dep = 0;
     float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows
@@ -201,7 +202,8 @@ struct tr_ctx {
             if (lane_shadow_stream[k]) cudaStreamDestroy(lane_shadow_stream[k]);
             lane_stream[k] = lane_shadow_stream[k] = nullptr;
         }
-        shadow_stream = nullptr;
+        if (light_stream) cudaStreamDestroy(light_stream);
+        shadow_stream = light_stream = nullptr;
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         if (ev0) cudaEventDestroy(ev0);
