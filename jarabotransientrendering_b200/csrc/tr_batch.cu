@@ -22,7 +22,9 @@ struct tr_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t shadow_stream = nullptr;   // shadow launches beside the next depth's extend
-    cudaEvent_t dep[4] = {};                // ordering events between the two, used in turn
+    // the second lane: every other batch, on its own wave and stream pair
+    cudaStream_t stream1 = nullptr, shadow_stream1 = nullptr;
+    cudaEvent_t dep[8] = {};                // ordering events between the streams, used in turn
     uint32_t next_dep = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<tr_ctx*> ctx;
@@ -32,8 +34,9 @@ struct tr_batch {
     trk::SceneSlot* d_scenes = nullptr;
     trk::BatchDesc* d_batches = nullptr;
     uint32_t batches_cap = 0;
-    uint32_t* d_cur = nullptr;
+    uint32_t* d_cur = nullptr;              // [lane]: index of the batch the lane is on
     trk::Wave wave{};
+    trk::Wave wave1{};                      // the second lane's (shares wave.stats)
     uint32_t max_bounces = 1, bvh_depth = 0;
     int trace_grid = 0;
     tr_batch_config cfg{1u << 21, 256, 1, 1};
@@ -43,6 +46,7 @@ struct tr_batch {
     float mix = 0.5f, lr = 1e-3f;
     uint32_t pool = 0;
     trk::GuideWave gw{};
+    uint4* vrec1 = nullptr;                 // the second lane's guided-vertex records
     uint32_t gw_capacity = 0;
     uint32_t* pool_state = nullptr;
 
@@ -152,10 +156,17 @@ Plan make_plan(const tr_batch* b, const uint64_t* s_begin, const uint32_t* s_cou
     return pl;
 }
 
+void ensure_lane(tr_batch* b, trk::Wave& w, uint32_t capacity, unsigned long long* stats);
+
 void ensure_batch_wave(tr_batch* b, uint32_t capacity) {
-    trk::Wave& w = b->wave;
-    if (w.capacity == capacity) return;
+    if (b->wave.capacity == capacity && b->wave1.capacity == capacity) return;
     b->drop_graph();
+    ensure_lane(b, b->wave, capacity, nullptr);
+    ensure_lane(b, b->wave1, capacity, b->wave.stats);
+}
+
+// one lane's wave buffers; `stats` null: allocate the statistics counters, else share them
+void ensure_lane(tr_batch* b, trk::Wave& w, uint32_t capacity, unsigned long long* stats) {
     b->drop(w.ray_o); b->drop(w.ray_d); b->drop(w.thr); b->drop(w.rng); b->drop(w.hit); b->drop(w.q[0]);
     b->drop(w.q[1]); b->drop(w.sh_o); b->drop(w.sh_d); b->drop(w.sh_L); b->drop(w.rec); b->drop(w.rec_n);
     w.ray_o = b->alloc<float4>(capacity);
@@ -177,7 +188,9 @@ void ensure_batch_wave(tr_batch* b, uint32_t capacity) {
     for (tr_ctx* x : b->ctx) tsm = tsm || (x->integ.flags & TR_FLAG_TIME_SAMPLING) != 0;
     w.target = tsm ? b->alloc<float4>(capacity) : nullptr;
     if (!w.counters) w.counters = b->alloc<uint32_t>(trk::kCounters);
-    if (!w.stats) {
+    if (stats) {
+        w.stats = stats;
+    } else if (!w.stats) {
         w.stats = b->alloc<unsigned long long>(8);
         TR_CUDA(cudaMemsetAsync(w.stats, 0, 8 * sizeof(unsigned long long), b->stream));
     }
@@ -190,6 +203,8 @@ void ensure_batch_guided(tr_batch* b, uint32_t capacity) {
     trk::GuideWave& g = b->gw;
     b->drop(g.vrec); b->drop(g.pool_feat); b->drop(g.pool_dir); b->drop(g.pool_w); b->drop(g.pool_meta);
     g.vrec = b->alloc<uint4>((size_t)capacity * 5);
+    b->drop(b->vrec1);
+    b->vrec1 = b->alloc<uint4>((size_t)capacity * 5);
     const uint32_t pc = std::max<uint32_t>(1u, b->pool);
     g.pool_feat = b->alloc<uint4>((size_t)pc * 8);
     g.pool_dir = b->alloc<float>((size_t)pc * 3);
@@ -200,14 +215,14 @@ void ensure_batch_guided(tr_batch* b, uint32_t capacity) {
     b->gw_capacity = capacity;
 }
 
-trk::Params batch_params(const tr_batch* b, const Plan& pl) {
+trk::Params batch_params(const tr_batch* b, const Plan& pl, int lane) {
     trk::Params p{};
-    p.wave = b->wave;
+    p.wave = lane ? b->wave1 : b->wave;
     p.bvh_depth = b->bvh_depth;
     p.max_bounces = b->max_bounces;
     p.multi.scenes = b->d_scenes;
     p.multi.batches = b->d_batches;
-    p.multi.cur = b->d_cur;
+    p.multi.cur = b->d_cur + lane;
     p.multi.nscenes = (uint32_t)b->ctx.size();
     p.multi.max_splat_blocks = std::max<uint32_t>(1u, pl.max_blocks);
     p.multi.shade_block = b->cfg.shade_block;
@@ -215,13 +230,15 @@ trk::Params batch_params(const tr_batch* b, const Plan& pl) {
         p.guide = b->gw;
         p.guide.net = guide_dev(b->guide);
         p.guide.err = guide_err(b->guide);
+        if (lane) p.guide.vrec = b->vrec1;
+        p.guide.tag = 1u;       // the lanes fill the pool at once: entries tagged by batch index
     }
     return p;
 }
 
 // `to` waits for the work enqueued on `from` so far (inside a capture: a graph dependency)
 void order(tr_batch* b, cudaStream_t from, cudaStream_t to) {
-    cudaEvent_t e = b->dep[b->next_dep++ % 4u];
+    cudaEvent_t e = b->dep[b->next_dep++ % 8u];
     TR_CUDA(cudaEventRecord(e, from));
     TR_CUDA(cudaStreamWaitEvent(to, e, 0));
 }
@@ -229,10 +246,9 @@ void order(tr_batch* b, cudaStream_t from, cudaStream_t to) {
 // the launches of one batch; `count` is incremented by the number of kernels.  The shadow
 // launch of depth d runs on the second stream beside the closest-hit launch of depth d + 1
 // (both only read what shade(d) wrote); shade(d + 1) refills the shadow queue and waits for it.
-void enqueue_batch(tr_batch* b, const trk::Params& p, cudaStream_t s, uint64_t& count) {
+void enqueue_batch(tr_batch* b, const trk::Params& p, cudaStream_t s, cudaStream_t sh, uint64_t& count) {
     const bool guided = b->guide != nullptr;
-    const cudaStream_t sh = b->shadow_stream;
-    TR_CUDA(cudaMemsetAsync(b->wave.counters, 0, trk::kCounters * sizeof(uint32_t), s));
+    TR_CUDA(cudaMemsetAsync(p.wave.counters, 0, trk::kCounters * sizeof(uint32_t), s));
     TR_CUDA(trk::launch_raygen(p, s));
     for (uint32_t d = 0; d < b->max_bounces; ++d) {
         TR_CUDA(trk::launch_extend(p, (int)d, b->trace_grid, s));
@@ -246,8 +262,17 @@ void enqueue_batch(tr_batch* b, const trk::Params& p, cudaStream_t s, uint64_t& 
     if (b->max_bounces) order(b, sh, s);
     if (guided && b->pool) { TR_CUDA(trk::launch_train_gather(p, b->pool_state, s)); count += 2; }
     TR_CUDA(trk::launch_splat(p, s));
-    TR_CUDA(trk::launch_advance(b->d_cur, s));
+    TR_CUDA(trk::launch_advance(p.multi.cur, 2u, s));   // this lane's next batch
     count += 3;
+}
+
+// Two batches, one per lane: lane 1 forks from the main stream and joins it again, so a
+// capture of the pair holds both as parallel branches.
+void enqueue_pair(tr_batch* b, const trk::Params& p0, const trk::Params& p1, uint64_t& count) {
+    order(b, b->stream, b->stream1);
+    enqueue_batch(b, p0, b->stream, b->shadow_stream, count);
+    enqueue_batch(b, p1, b->stream1, b->shadow_stream1, count);
+    order(b, b->stream1, b->stream);
 }
 
 tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_count) {
@@ -261,6 +286,9 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
     b->stats.train_steps = 0;
     b->stats.render_ms = 0.0;
     if (pl.batches.empty()) return TR_OK;
+    // batches run in pairs, one per lane; an odd count ends with an empty batch (no slots, no
+    // splat blocks: its kernels find no work)
+    if (pl.batches.size() % 2u) pl.batches.push_back(trk::BatchDesc{});
     ensure_batch_wave(b, b->cfg.capacity);
     const bool guided = b->guide != nullptr;
     if (guided) {
@@ -268,6 +296,8 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
         b->gw.keep_prob = b->pool ? std::min(1.0f, (float)b->pool / (1.5f * (float)pl.slots)) : 0.0f;
         b->gw.mix_prob = b->mix;
         TR_CUDA(cudaMemsetAsync(b->pool_state, 0, 2 * sizeof(uint32_t), s));
+        // entries are tagged by batch index: no tag of an earlier render may remain
+        if (b->pool) TR_CUDA(cudaMemsetAsync(b->gw.pool_meta, 0, (size_t)b->pool * sizeof(uint4), s));
     }
     if (pl.batches.size() > b->batches_cap) {
         b->drop_graph();
@@ -277,13 +307,15 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
     }
     TR_CUDA(cudaMemcpyAsync(b->d_batches, pl.batches.data(), pl.batches.size() * sizeof(trk::BatchDesc),
                             cudaMemcpyHostToDevice, s));
-    TR_CUDA(cudaMemsetAsync(b->d_cur, 0, sizeof(uint32_t), s));
-    const trk::Params p = batch_params(b, pl);
+    // lane 0 starts at batch 0, lane 1 at batch 1
+    TR_CUDA(cudaMemsetAsync(b->d_cur, 0, 2 * sizeof(uint32_t), s));
+    TR_CUDA(trk::launch_advance(b->d_cur + 1, 1u, s));
+    const trk::Params p0 = batch_params(b, pl, 0), p1 = batch_params(b, pl, 1);
 
     tr_batch::Shape shape;
     shape.capacity = b->cfg.capacity;
     shape.shade_block = b->cfg.shade_block;
-    shape.max_blocks = p.multi.max_splat_blocks;
+    shape.max_blocks = p0.multi.max_splat_blocks;
     shape.guided = guided ? 1u : 0u;
     shape.pool = b->pool;
     shape.mix = guided ? b->gw.mix_prob : 0.f;
@@ -291,20 +323,21 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
 
     uint64_t launches = 0;
     TR_CUDA(cudaEventRecord(b->ev0, s));
+    const size_t pairs = pl.batches.size() / 2;
     size_t done = 0;
     if (b->cfg.use_graph) {
         if (!(b->exec && shape == b->shape)) {
-            // new launch shape: the first batch runs directly (which also performs the kernels'
-            // one-time attribute calls outside any capture), then the sequence is captured for
-            // the remaining batches and later calls with the same shape
-            enqueue_batch(b, p, s, launches);
+            // new launch shape: the first pair runs directly (which also performs the kernels'
+            // one-time attribute calls outside any capture), then one pair is captured for the
+            // remaining pairs and later calls with the same shape
+            enqueue_pair(b, p0, p1, launches);
             done = 1;
             b->drop_graph();
-            if (done < pl.batches.size()) {
+            if (done < pairs) {
                 uint64_t n_capt = 0;
                 TR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 try {
-                    enqueue_batch(b, p, s, n_capt);
+                    enqueue_pair(b, p0, p1, n_capt);
                 } catch (...) {
                     cudaGraph_t g = nullptr;
                     cudaStreamEndCapture(s, &g);
@@ -316,14 +349,14 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
                 b->shape = shape;
             }
         }
-        // kernels per replay (the sequence of enqueue_batch)
-        const uint64_t per = 3 + 3ull * b->max_bounces + (guided ? b->max_bounces + (b->pool ? 2 : 0) : 0);
-        for (; done < pl.batches.size(); ++done) {
+        // kernels per replay (two batches of enqueue_batch)
+        const uint64_t per = 2 * (3 + 3ull * b->max_bounces + (guided ? b->max_bounces + (b->pool ? 2 : 0) : 0));
+        for (; done < pairs; ++done) {
             TR_CUDA(cudaGraphLaunch(b->exec, s));
             launches += per;
         }
     } else {
-        for (; done < pl.batches.size(); ++done) enqueue_batch(b, p, s, launches);
+        for (; done < pairs; ++done) enqueue_pair(b, p0, p1, launches);
     }
     TR_CUDA(cudaEventRecord(b->ev1, s));
     TR_CUDA(cudaEventSynchronize(b->ev1));
@@ -374,6 +407,8 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         TR_CUDA(cudaSetDevice(b->device));
         TR_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         TR_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream, cudaStreamNonBlocking));
+        TR_CUDA(cudaStreamCreateWithFlags(&b->stream1, cudaStreamNonBlocking));
+        TR_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream1, cudaStreamNonBlocking));
         for (cudaEvent_t& e : b->dep) TR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         TR_CUDA(cudaEventCreate(&b->ev0));
         TR_CUDA(cudaEventCreate(&b->ev1));
@@ -398,7 +433,7 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         // before the data lands, on a stream that does not order with this one)
         TR_CUDA(cudaMemcpyAsync(b->d_scenes, slots.data(), n * sizeof(trk::SceneSlot), cudaMemcpyHostToDevice, b->stream));
         TR_CUDA(cudaStreamSynchronize(b->stream));
-        b->d_cur = b->alloc<uint32_t>(1);
+        b->d_cur = b->alloc<uint32_t>(2);
         b->trace_grid = trk::trace_grid_size(b->device, b->bvh_depth, true);
         b->stats.device_bytes = b->bytes;
     } catch (const CudaError& e) {
@@ -406,6 +441,8 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         for (cudaEvent_t e : b->dep)
             if (e) cudaEventDestroy(e);
         if (b->shadow_stream) cudaStreamDestroy(b->shadow_stream);
+        if (b->stream1) cudaStreamDestroy(b->stream1);
+        if (b->shadow_stream1) cudaStreamDestroy(b->shadow_stream1);
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
@@ -543,6 +580,8 @@ tr_status tr_batch_destroy(tr_batch* b) {
     for (cudaEvent_t e : b->dep)
         if (e) cudaEventDestroy(e);
     if (b->shadow_stream) cudaStreamDestroy(b->shadow_stream);
+    if (b->stream1) cudaStreamDestroy(b->stream1);
+    if (b->shadow_stream1) cudaStreamDestroy(b->shadow_stream1);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return TR_OK;

@@ -129,6 +129,14 @@ __device__ __forceinline__ bool ggx_sample_fast(const GgxVertex& g, float sp, fl
 // accumulator row in registers and samples the direction.  Neither features nor mixtures touch
 // HBM.  Four CTAs per SM (50 KB shared memory, 64 TMEM columns each) overlap one CTA's MMA waits
 // with the others' gathers.
+// Training-pool tag of the current batch (0: untagged).  Single-scene launches carry theirs in
+// the parameters; multi-scene launches, replayed from one graph for every batch, use the batch
+// index + 1 (the pool's tags are cleared before each render).
+__device__ __forceinline__ uint32_t pool_tag(const Params& p) {
+    if (!p.guide.tag) return 0u;
+    return p.multi.scenes ? *p.multi.cur + 1u : p.guide.tag;
+}
+
 template <bool kMulti>
 __global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params p, int depth, uint32_t* pool_count) {
     const GuideWave& G = p.guide;
@@ -296,7 +304,7 @@ __global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params
                             G.pool_dir[3 * (size_t)k] = wi.x;
                             G.pool_dir[3 * (size_t)k + 1] = wi.y;
                             G.pool_dir[3 * (size_t)k + 2] = wi.z;
-                            G.pool_meta[k] = make_uint4(slot, (uint32_t)depth, __float_as_uint(avg3(f)), G.tag);
+                            G.pool_meta[k] = make_uint4(slot, (uint32_t)depth, __float_as_uint(avg3(f)), pool_tag(p));
                         }
                     }
                 }
@@ -322,11 +330,12 @@ __global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params
 __global__ void k_train_gather(Params p, const uint32_t* pool_state) {
     const GuideWave& G = p.guide;
     const uint32_t end = min(pool_state[0], G.pool_cap);
-    const uint32_t begin = G.tag ? 0u : pool_state[1];
+    const uint32_t tag = pool_tag(p);
+    const uint32_t begin = tag ? 0u : pool_state[1];
     const size_t rs = p.wave.capacity;
     for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const uint4 meta = G.pool_meta[i];
-        if (meta.w != G.tag) continue;
+        if (meta.w != tag) continue;
         const uint32_t slot = meta.x, d = meta.y;
         const float lumf = __uint_as_float(meta.z);
         const uint32_t cnt = p.wave.rec_n[slot];

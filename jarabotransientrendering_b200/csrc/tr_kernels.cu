@@ -917,9 +917,10 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
             atomicAdd(sd, (double)ax); atomicAdd(sd + 1, (double)ay); atomicAdd(sd + 2, (double)az);
         }
     }
-    // weight: one per camera sample; the block owns its pixels, so a plain update
+    // weight: one per camera sample (atomic: batches on different lanes can hold different
+    // sample chunks of the same pixels)
     if (bsel < 0)
-        for (uint32_t pl = threadIdx.x; pl < gp; pl += blockDim.x) film.weight[film_pixel(pl)] += (double)B.ns;
+        for (uint32_t pl = threadIdx.x; pl < gp; pl += blockDim.x) atomicAdd(&film.weight[film_pixel(pl)], (double)B.ns);
 }
 
 // Per-bounce film weights (MultibounceStreakCameraFilm.h:151-171 with StreakCameraFilm.h:139-160):
@@ -1496,9 +1497,9 @@ cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t 
 }
 
 // last node of a multi-scene batch: the next replay renders the next batch descriptor
-__global__ void k_advance(uint32_t* cur) { *cur += 1u; }
-cudaError_t launch_advance(uint32_t* cur, cudaStream_t s) {
-    k_advance<<<1, 1, 0, s>>>(cur);
+__global__ void k_advance(uint32_t* cur, uint32_t step) { *cur += step; }
+cudaError_t launch_advance(uint32_t* cur, uint32_t step, cudaStream_t s) {
+    k_advance<<<1, 1, 0, s>>>(cur, step);
     return cudaGetLastError();
 }
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit, void* out,

@@ -246,7 +246,7 @@ cudaError_t launch_build_tris(const float* vertices, const uint32_t* triangles, 
                               const uint32_t* order, uint32_t nt, float4* tris, float4* tri_ng, cudaStream_t s);
 // FP64 film sums -> FP32 (film streaming)
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
-cudaError_t launch_advance(uint32_t* cur, cudaStream_t s);
+cudaError_t launch_advance(uint32_t* cur, uint32_t step, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);
 // fused proposal inference + one-sample MIS direction sampling of the guided vertices of `depth`
