@@ -287,3 +287,26 @@ def test_reference_shaped_api(gpu, tmp_path):
     assert np.allclose(film.streak, f["streak"], rtol=1e-4, atol=1e-9)
     with pytest.raises(RuntimeError):
         gpu.TransientRenderer().render(None, w, None, cam, film, sampler)
+
+
+def test_render_on_a_caller_stream_with_wave_lanes(gpu):
+    # tr_set_stream: the lanes fork from the caller's stream and join it again before the call
+    # returns; the film equals a render on the context's own stream
+    import torch
+    from jarabotransientrendering_b200 import _abi
+    sc = S.cornell(width=96, height=96, time_bins=128, exposure=0.04, sqrt_spp=32, max_bounces=4)
+    with gpu.Context(sc) as ctx:
+        ctx.render(0, sc.spp)
+        ref = ctx.film()
+    stream = torch.cuda.Stream()
+    busy = torch.empty(1 << 28, dtype=torch.uint8, device="cuda")
+    with gpu.Context(sc) as ctx:
+        _abi.check(_abi.lib().tr_set_stream(ctx.h, stream.cuda_stream))
+        with torch.cuda.stream(stream):
+            busy.fill_(1)                      # work queued ahead of the render on that stream
+        ctx.render(0, sc.spp)
+        assert stream.query()                  # nothing of the render is left in flight
+        got = ctx.film()
+    assert (got["weight"] == ref["weight"]).all()
+    assert ((got["streak"] != 0) == (ref["streak"] != 0)).all()
+    assert np.allclose(got["streak"], ref["streak"], rtol=RTOL_TILE, atol=1e-12)
