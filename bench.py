@@ -412,7 +412,9 @@ def main():
     ctx = T.Context(sc, device=local)
     stream = torch.cuda.Stream()
     T._abi.check(T._abi.lib().tr_set_stream(ctx.h, stream.cuda_stream))
-    T._abi.check(T._abi.lib().tr_set_profiling(ctx.h, 1))
+    # per-kernel events around every launch of the timed renders, read out once after the timed
+    # region (profiling 2: the read-out costs host time, not device time)
+    T._abi.check(T._abi.lib().tr_set_profiling(ctx.h, 2))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
 
     for _ in range(args.warmup):
@@ -428,27 +430,24 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     kern = {"extend_ms": 0.0, "shade_ms": 0.0, "shadow_ms": 0.0, "splat_ms": 0.0, "raygen_ms": 0.0, "trace_ms": 0.0}
-    launches = 0
-    ext_launches = 0
-    sh_launches = 0
-    st0 = ctx.stats()
+    st0 = ctx.stats()                     # also drops the warm-up renders' pending times
     ev0.record(stream)
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         ctx.render(0, spp)
-        st = ctx.stats()
-        for k in kern:
-            kern[k] += st[k]
-        launches += st["kernel_launches"]
-        ext_launches += st["extend_launches"]
-        sh_launches += st["shadow_launches"]
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    st1 = ctx.stats()
+    st1 = ctx.stats()                     # per-kernel sums over the timed renders
+    for k in kern:
+        kern[k] = st1[k]
+    # launches per render are the same in every step
+    launches = st1["kernel_launches"] * args.steps
+    ext_launches = st1["extend_launches"] * args.steps
+    sh_launches = st1["shadow_launches"] * args.steps
     closest = st1["closest_rays"] - st0["closest_rays"]
     shadow = st1["shadow_rays"] - st0["shadow_rays"]
     ms = max_over_ranks(ms, dist, "cuda")

@@ -199,7 +199,8 @@ typedef struct tr_stats {
     uint32_t bvh_depth;
     uint64_t device_bytes;     /* device memory held by the context                          */
     uint64_t kernel_launches;  /* kernels launched by the last tr_render call                */
-    /* per-kernel device time of the last tr_render call (only with tr_set_profiling(ctx,1)),
+    /* per-kernel device time of the last tr_render call (tr_set_profiling(ctx,1)) or of the
+     * renders since the previous tr_stats_get (tr_set_profiling(ctx,2)),
      * measured with CUDA events around each launch on the stream it runs on.  Shadow launches
      * run on a second stream beside the next depth's closest-hit launch, so extend_ms and
      * shadow_ms overlap; trace_ms below is the time either of them was running.              */
@@ -390,7 +391,10 @@ tr_status tr_batch_destroy(tr_batch* b);
  * NULL restores the context's own stream).  The stream must belong to the context's device. */
 tr_status tr_set_stream(tr_ctx* ctx, void* stream);
 
-/* Enables (1) or disables (0) per-kernel CUDA-event timing inside tr_render. */
+/* Per-kernel CUDA-event timing inside tr_render: 0 off; 1 on, the times of each render read out
+ * when it ends (tr_stats: the last render's); 2 on, read out at the next tr_stats_get (tr_stats:
+ * the sums over the renders since the previous read), which keeps the read-out, about 1.5 us of
+ * host time per timed launch, out of the renders.                                          */
 tr_status tr_set_profiling(tr_ctx* ctx, int on);
 tr_status tr_destroy(tr_ctx* ctx);
 

@@ -219,6 +219,38 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
     w.capacity = capacity;
 }
 
+// Per-kind kernel times of the pending timed launches and the union of the traversal (extend,
+// shadow) launch intervals, into the context's statistics; one cudaEventElapsedTime per event,
+// relative to the first pending event.  Clears the pending launches.
+cudaError_t prof_readout(tr_ctx* x) {
+    if (x->prof_marks.empty()) { x->prof_next = 0; return cudaSuccess; }
+    std::vector<float> t(x->prof_next, 0.f);
+    for (size_t i = 0; i < x->prof_next; ++i) {
+        const cudaError_t e = cudaEventElapsedTime(&t[i], x->prof_events[0], x->prof_events[i]);
+        if (e != cudaSuccess) return e;
+    }
+    double kms[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<std::pair<float, float>> trace_iv;
+    for (const tr_ctx::ProfMark& m : x->prof_marks) {
+        kms[m.kind] += t[m.ev + 1] - t[m.ev];
+        if (m.kind == 1 || m.kind == 3) trace_iv.push_back({t[m.ev], t[m.ev + 1]});
+    }
+    std::sort(trace_iv.begin(), trace_iv.end());
+    double trace_ms = 0.0;
+    for (size_t i = 0; i < trace_iv.size();) {
+        float a = trace_iv[i].first, b = trace_iv[i].second;
+        for (++i; i < trace_iv.size() && trace_iv[i].first <= b; ++i) b = std::max(b, trace_iv[i].second);
+        trace_ms += b - a;
+    }
+    x->stats.trace_ms = trace_ms;
+    x->stats.raygen_ms = kms[0]; x->stats.extend_ms = kms[1]; x->stats.shade_ms = kms[2];
+    x->stats.shadow_ms = kms[3]; x->stats.splat_ms = kms[4];
+    x->stats.guide_ms = kms[5];
+    x->prof_marks.clear();
+    x->prof_next = 0;
+    return cudaSuccess;
+}
+
 // Lane k + 1's buffers: the per-slot arrays of the first wave at its capacity, its own queue
 // counters, the first wave's statistics counters.
 void ensure_lane_wave(tr_ctx* x, int k) {
@@ -353,10 +385,12 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     // samples per pixel per batch, and pixels per batch
     uint32_t ns_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(ns_total, cap / ninc));
     cudaStream_t strm = x->s();
-    // per-kernel timing: an event before and after each launch, kind-tagged
-    struct Mark { int kind; size_t ev; };
-    std::vector<Mark> marks;
-    size_t next_ev = 0;
+    // per-kernel timing: an event before and after each launch, kind-tagged.  Read out at the
+    // end of the render (profiling 1) or at tr_stats_get (profiling 2; a long series of renders
+    // is read out once 2^16 events are pending)
+    if (x->profiling == 2 && x->prof_next > (1u << 16)) TR_CUDA(prof_readout(x));
+    if (x->profiling != 2) { x->prof_marks.clear(); x->prof_next = 0; }
+    size_t& next_ev = x->prof_next;
     auto ev_get = [&]() -> cudaEvent_t {
         if (next_ev == x->prof_events.size()) {
             cudaEvent_t e;
@@ -371,7 +405,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         TR_CUDA(cudaEventRecord(ev_get(), st));
         TR_CUDA(launch());
         TR_CUDA(cudaEventRecord(ev_get(), st));
-        marks.push_back({kind, a});
+        x->prof_marks.push_back({kind, a});
     };
     // `to` waits for the work queued on `from` so far
     auto order = [&](cudaStream_t from, cudaStream_t to) -> cudaError_t {
@@ -571,30 +605,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     TR_CUDA(cudaEventSynchronize(x->ev1));
     float ms = 0.f;
     TR_CUDA(cudaEventElapsedTime(&ms, x->ev0, x->ev1));
-    double kms[6] = {0, 0, 0, 0, 0, 0};
-    std::vector<std::pair<float, float>> trace_iv;      // extend / shadow intervals after ev0
-    for (const Mark& m : marks) {
-        float e = 0.f;
-        TR_CUDA(cudaEventElapsedTime(&e, x->prof_events[m.ev], x->prof_events[m.ev + 1]));
-        kms[m.kind] += e;
-        if (m.kind == 1 || m.kind == 3) {
-            float a = 0.f, b = 0.f;
-            TR_CUDA(cudaEventElapsedTime(&a, x->ev0, x->prof_events[m.ev]));
-            TR_CUDA(cudaEventElapsedTime(&b, x->ev0, x->prof_events[m.ev + 1]));
-            trace_iv.push_back({a, b});
-        }
-    }
-    std::sort(trace_iv.begin(), trace_iv.end());
-    double trace_ms = 0.0;
-    for (size_t i = 0; i < trace_iv.size();) {
-        float a = trace_iv[i].first, b = trace_iv[i].second;
-        for (++i; i < trace_iv.size() && trace_iv[i].first <= b; ++i) b = std::max(b, trace_iv[i].second);
-        trace_ms += b - a;
-    }
-    x->stats.trace_ms = trace_ms;
-    x->stats.raygen_ms = kms[0]; x->stats.extend_ms = kms[1]; x->stats.shade_ms = kms[2];
-    x->stats.shadow_ms = kms[3]; x->stats.splat_ms = kms[4];
-    x->stats.guide_ms = kms[5];
+    if (x->profiling == 1) TR_CUDA(prof_readout(x));
     x->stats.kernel_launches = launches;
     x->stats.extend_launches = ext_l;
     x->stats.shadow_launches = sh_l;
@@ -1063,6 +1074,11 @@ tr_status tr_trace_rays(tr_ctx* x, const float* rays, uint32_t n, int any_hit, t
 
 tr_status tr_stats_get(tr_ctx* x, tr_stats* out) {
     if (!x || !out) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    if (x->profiling == 2 && !x->prof_marks.empty()) {
+        cudaSetDevice(x->device);
+        const cudaError_t e = prof_readout(x);
+        if (e != cudaSuccess) return fail(TR_ERR_CUDA, cudaGetErrorString(e));
+    }
     *out = x->stats;
     out->device_bytes = x->bytes;
     return TR_OK;
@@ -1438,7 +1454,10 @@ tr_status tr_set_stream(tr_ctx* x, void* stream) {
 
 tr_status tr_set_profiling(tr_ctx* x, int on) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
-    x->profiling = on != 0;
+    if (on < 0 || on > 2) return fail(TR_ERR_INVALID_ARGUMENT, "profiling must be 0, 1 or 2");
+    x->profiling = on;
+    x->prof_marks.clear();          // launches timed under another setting are dropped
+    x->prof_next = 0;
     return TR_OK;
 }
 

@@ -181,8 +181,11 @@ struct tr_ctx {
     float last_train_loss = 0.0f;
     uint32_t train_steps = 0;
     cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null
-    bool profiling = false;
+    int profiling = 0;                    // 0 off, 1 read out per render, 2 read out at tr_stats_get
     std::vector<cudaEvent_t> prof_events; // pool of timing events
+    struct ProfMark { int kind; size_t ev; };
+    std::vector<ProfMark> prof_marks;     // launches timed and not read out yet
+    size_t prof_next = 0;                 // events of prof_events in use
     cudaStream_t s() const { return user_stream ? user_stream : stream; }
 
     template <class T>

@@ -310,3 +310,31 @@ def test_render_on_a_caller_stream_with_wave_lanes(gpu):
     assert (got["weight"] == ref["weight"]).all()
     assert ((got["streak"] != 0) == (ref["streak"] != 0)).all()
     assert np.allclose(got["streak"], ref["streak"], rtol=RTOL_TILE, atol=1e-12)
+
+
+def test_deferred_profiling_sums_the_renders_since_the_last_read(gpu):
+    # tr_set_profiling(ctx, 2): the events of every timed launch are read out at tr_stats_get,
+    # as sums over the renders since the previous read
+    from jarabotransientrendering_b200 import _abi
+    sc = S.cornell(width=96, height=96, time_bins=128, exposure=0.04, sqrt_spp=32, max_bounces=4)
+    keys = ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "splat_ms", "trace_ms")
+    with gpu.Context(sc) as ctx:
+        ctx.render(0, sc.spp)                                   # allocations, lanes
+        _abi.check(_abi.lib().tr_set_profiling(ctx.h, 1))
+        one = []
+        for _ in range(3):
+            ctx.render(0, sc.spp)
+            one.append(ctx.stats())
+        _abi.check(_abi.lib().tr_set_profiling(ctx.h, 2))
+        ctx.render(0, sc.spp)
+        ctx.render(0, sc.spp)
+        two = ctx.stats()
+        again = ctx.stats()                                     # nothing pending: unchanged
+    per = {k: np.median([s[k] for s in one]) for k in keys}
+    for k in keys:
+        assert per[k] > 0 and 1.2 * per[k] < two[k] < 3.0 * per[k], (k, per[k], two[k])
+        assert again[k] == two[k]
+    assert two["trace_ms"] <= two["extend_ms"] + two["shadow_ms"]
+    with gpu.Context(sc) as ctx:
+        with pytest.raises(gpu.TransientError, match="profiling"):
+            _abi.check(_abi.lib().tr_set_profiling(ctx.h, 3))
