@@ -469,7 +469,7 @@ def main():
                 "frac": achieved / peak if achieved else None,
                 "peak_source": peak_kind,
                 # the same algorithmic bytes over the whole timed step (shading, splat and gaps
-                # included): the survey's (N_closest B_closest + N_shadow B_shadow) / wall
+                # included): (N_closest B_closest + N_shadow B_shadow) / wall time
                 "achieved_over_step": algo / (ms / 1e3) / 1e9,
                 "frac_over_step": algo / (ms / 1e3) / 1e9 / peak,
                 "traffic": ((DRAM_BYTES_PER_CLOSEST_QUERY * closest + DRAM_BYTES_PER_SHADOW_QUERY * shadow) / pairs)
