@@ -545,7 +545,7 @@ def main():
                       "phases_per_step": ph,
                       "fp64_film": {"value": whole_job_rate(paths_per_step, world, et64), "d2h_bytes_per_step": int(d2h64),
                                     "ms_per_step": et64 * 1e3, "phases": ph64},
-                      "includes": "tr_create (scene H2D from pinned memory + host BVH build + film alloc), "
+                      "includes": "tr_create (scene H2D from pinned memory + device BVH build + film alloc), "
                                   "tr_render_film (render with the film streamed into pinned host memory as "
                                   "pixel rows complete), tr_destroy"}
     else:
