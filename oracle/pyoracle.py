@@ -87,6 +87,7 @@ def lib():
         L.orc_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p,
                                 C.c_void_p]
         L.orc_trace_moller.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_moller_terms.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32] + [C.c_void_p] * 4
         L.orc_render_ex.restype = C.c_int
         L.orc_render_ex.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                     C.c_uint32, C.c_int] + [C.c_void_p] * 10
@@ -187,6 +188,16 @@ class Oracle:
         rays = np.ascontiguousarray(rays, np.float32)
         out = np.zeros(len(rays), HIT_DTYPE)
         lib().orc_trace_moller(self.h, rays.ctypes.data, len(rays), out.ctypes.data)
+        return out
+
+    def moller_terms(self, rays, ids):
+        """Embree's Moeller-Trumbore terms of ray i against triangle ids[i]: dict of float32
+        arrays T, absden, u, v (unnormalised; the distance is T / absden)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        out = {k: np.zeros(len(rays), np.float32) for k in ("T", "absden", "u", "v")}
+        lib().orc_moller_terms(self.h, rays.ctypes.data, ids.ctypes.data, len(rays),
+                               *(out[k].ctypes.data for k in ("T", "absden", "u", "v")))
         return out
 
     def render(self, sample_begin=0, sample_count=None, window=None, nthreads=1,

@@ -4,7 +4,7 @@
  * Provides the compile-time configuration of src/bunnykiller.h:26-78 (DIM 3, RGB spectrum,
  * float Real, MAX_BPT_VERTICES 64, _SIGMA_VISIBILITY_ 1e-5) and defines its include guard,
  * so the reference headers compile with their own triangle/BVH backend instead of the
- * hard-wired _USE_EMBREE_ (vendored Embree cannot be built without CMake-generated headers).
+ * hard-wired _USE_EMBREE_: the ref_render_bvh build of oracle/ref_harness.cpp.
  */
 #ifndef _GLOBALS_H_
 #define _GLOBALS_H_

@@ -5,26 +5,30 @@
  * reference's header sources where they lie; it is the statistical pin of the CPU oracle and
  * the CPU baseline of bench.py.  Nothing in the product links it.
  *
- * Everything on the sampling path is the reference's code: World (non-Embree backend),
- * PinholeCamera, StratifiedSampler, BidirectionalPathTracing in path-tracing-only steady-state
- * mode, UberMaterial+Lambertian, PointLightSource, RectangularAreaLightSource,
- * HomogeneousMedium with Henyey-Greenstein / isotropic phase, TransientRenderer::render.
- * Set-up follows main() (src/bunnykiller.cpp:1504-1827).  Two pieces are the harness's own:
- *   - triangles are the reference's smooth Triangle (src/Geometry/Primitives/3D/Triangle.h)
- *     with all three shading normals = the Embree geometric normal
- *     normalize(cross(p2-p0, p1-p0)) (src/RayTracing/World.h:449,514-540), placed in the
- *     reference's BVH (src/Geometry/Aggregate/BVH.h), because the Embree backend needs
- *     CMake-generated headers;
- *   - the film is a StreakCameraFilm whose add_samples (StreakCameraFilm.h:139-192) is
- *     overridden to accumulate the same (pixel, bin) sums in double precision into one
- *     buffer instead of averaging and writing RGBE scanlines; with `filmopts U N` it also
- *     applies the camera unwarp of StreakCameraFilm.h:167 (sample time minus the record's
- *     camera distance) and, for N > 0, routes the samples to N per-bounce films with the
- *     weights of MultibounceStreakFilm::add_samples (MultibounceStreakCameraFilm.h:151-171),
- *     the main steady image then being the base Film's (all samples, Film.h:263-284);
- *     `mode transient` selects the time-sampling mode (-time-sampling, bunnykiller.cpp:1337-1345,
- *     1754, 1812-1817); `bidir 1` turns off path-tracing-only (light subpaths and vertex
- *     connections; BidirectionalPathTracing::set_path_tracing_only, reachable through the API).
+ * Everything on the sampling path is the reference's code: World, PinholeCamera,
+ * StratifiedSampler, BidirectionalPathTracing in path-tracing-only steady-state mode,
+ * UberMaterial+Lambertian, PointLightSource, RectangularAreaLightSource, HomogeneousMedium with
+ * Henyey-Greenstein / isotropic phase, TransientRenderer::render.  Set-up follows main()
+ * (src/bunnykiller.cpp:1504-1827).  Two builds:
+ *   - ref_render: the shipped configuration (src/bunnykiller.h defines _USE_EMBREE_).  Every
+ *     mesh is written to an OBJ file and loaded by World::add_triangle_mesh
+ *     (src/RayTracing/World.h:209-541), as `-name-mesh FILE -lambertian ...` does, and rays are
+ *     cast by the vendored Embree 2.17.4 (compiled by oracle/embree.mk);
+ *   - ref_render_bvh: the reference's own non-Embree backend (ref_globals.h pre-defines the
+ *     src/bunnykiller.h include guard): triangles are the smooth Triangle
+ *     (src/Geometry/Primitives/3D/Triangle.h) with all three shading normals = the Embree
+ *     geometric normal normalize(cross(p2-p0, p1-p0)) (World.h:449,514-540), placed in the
+ *     reference's BVH (src/Geometry/Aggregate/BVH.h).
+ * The one piece that is the harness's own: the film is a StreakCameraFilm whose add_samples
+ * (StreakCameraFilm.h:139-192) is overridden to accumulate the same (pixel, bin) sums in double
+ * precision into one buffer instead of averaging and writing RGBE scanlines; with `filmopts U N`
+ * it also applies the camera unwarp of StreakCameraFilm.h:167 (sample time minus the record's
+ * camera distance) and, for N > 0, routes the samples to N per-bounce films with the weights of
+ * MultibounceStreakFilm::add_samples (MultibounceStreakCameraFilm.h:151-171), the main steady
+ * image then being the base Film's (all samples, Film.h:263-284); `mode transient` selects the
+ * time-sampling mode (-time-sampling, bunnykiller.cpp:1337-1345, 1754, 1812-1817); `bidir 1`
+ * turns off path-tracing-only (light subpaths and vertex connections;
+ * BidirectionalPathTracing::set_path_tracing_only, reachable through the API).
  *
  * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
  *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
@@ -32,7 +36,7 @@
  *   bounce films bstreak [N][H][W][T][3], bsteady [N][H][W][3], bweight [N][H][W], then with
  *   components (`filmopts U N C`, C != 0) depth [H][W], positions [H][W][3], normals [H][W][3]
  *   summed from each camera sample's record (Film::add_components, Film.h:127-145).
- *   Prints one JSON line with paths, seconds and paths/s on stdout.
+ *   Prints one JSON line with paths, seconds and paths/s on stderr.
  */
 #include <chrono>
 #include <cmath>
@@ -43,15 +47,18 @@
 #include <sstream>
 #include <string>
 #include <vector>
+#include <unistd.h>
 
 #include "Utils/RandomNumbers.h"
 #include "Camera/PinholeCamera.h"
 #include "RayTracing/World.h"
 #include "Renderer/TransientRenderer.h"
 #include "Film/StreakCameraFilm.h"
+#ifndef _USE_EMBREE_
 #include "Geometry/Primitives/3D/Triangle.h"
 #include "Geometry/Aggregate/BVH.h"
 #include "Geometry/ObjectPointer.h"
+#endif
 #include "Material/UberMaterial.h"
 #include "Material/Reflectance/Lambertian.h"
 #include "LightSource/PointLightSource.h"
@@ -159,7 +166,14 @@ int main(int argc, char** argv) {
     int med_on = 0; float sa[3] = {0, 0, 0}, ss[3] = {0, 0, 0}, g = 0;
     std::vector<UberMaterial3D*> mats;
     World<3, Radiance> w;
+#ifdef _USE_EMBREE_
+    char tmpl[] = "/tmp/tr_ref_render_XXXXXX";
+    if (!mkdtemp(tmpl)) fail("cannot create a temporary directory");
+    const std::string objdir(tmpl);
+    std::vector<std::string> objs;
+#else
     BVH<Object3DPointer, 3>* bvh = new BVH<Object3DPointer, 3>();
+#endif
     std::vector<std::string> light_lines;
     while (in >> tag) {
         if (tag == "film") { in >> W >> H >> T >> exposure >> offset; }
@@ -181,6 +195,19 @@ int main(int argc, char** argv) {
         else if (tag == "mesh") {
             size_t nv, nt; unsigned m; in >> nv >> nt >> m;
             if (m >= mats.size()) fail("bad material index");
+#ifdef _USE_EMBREE_
+            /* the CLI's `-name-mesh FILE -lambertian ...` (bunnykiller.cpp:328-337): an OBJ file
+               loaded by World::add_triangle_mesh; %.9g round-trips every float */
+            std::string path = objdir + "/mesh" + std::to_string(objs.size()) + ".obj";
+            FILE* f = fopen(path.c_str(), "w");
+            if (!f) fail("cannot write an OBJ file");
+            for (size_t i = 0; i < nv; ++i) { float a, b, c; in >> a >> b >> c; fprintf(f, "v %.9g %.9g %.9g\n", a, b, c); }
+            for (size_t i = 0; i < nt; ++i) { size_t a, b, c; in >> a >> b >> c; fprintf(f, "f %zu %zu %zu\n", a + 1, b + 1, c + 1); }
+            fclose(f);
+            w.add_triangle_mesh(path, mats[m]);
+            unlink(path.c_str());
+            objs.push_back(path);
+#else
             std::vector<Vector3f> v(nv);
             for (size_t i = 0; i < nv; ++i) { float a, b, c; in >> a >> b >> c; v[i] = Vector3f(a, b, c); }
             for (size_t i = 0; i < nt; ++i) {
@@ -194,6 +221,7 @@ int main(int argc, char** argv) {
                                              Vector3(p2[0], p2[1], p2[2]), ng, uv0, mats[m]);
                 bvh->add_primitive(Object3DPointer(tri));
             }
+#endif
         } else if (tag == "end") break;
         else fail("unknown tag");
     }
@@ -218,8 +246,12 @@ int main(int argc, char** argv) {
             w.set_medium(new HomogeneousMedium<3, PhaseFunction::HenyeyGreenstein<3>>(a, s,
                          PhaseFunction::HenyeyGreenstein<3>(g, 0.)));
     }
+#ifdef _USE_EMBREE_
+    rmdir(objdir.c_str());
+#else
     bvh->freeze();
     w.add_object(Object3DPointer(bvh));
+#endif
     w.set_background(Spectrum(0.));
     w.freeze();
 

@@ -20,7 +20,8 @@ def ref_available():
     return os.path.exists(REF_BIN)
 
 
-REF_SRC = "/root/reference/src"     # where the reference sources lie in the build container
+# where the reference sources lie: $TR_REFERENCE_SRC, else the build container's location
+REF_SRC = os.environ.get("TR_REFERENCE_SRC", "/root/reference/src")
 
 
 def sources_available(ref_src=REF_SRC):
@@ -28,9 +29,12 @@ def sources_available(ref_src=REF_SRC):
 
 
 def build_ref(ref_src=REF_SRC):
-    """Compile the harness from the reference sources (only where those sources exist)."""
+    """Compile the reference programs (oracle/_ref: the renderer with Embree and with the
+    reference's own BVH, the hit harness) from the reference sources, only where those sources
+    exist; the first build compiles the vendored Embree (about three minutes on eight cores)."""
     if os.path.isdir(ref_src):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_SRC={ref_src}"])
+        subprocess.check_call(["make", "-s", "-j", str(os.cpu_count() or 4), "-C", HERE, "ref",
+                               f"REF_SRC={ref_src}"])
     return ref_available()
 
 

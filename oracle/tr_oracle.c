@@ -514,6 +514,32 @@ void orc_trace_moller(const orc_ctx* x, const float* rays, uint32_t n, orc_hit* 
     }
 }
 
+/* Embree's Moeller-Trumbore terms for ray i against triangle ids[i] (same operations as the
+ * leaf loop above, triangle_intersector_moeller.h:66-104): the unnormalised distance T, |den|
+ * and the edge terms U, V, so that a caller can form the exact quotients T/|den| etc. and
+ * bound the reference's Newton-refined reciprocal against them.  ids[i] = ~0u gives zeros. */
+void orc_moller_terms(const orc_ctx* x, const float* rays, const uint32_t* ids, uint32_t n,
+                      float* T_out, float* absden_out, float* U_out, float* V_out) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* q = &rays[8 * i];
+        const uint32_t id = ids[i];
+        T_out[i] = absden_out[i] = U_out[i] = V_out[i] = 0.0f;
+        if (id >= x->nt) continue;
+        v3 o = mk(q[0], q[1], q[2]), d = mk(q[4], q[5], q[6]);
+        v3 v0 = x->p0[id];
+        v3 e1 = sub(v0, x->p1[id]), e2 = sub(x->p2[id], v0);
+        v3 Ng = fcross(e1, e2);
+        v3 C = sub(v0, o);
+        v3 R = fcross(d, C);
+        float den = fdot(Ng, d);
+        uint32_t sgn = as_u(den) & 0x80000000u;
+        T_out[i] = as_f(as_u(fdot(Ng, C)) ^ sgn);
+        absden_out[i] = fabsf(den);
+        U_out[i] = as_f(as_u(fdot(R, e2)) ^ sgn);
+        V_out[i] = as_f(as_u(fdot(R, e1)) ^ sgn);
+    }
+}
+
 /* ------------------------------------------------------------------------------------------
  * The transient path tracer.
  * ---------------------------------------------------------------------------------------- */

@@ -88,6 +88,9 @@ void orc_trace(const orc_ctx* ctx, const float* rays, uint32_t n, int any_hit, o
  * (kernels/geometry/triangle_intersector_moeller.h:66-104, t = T * rcp(absDen) with one
  * Newton step as in common/simd/vfloat8_avx.h:242-254). */
 void orc_trace_moller(const orc_ctx* ctx, const float* rays, uint32_t n, orc_hit* out);
+/* Embree's Moeller terms (T, |den|, U, V) of ray i against triangle ids[i]. */
+void orc_moller_terms(const orc_ctx* ctx, const float* rays, const uint32_t* ids, uint32_t n,
+                      float* T, float* absden, float* U, float* V);
 
 /* Renders camera samples [sample_begin, sample_begin+sample_count) of the pixel window and
  * ADDS them into full-frame buffers (any may be NULL):
