@@ -121,43 +121,64 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference(scene, rows_per_proc, procs):
-    """Times the reference renderer (oracle/_ref/ref_render, the reference's own integrator and
-    film built from its sources) on host cores: `procs` processes over disjoint scanlines."""
+def _spread_rows(height, procs, per_proc):
+    """Scanlines for `procs` processes x `per_proc` scanlines each, spread evenly over the
+    image; process p's j-th scanline is sample j * procs + p (so every step's scanlines span the
+    whole image).  Rows repeat only when more are asked for than the image has."""
+    n = procs * per_proc
+    return [[int(((j * procs + p) + 0.5) * height / n) % height for j in range(per_proc)] for p in range(procs)]
+
+
+def cpu_reference(scene, procs, warmup, steps, binary=None, what="reference integrator and streak film, "
+                  "rays cast by its vendored Embree 2.17.4"):
+    """Times the reference renderer (oracle/_ref/ref_render: the reference's own World + Embree,
+    integrator and streak film, built from its sources) on `procs` host processes at once.
+    One step = every process renders one scanline (512 px x 256 spp, streak splat on; the
+    scanlines of a step are spread over the image); the first `warmup` steps are untimed.
+    Step time = the slowest process's render call for that step's scanline (scene parsing and
+    the Embree build happen once per process, before the timed loop, as in the reference's own
+    `Total time`).  Without the reference programs, the oracle port on all threads."""
     from oracle import refscene, pyoracle
-    if not refscene.ref_available():
-        # the oracle port, all threads, on the same rows
+    binary = binary or refscene.REF_BIN
+    if not os.path.exists(binary):
         o = pyoracle.Oracle(scene)
         nthreads = os.cpu_count() or 1
         y0 = scene.height // 2
         t0 = time.perf_counter()
-        r = o.render(sample_count=scene.spp, window=(0, y0, scene.width, y0 + rows_per_proc), nthreads=nthreads,
+        r = o.render(sample_count=scene.spp, window=(0, y0, scene.width, y0 + steps), nthreads=nthreads,
                      streak=False)
         dt = time.perf_counter() - t0
         return {"value": r["stats"]["paths"] / dt, "unit": "paths/s", "cores": nthreads, "kind": "port",
-                "sample": f"{rows_per_proc} scanlines x {scene.width} px x {scene.spp} spp, oracle port"}
+                "ms_per_step": dt * 1e3 / steps,
+                "sample": f"{steps} scanlines x {scene.width} px x {scene.spp} spp, oracle port"}
     wd = tempfile.mkdtemp(prefix="bk_bench_")
     sp = os.path.join(wd, "scene.txt")
     refscene.write_scene(scene, sp)
+    rows = _spread_rows(scene.height, procs, warmup + steps)
     ps = []
     for i in range(procs):
-        y0 = (scene.height // 2 - procs * rows_per_proc // 2 + i * rows_per_proc) % scene.height
-        y1 = min(scene.height, y0 + rows_per_proc)
-        ps.append(subprocess.Popen([refscene.REF_BIN, sp, os.path.join(wd, f"out{i}.bin"), str(y0), str(y1),
-                                    "--no-streak"], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True))
-    paths, secs = 0, 0.0
+        # --timing: each process adds all its scanlines into one film row (T x W x 3 doubles)
+        ps.append(subprocess.Popen([binary, sp, os.path.join(wd, f"out{i}.bin"), "--rows", ",".join(map(str, rows[i])),
+                                    "--timing"],
+                                   stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True))
+    per = []
     for p in ps:
         _, err = p.communicate()
-        info = json.loads(err.strip().splitlines()[-1])
-        paths += info["paths"]
-        secs = max(secs, info["seconds"])
+        if p.returncode != 0:
+            raise RuntimeError("reference renderer failed: " + err[-400:])
+        per.append(json.loads(err.strip().splitlines()[-1])["row_seconds"])
     for f in os.listdir(wd):
         os.remove(os.path.join(wd, f))
     os.rmdir(wd)
+    paths_row = scene.width * scene.spp * scene.incoming_samples
+    step_s = [max(r[warmup + k] for r in per) for k in range(steps)]
+    secs = sum(step_s)
+    paths = procs * paths_row * steps
     return {"value": paths / secs, "unit": "paths/s", "cores": procs, "kind": "reference",
-            "sample": f"{procs} processes x {rows_per_proc} scanline(s) x {scene.width} px x {scene.spp} spp "
-                      f"({paths} paths), reference integrator with its own triangle/BVH backend, "
-                      f"render loop time of the slowest process"}
+            "ms_per_step": secs * 1e3 / steps,
+            "sample": f"per step {procs} processes x 1 scanline x {scene.width} px x {scene.spp} spp "
+                      f"({procs * paths_row} paths, scanlines spread over the image), {steps} timed steps after "
+                      f"{warmup} untimed; {what}; step time = slowest process's render call"}
 
 
 def max_over_ranks(x, dist=None, device="cpu"):
@@ -176,20 +197,33 @@ def whole_job_rate(units_per_rank, world, seconds):
     return units_per_rank * world / seconds
 
 
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+WORKLOAD_CONFIG = "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8"
+
+
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own renderer (Embree backend, streak splat on) on all
+    host cores; rank 0 alone runs it under torchrun."""
     from jarabotransientrendering_b200 import scenes as S
     if rank != 0:
         return
     sc = S.WORKLOADS[WORKLOAD]()
-    procs = max(1, min(os.cpu_count() or 1, 64))
-    rows = max(1, args.steps)
-    cb = cpu_reference(sc, rows, procs)
-    paths_per_step = sc.paths_per_frame()
+    procs = max(1, min(host_cores(), sc.height))
+    cb = cpu_reference(sc, procs, args.warmup, args.steps)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "paths/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": paths_per_step / cb["value"] * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8",
-                       "triangles": sc.num_triangles, "paths_per_step": paths_per_step},
+            "config": {"workload": WORKLOAD_CONFIG, "triangles": sc.num_triangles,
+                       "paths_per_step": sc.paths_per_frame(),
+                       "film": "FP64 [512][512][2048][3] in HBM (12.9 GB)",
+                       "l2": "film and path state larger than L2; 256 MiB write between steps",
+                       "parallelism": f"replicas x{world}"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -483,7 +517,7 @@ def main():
     out = {"metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "icosphere subdiv 7 in Cornell box, 512x512, 2048 bins x 0.0025, 256 spp, depth 8",
+           "config": {"workload": WORKLOAD_CONFIG,
                       "triangles": sc.num_triangles, "paths_per_step": paths_per_step,
                       "film": "FP64 [512][512][2048][3] in HBM (12.9 GB)",
                       "l2": "film and path state larger than L2; 256 MiB write between steps",
@@ -552,8 +586,15 @@ def main():
         ctx.close()
 
     if rank == 0 and not args.no_cpu_baseline:
-        procs = max(1, min(os.cpu_count() or 1, 32))
-        out["cpu_baseline"] = cpu_reference(sc, 1, procs)
+        procs = max(1, min(host_cores(), sc.height))
+        out["cpu_baseline"] = cpu_reference(sc, procs, 1, 3)
+        # the reference's own non-Embree triangle/BVH backend (src/Geometry), for comparison
+        from oracle import refscene
+        bvh = os.path.join(os.path.dirname(refscene.REF_BIN), "ref_render_bvh")
+        if os.path.exists(bvh):
+            nb = cpu_reference(sc, procs, 0, 1, binary=bvh, what="reference integrator and streak film, "
+                               "rays cast by its own non-Embree BVH (src/Geometry)")
+            out["cpu_baseline"]["non_embree_backend"] = {"value": nb["value"], "sample": nb["sample"]}
     if rank == 0 and world == 1 and not args.no_batched:
         try:
             out["batched"] = batched(args, local)

@@ -30,13 +30,18 @@
  * turns off path-tracing-only (light subpaths and vertex connections;
  * BidirectionalPathTracing::set_path_tracing_only, reachable through the API).
  *
- * Usage: ref_render SCENE OUT [y0 y1] [--no-streak]
- *   SCENE: text file written by oracle/refscene.py; OUT: raw doubles
+ * Usage: ref_render SCENE OUT [y0 y1 | --rows y,y,...] [--no-streak] [--timing]
+ *   SCENE: text file written by oracle/refscene.py; y0 y1 / --rows: render only scanlines
+ *   [y0, y1) / the listed ones (-film-scanline, one call of TransientRenderer::render per line;
+ *   the film then holds only those rows, in that order, H below = their count; with --timing
+ *   every scanline is added into one stored row - the same splat work in a film of one row, for
+ *   timing many scanlines per process); OUT: raw doubles
  *   streak [H][W][T][3] (unless --no-streak), steady [H][W][3], weight [H][W], then with N
  *   bounce films bstreak [N][H][W][T][3], bsteady [N][H][W][3], bweight [N][H][W], then with
  *   components (`filmopts U N C`, C != 0) depth [H][W], positions [H][W][3], normals [H][W][3]
  *   summed from each camera sample's record (Film::add_components, Film.h:127-145).
- *   Prints one JSON line with paths, seconds and paths/s on stderr.
+ *   Prints one JSON line on stderr: paths, seconds and paths/s of the render loop, and with a
+ *   scanline range the seconds of each scanline's render call.
  */
 #include <chrono>
 #include <cmath>
@@ -76,6 +81,7 @@ class AccumStreakFilm : public StreakCameraFilm<3, Radiance> {
     using Base = StreakCameraFilm<3, Radiance>;
 public:
     unsigned W, H, T;
+    std::vector<int> row_of;           /* scanline -> stored row (the film holds only rendered rows) */
     Real exposure, offset;
     std::vector<double> streak, steady, weight;
     bool keep_streak;
@@ -84,9 +90,13 @@ public:
     unsigned comps;
     std::vector<double> bstreak, bsteady, bweight;
     std::vector<double> cdepth, cpos, cnorm;
-    AccumStreakFilm(unsigned w, unsigned h, unsigned t, Real exp_, Real off, bool ks, bool uw, unsigned nb, unsigned cm)
-        : Base(w, h, t, exp_, uw, nullptr), W(w), H(h), T(t), exposure(exp_), offset(off),
+    AccumStreakFilm(unsigned w, unsigned full_h, const std::vector<int>& rows, unsigned t, Real exp_, Real off,
+                    bool ks, bool uw, unsigned nb, unsigned cm)
+        : Base(w, full_h, t, exp_, uw, nullptr), W(w), H((unsigned)rows.size()), T(t), exposure(exp_), offset(off),
           keep_streak(ks), unwarp(uw), NB(nb), comps(cm) {
+        const unsigned h = H;
+        row_of.assign(full_h, -1);
+        for (size_t i = 0; i < rows.size(); ++i) row_of[rows[i]] = (int)i;
         if (cm) {
             cdepth.assign((size_t)h * w, 0.0);
             cpos.assign((size_t)h * w * 3, 0.0);
@@ -105,7 +115,7 @@ public:
     /* StreakCameraFilm::add_samples with the box filter of size 1 (weight 1, one pixel): */
     void add_samples(const Sample& sample, const RadianceSampleRecordVector<3, Radiance>& rec) override {
         unsigned x = (unsigned)std::floor(sample.position[0]);
-        unsigned y = (unsigned)std::floor(sample.position[1]);
+        unsigned y = (unsigned)row_of[(unsigned)std::floor(sample.position[1])];
         size_t pix = (size_t)y * W + x;
         const size_t npix = (size_t)W * H;
         weight[pix] += sample.weight;
@@ -144,16 +154,23 @@ public:
 static void fail(const char* m) { fprintf(stderr, "ref_render: %s\n", m); exit(2); }
 
 int main(int argc, char** argv) {
-    if (argc < 3) fail("usage: ref_render SCENE OUT [y0 y1] [--no-streak]");
+    if (argc < 3) fail("usage: ref_render SCENE OUT [y0 y1 | --rows y,y,...] [--no-streak] [--timing]");
     bool keep_streak = true;
-    int y0 = -1, y1 = -1;
+    bool one_row = false;                  /* --timing: every scanline splats into one stored row */
+    std::vector<int> rows;                 /* scanlines to render; empty = the whole film */
     std::vector<std::string> pos;
     for (int i = 3; i < argc; ++i) {
         if (!strcmp(argv[i], "--no-streak")) keep_streak = false;
-        else pos.push_back(argv[i]);
+        else if (!strcmp(argv[i], "--timing")) one_row = true;
+        else if (!strcmp(argv[i], "--rows") && i + 1 < argc) {
+            std::stringstream ss(argv[++i]);
+            std::string item;
+            while (std::getline(ss, item, ',')) rows.push_back(atoi(item.c_str()));
+        } else pos.push_back(argv[i]);
     }
-    if (pos.size() >= 2) { y0 = atoi(pos[0].c_str()); y1 = atoi(pos[1].c_str()); }
-
+    if (pos.size() >= 2)
+        for (int y = atoi(pos[0].c_str()); y < atoi(pos[1].c_str()); ++y) rows.push_back(y);
+    const bool region = !rows.empty() || pos.size() >= 2;
     std::ifstream in(argv[1]);
     if (!in) fail("cannot open scene");
     std::string tag;
@@ -258,7 +275,17 @@ int main(int argc, char** argv) {
     Real fovr = M_PI / 180. * fov / 2;                                   /* bunnykiller.cpp:1156-1161 */
     Real fd = 1. / tan(fovr);
     PinholeCamera camera(cpos, cfoc, cup, fd);
-    AccumStreakFilm film(W, H, T, exposure, offset, keep_streak, unwarp != 0, nbounce, comps);
+    /* a scanline set stores only its own rows, so a full-size streak film fits per process */
+    std::vector<int> stored = rows;
+    if (!region) for (unsigned y = 0; y < H; ++y) stored.push_back((int)y);
+    if (one_row && region) stored.assign(1, rows[0]);
+    if (region && rows.empty()) fail("empty scanline range");
+    for (size_t i = 0; i < stored.size(); ++i) {
+        if (stored[i] < 0 || (unsigned)stored[i] >= H) fail("scanline out of range");
+        for (size_t j = 0; j < i; ++j) if (stored[j] == stored[i]) fail("repeated scanline");
+    }
+    AccumStreakFilm film(W, H, stored, T, exposure, offset, keep_streak, unwarp != 0, nbounce, comps);
+    if (one_row && region) for (int y : rows) film.row_of[y] = 0;
     StratifiedSampler sampler(W, H, sqrt_spp, true);
     TransientRenderer<3, Radiance, RadianceAttenuation> engine(nullptr, time_sampling);   /* bunnykiller.cpp:1754 */
     Random::StdRNG.seed(seed);                                           /* bunnykiller.cpp:1794 */
@@ -274,11 +301,14 @@ int main(int argc, char** argv) {
     (void)devnull;
     auto t0 = std::chrono::steady_clock::now();
     unsigned long long paths = 0;
-    if (y0 >= 0) {
-        for (int y = y0; y < y1; ++y) {
+    std::vector<double> row_seconds;
+    if (region) {
+        for (int y : rows) {
+            auto r0 = std::chrono::steady_clock::now();
             sampler.set_scanline(y);                                     /* -film-scanline, :1782-1791 */
             engine.render("ref", w, &bpt, camera, &film, &sampler);
             paths += (unsigned long long)W * sqrt_spp * sqrt_spp * ninc;
+            row_seconds.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - r0).count());
         }
     } else {
         engine.render("ref", w, &bpt, camera, &film, &sampler);
@@ -303,7 +333,10 @@ int main(int argc, char** argv) {
     }
     fclose(out);
     FILE* tty = fopen("/dev/stderr", "w");
-    fprintf(tty, "{\"paths\": %llu, \"seconds\": %.6f, \"paths_per_s\": %.3f}\n", paths, secs, paths / secs);
+    fprintf(tty, "{\"paths\": %llu, \"seconds\": %.6f, \"paths_per_s\": %.3f, \"row_seconds\": [",
+            paths, secs, paths / secs);
+    for (size_t i = 0; i < row_seconds.size(); ++i) fprintf(tty, "%s%.6f", i ? ", " : "", row_seconds[i]);
+    fprintf(tty, "]}\n");
     fclose(tty);
     return 0;
 }

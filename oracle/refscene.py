@@ -75,13 +75,15 @@ def write_scene(scene, path, seed=None):
         fh.write("end\n")
 
 
-def render(scene, seed=None, rows=None, keep_streak=True, workdir=None):
-    """Run the reference renderer; returns dict(streak, steady, weight, seconds, paths)."""
+def render(scene, seed=None, rows=None, keep_streak=True, workdir=None, binary=None):
+    """Run the reference renderer (`binary`, default oracle/_ref/ref_render: the Embree build);
+    returns dict(streak, steady, weight, seconds, paths).  rows=(y0, y1) renders scanlines
+    [y0, y1) only and returns films of y1 - y0 rows."""
     wd = workdir or tempfile.mkdtemp(prefix="bk_ref_")
     sp = os.path.join(wd, "scene.txt")
     op = os.path.join(wd, "film.bin")
     write_scene(scene, sp, seed)
-    cmd = [REF_BIN, sp, op]
+    cmd = [binary or REF_BIN, sp, op]
     if rows is not None:
         cmd += [str(rows[0]), str(rows[1])]
     if not keep_streak:
@@ -89,6 +91,8 @@ def render(scene, seed=None, rows=None, keep_streak=True, workdir=None):
     res = subprocess.run(cmd, check=True, capture_output=True, text=True)
     info = json.loads(res.stderr.strip().splitlines()[-1])
     H, W, T = scene.height, scene.width, scene.time_bins
+    if rows is not None:                     # a band holds only its own scanlines
+        H = rows[1] - rows[0]
     raw = np.fromfile(op, np.float64)
     off = 0
     streak = None
