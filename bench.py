@@ -58,7 +58,53 @@ def parse():
                     help="skip the sampling-mode throughputs (time sampling, light subpaths)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the 16-scene batched (CUDA-graph) throughput and accuracy leg")
+    # --case: a small render of one workload for ncu captures of single kernels (no JSON line)
+    ap.add_argument("--case", default=None, help="render a small case of this workload and exit")
+    ap.add_argument("--case-spp", type=int, default=8)
+    ap.add_argument("--case-bins", type=int, default=64)
+    ap.add_argument("--case-repeat", type=int, default=1)
+    ap.add_argument("--case-width", type=int, default=0)
+    ap.add_argument("--case-height", type=int, default=0)
+    ap.add_argument("--case-guided", action="store_true")
+    ap.add_argument("--case-mix", type=float, default=0.7)
+    ap.add_argument("--case-train-pool", type=int, default=0)
     return ap.parse_args()
+
+
+def profile_case(a):
+    """Small render for ncu captures: `--case-spp` samples per pixel of a workload's geometry and
+    camera at its full resolution but with a short film (`--case-bins` time bins, exposure scaled
+    to keep the film's time span), so that the device footprint stays small (the icosphere
+    geometry at 512x512, 8 spp, 64 bins: one 2M-path batch, ~0.5 GB on the device) while the
+    traversal kernels see the real BVH and the real first-bounce ray distribution.
+    `--case-width`/`--case-height` override the resolution (same camera, fewer pixels): 128x64
+    pixels at 256 spp and 2048 bins is one 2M-path batch with the benchmark's per-batch shape
+    (8192 pixels x 256 paths) and a 0.4 GB film.  `--case-guided` attaches a learned proposal
+    (orthonormal shading frames, mixture probability `--case-mix`); with `--case-train-pool 0`
+    the network stays at its seeded initialisation, otherwise it trains after every pass."""
+    from jarabotransientrendering_b200 import scenes as S
+    from jarabotransientrendering_b200.renderer import Context, Guide
+    sc = S.WORKLOADS[a.case]()
+    sc.exposure = sc.exposure * sc.time_bins / a.case_bins
+    sc.time_bins = a.case_bins
+    if a.case_width:
+        sc.width = a.case_width
+    if a.case_height:
+        sc.height = a.case_height
+    guide = None
+    if a.case_guided:
+        sc.flags |= S.FLAG_ORTHONORMAL_FRAME
+        guide = Guide(seed=1)
+    with Context(sc) as ctx:
+        if guide is not None:
+            ctx.set_guide(guide, mix_prob=a.case_mix, learning_rate=3e-3, train_pool=a.case_train_pool)
+        for r in range(a.case_repeat):
+            ctx.render(r * a.case_spp, a.case_spp)
+        st = ctx.stats()
+    print({k: st[k] for k in ("paths", "closest_rays", "shadow_rays", "splats", "render_ms", "bvh_nodes", "bvh_depth",
+                              "train_steps", "raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "splat_ms")})
+    if guide is not None:
+        guide.close()
 
 
 def peaks():
@@ -420,6 +466,9 @@ def batched(args, device, frames=2):
 
 def main():
     args = parse()
+    if args.case:
+        profile_case(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -304,9 +304,12 @@ tr_status tr_trace_rays_device(tr_ctx* ctx, const float* d_rays, uint32_t n, int
  * TR_ERR_INVALID_ARGUMENT -- split the window or the sample range over several calls.
  * The array is shared by every call in the process on that GPU: calls that can overlap on
  * the GPU (different streams, or different contexts on one device) race and corrupt each
- * other's paths, so issue them on one stream.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before any stream
- * capture begins. */
+ * other's paths, so issue them on one stream.  tr_create looks the array's device address up
+ * on its device (cudaGetSymbolAddress, which also loads the array there), so the calls only
+ * read a cached address; should that set-up look-up have failed, the first call retries it,
+ * so make the first call before any stream capture begins.  The paths, rays and splats of
+ * these calls count in tr_stats_get like tr_render's (read after the call's stream has
+ * finished). */
 #define TR_NOALLOC_MAX_PATHS 65536u
 #define TR_NOALLOC_MAX_BOUNCES 16u
 tr_status tr_render_region_noalloc(tr_ctx* ctx, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
@@ -345,6 +348,8 @@ tr_status tr_guide_destroy(tr_guide* g);
  * on the context's device and outlive its use. */
 tr_status tr_set_guide(tr_ctx* ctx, tr_guide* guide, float mix_prob, float learning_rate, uint32_t train_pool);
 
+/* Counters of the context (tr_stats).  Waits for the context's stream, then reads the device
+ * ray and splat counters, which every render entry point adds to. */
 tr_status tr_stats_get(tr_ctx* ctx, tr_stats* out);
 
 /* ---- multi-scene batches (no counterpart in the reference renderer) -------------------------

@@ -222,6 +222,9 @@ void ensure_wave(tr_ctx* x, uint32_t capacity) {
 // Per-kind kernel times of the pending timed launches and the union of the traversal (extend,
 // shadow) launch intervals, into the context's statistics; one cudaEventElapsedTime per event,
 // relative to the first pending event.  Clears the pending launches.
+// Reads the pending launch events out and adds their kernel times to x->prof_sum (each
+// read-out's traversal union is over its own launches, which end before the next read-out's
+// begin, so the sums stay exact unions).
 cudaError_t prof_readout(tr_ctx* x) {
     if (x->prof_marks.empty()) { x->prof_next = 0; return cudaSuccess; }
     std::vector<float> t(x->prof_next, 0.f);
@@ -229,26 +232,28 @@ cudaError_t prof_readout(tr_ctx* x) {
         const cudaError_t e = cudaEventElapsedTime(&t[i], x->prof_events[0], x->prof_events[i]);
         if (e != cudaSuccess) return e;
     }
-    double kms[6] = {0, 0, 0, 0, 0, 0};
     std::vector<std::pair<float, float>> trace_iv;
     for (const tr_ctx::ProfMark& m : x->prof_marks) {
-        kms[m.kind] += t[m.ev + 1] - t[m.ev];
+        x->prof_sum[m.kind] += t[m.ev + 1] - t[m.ev];
         if (m.kind == 1 || m.kind == 3) trace_iv.push_back({t[m.ev], t[m.ev + 1]});
     }
     std::sort(trace_iv.begin(), trace_iv.end());
-    double trace_ms = 0.0;
     for (size_t i = 0; i < trace_iv.size();) {
         float a = trace_iv[i].first, b = trace_iv[i].second;
         for (++i; i < trace_iv.size() && trace_iv[i].first <= b; ++i) b = std::max(b, trace_iv[i].second);
-        trace_ms += b - a;
+        x->prof_sum[6] += b - a;
     }
-    x->stats.trace_ms = trace_ms;
-    x->stats.raygen_ms = kms[0]; x->stats.extend_ms = kms[1]; x->stats.shade_ms = kms[2];
-    x->stats.shadow_ms = kms[3]; x->stats.splat_ms = kms[4];
-    x->stats.guide_ms = kms[5];
     x->prof_marks.clear();
     x->prof_next = 0;
     return cudaSuccess;
+}
+
+// Moves the accumulated kernel times into x->stats and starts a new sum.
+void prof_publish(tr_ctx* x) {
+    x->stats.raygen_ms = x->prof_sum[0]; x->stats.extend_ms = x->prof_sum[1]; x->stats.shade_ms = x->prof_sum[2];
+    x->stats.shadow_ms = x->prof_sum[3]; x->stats.splat_ms = x->prof_sum[4]; x->stats.guide_ms = x->prof_sum[5];
+    x->stats.trace_ms = x->prof_sum[6];
+    for (double& v : x->prof_sum) v = 0.0;
 }
 
 // Lane k + 1's buffers: the per-slot arrays of the first wave at its capacity, its own queue
@@ -605,7 +610,10 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     TR_CUDA(cudaEventSynchronize(x->ev1));
     float ms = 0.f;
     TR_CUDA(cudaEventElapsedTime(&ms, x->ev0, x->ev1));
-    if (x->profiling == 1) TR_CUDA(prof_readout(x));
+    if (x->profiling == 1) {
+        TR_CUDA(prof_readout(x));
+        prof_publish(x);
+    }
     x->stats.kernel_launches = launches;
     x->stats.extend_launches = ext_l;
     x->stats.shadow_launches = sh_l;
@@ -621,6 +629,10 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     return TR_OK;
 }
 
+}  // namespace
+
+namespace {
+void noalloc_prepare(int device);
 }  // namespace
 
 extern "C" {
@@ -709,6 +721,12 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             if (x->d_cpos) TR_CUDA(cudaMemsetAsync(x->d_cpos, 0, npix * 3u * sizeof(double), x->stream));
             if (x->d_cnorm) TR_CUDA(cudaMemsetAsync(x->d_cnorm, 0, npix * 3u * sizeof(double), x->stream));
         }
+        // the context's ray and splat counters (every render entry point adds to them) and,
+        // for tr_render_region_noalloc, the scratch array's device address: both at set-up, so
+        // that entry point allocates nothing and loads no module when it is called
+        x->wave.stats = x->alloc<unsigned long long>(8);
+        TR_CUDA(cudaMemsetAsync(x->wave.stats, 0, 8 * sizeof(unsigned long long), x->stream));
+        noalloc_prepare(device);
 
         // the scene's own arrays go to the device first (the BVH is built there from them)
         const size_t ntri = s->num_triangles;
@@ -1074,15 +1092,28 @@ tr_status tr_trace_rays(tr_ctx* x, const float* rays, uint32_t n, int any_hit, t
 
 tr_status tr_stats_get(tr_ctx* x, tr_stats* out) {
     if (!x || !out) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
-    if (x->profiling == 2 && !x->prof_marks.empty()) {
+    if (x->profiling == 2) {            // the sums over every render since the previous read
         cudaSetDevice(x->device);
         const cudaError_t e = prof_readout(x);
         if (e != cudaSuccess) return fail(TR_ERR_CUDA, cudaGetErrorString(e));
+        prof_publish(x);
+    }
+    if (x->wave.stats) {                // counters of every render, tr_render_region_noalloc's included
+        cudaSetDevice(x->device);
+        unsigned long long st[8];
+        cudaError_t e = cudaStreamSynchronize(x->s());
+        if (e == cudaSuccess) e = cudaMemcpy(st, x->wave.stats, sizeof(st), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail(TR_ERR_CUDA, cudaGetErrorString(e));
+        x->stats.closest_rays = st[0];
+        x->stats.shadow_rays = st[1];
+        x->stats.splats = st[2];
     }
     *out = x->stats;
     out->device_bytes = x->bytes;
     return TR_OK;
 }
+
+}  // extern "C"
 
 // -----------------------------------------------------------------------------------------
 // tr_render_region_noalloc: the same wavefront kernels, with every per-path buffer carved out
@@ -1099,7 +1130,6 @@ constexpr size_t kNaBytes = 7 * kNaF4                                           
                           + na_align(sizeof(float4) * kNaSlots * TR_NOALLOC_MAX_BOUNCES)  // records
                           + na_align(kNaSlots)                                    // records per slot
                           + na_align(sizeof(uint32_t) * trk::kCounters)           // queue counters
-                          + na_align(sizeof(unsigned long long) * 8)              // ray / splat counts
                           + na_align(sizeof(float) * kNaSlots)                    // camera distances
                           + kNaF4;                                                // light points (time sampling)
 
@@ -1125,7 +1155,17 @@ tr_status noalloc_scratch(int device, unsigned char** out) {
     return TR_OK;
 }
 
+// Set-up half of the look-up, run by tr_create with `device` current: loads the array on this
+// device once, so that tr_render_region_noalloc's calls only read the cached address.  A
+// failure here is not fatal to the context; the entry point then retries and reports it.
+void noalloc_prepare(int device) {
+    unsigned char* p = nullptr;
+    if (noalloc_scratch(device, &p) != TR_OK) cudaGetLastError();
+}
+
 }  // namespace
+
+extern "C" {
 
 extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
                                               uint64_t s0, uint32_t ns, void* stream) {
@@ -1170,14 +1210,13 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
         w.rec = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots * TR_NOALLOC_MAX_BOUNCES));
         w.rec_n = take(kNaSlots);
         w.counters = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * trk::kCounters));
-        w.stats = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 8));
+        w.stats = x->wave.stats;         // the context's own ray / splat counters (from tr_create)
         w.cam_dist = reinterpret_cast<float*>(take(sizeof(float) * kNaSlots));
         w.target = reinterpret_cast<float4*>(take(sizeof(float4) * kNaSlots));
         w.capacity = (uint32_t)kNaSlots;
-        // what the kernels expect to start at zero: queue counters / fetch cursors and the
-        // ray counters (records-per-slot are reset by the ray generation kernel)
+        // what the kernels expect to start at zero: queue counters / fetch cursors (records per
+        // slot are reset by the ray generation kernel; the ray counters keep adding up)
         TR_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * trk::kCounters, strm));
-        TR_CUDA(cudaMemsetAsync(w.stats, 0, sizeof(unsigned long long) * 8, strm));
         p.batch.win_x0 = x0; p.batch.win_y0 = y0; p.batch.win_w = x1 - x0;
         p.batch.pix_begin = 0; p.batch.npix = (uint32_t)npix;
         p.batch.s0 = s0; p.batch.ns = ns; p.batch.ninc = x->integ.incoming_samples;
@@ -1458,6 +1497,7 @@ tr_status tr_set_profiling(tr_ctx* x, int on) {
     x->profiling = on;
     x->prof_marks.clear();          // launches timed under another setting are dropped
     x->prof_next = 0;
+    for (double& v : x->prof_sum) v = 0.0;
     return TR_OK;
 }
 

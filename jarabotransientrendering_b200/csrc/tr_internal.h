@@ -186,6 +186,9 @@ struct tr_ctx {
     struct ProfMark { int kind; size_t ev; };
     std::vector<ProfMark> prof_marks;     // launches timed and not read out yet
     size_t prof_next = 0;                 // events of prof_events in use
+    // read-out kernel times not yet handed to tr_stats_get: raygen, extend, shade, shadow,
+    // splat, guide, then the union of the traversal intervals (milliseconds)
+    double prof_sum[7] = {0, 0, 0, 0, 0, 0, 0};
     cudaStream_t s() const { return user_stream ? user_stream : stream; }
 
     template <class T>

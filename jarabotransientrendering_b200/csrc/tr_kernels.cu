@@ -3,12 +3,13 @@
 // Pipeline per batch of path slots (one slot = one camera sample x incoming sample):
 //   raygen  -> camera ray, per-path PCG32 stream, optional free-flight distance
 //   for depth in [0, max_bounces):
-//     extend  (persistent, closest hit, shared-memory stack)
+//     extend  (persistent warps, closest hit, shared-memory stack, lane refill from the queue)
 //     shade   (vertex, next-event estimate -> shadow queue, Russian roulette, new direction
-//              -> next extend queue; queues compacted with warp ballots)
+//              -> next extend queue, appended per block grouped by direction octant)
 //     shadow  (persistent, any hit) -> splat record per surviving connection
-//   splat   (per group of pixels: records -> shared-memory FP32 (pixel, bin) tile with
-//            warp-aggregated atomics -> FP64 film in HBM)
+//   splat   (per group of whole pixels: records read bounce-major; lanes with equal
+//            (pixel, bin) keys found with __match_any_sync, summed in FP32 by a shuffle tree,
+//            one native FP64 atomicAdd per group into the film in HBM)
 // Reference path: src/Integrator/BidirectionalPathTracing.h:485-692,975-1140 and
 // src/Film/StreakCameraFilm.h:139-192 (details at each kernel).
 #include "tr_bsdf.cuh"

@@ -4,8 +4,9 @@ It serves callers that cannot allocate GPU memory once set up -- under an engine
 pool owns the device, or in a frame loop that cannot pay cudaMalloc's device-wide
 synchronisation mid-frame.  Its per-path state lives in one fixed array inside the library;
 this file checks, through the C ABI, that it renders exactly what tr_render renders, on two
-calls in a row (the array keeps the previous call's contents), and that requests beyond its
-stated limits are refused.  Named test_zz_* so pytest runs it last; it also passes alone in
+calls in a row (the array keeps the previous call's contents), that its calls allocate no device
+memory and count their rays like tr_render's, and that requests beyond its stated limits are
+refused.  Named test_zz_* so pytest runs it last; it also passes alone in
 a fresh process, where its first call performs the per-device set-up.
 """
 import ctypes as C
@@ -64,3 +65,26 @@ def test_noalloc_refuses_requests_beyond_its_limits(gpu):
     with gpu.Context(deep) as ctx:
         rc = _noalloc(ctx, (0, 0, 8, 8), 0, 1)
         assert rc == 1 and b"max_bounces" in _abi.lib().tr_last_error()
+
+
+def test_noalloc_calls_allocate_nothing_and_count_their_rays(gpu):
+    """After set-up (tr_create), further calls change neither the device's free memory nor the
+    context's device bytes, and the context's ray and splat counters match tr_render's."""
+    import torch
+    sc = S.cornell(width=32, height=24, time_bins=256, exposure=0.02, sqrt_spp=4, max_bounces=6)
+    window = (0, 0, sc.width, sc.height)
+    with gpu.Context(sc) as ref, gpu.Context(sc) as na:
+        _abi.check(_noalloc(na, window, 0, 4))       # warm-up call
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        bytes0 = na.stats()["device_bytes"]
+        for s0 in (4, 8, 12):
+            _abi.check(_noalloc(na, window, s0, 4))
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        st = na.stats()
+        assert free1 == free0 and st["device_bytes"] == bytes0
+        ref.render(0, 16)
+        sr = ref.stats()
+        for k in ("paths", "camera_samples", "closest_rays", "shadow_rays", "splats"):
+            assert st[k] == sr[k] and st[k] > 0, k
