@@ -398,7 +398,8 @@ tr_status tr_set_stream(tr_ctx* ctx, void* stream);
 
 /* Per-kernel CUDA-event timing inside tr_render: 0 off; 1 on, the times of each render read out
  * when it ends (tr_stats: the last render's); 2 on, read out at the next tr_stats_get (tr_stats:
- * the sums over the renders since the previous read), which keeps the read-out, about 1.5 us of
+ * the sums over the renders since the previous read, or the previous sums again when no render
+ * ran since), which keeps the read-out, about 1.5 us of
  * host time per timed launch, out of the renders.                                          */
 tr_status tr_set_profiling(tr_ctx* ctx, int on);
 tr_status tr_destroy(tr_ctx* ctx);

@@ -245,6 +245,7 @@ cudaError_t prof_readout(tr_ctx* x) {
     }
     x->prof_marks.clear();
     x->prof_next = 0;
+    x->prof_dirty = true;
     return cudaSuccess;
 }
 
@@ -254,6 +255,7 @@ void prof_publish(tr_ctx* x) {
     x->stats.shadow_ms = x->prof_sum[3]; x->stats.splat_ms = x->prof_sum[4]; x->stats.guide_ms = x->prof_sum[5];
     x->stats.trace_ms = x->prof_sum[6];
     for (double& v : x->prof_sum) v = 0.0;
+    x->prof_dirty = false;
 }
 
 // Lane k + 1's buffers: the per-slot arrays of the first wave at its capacity, its own queue
@@ -1092,7 +1094,8 @@ tr_status tr_trace_rays(tr_ctx* x, const float* rays, uint32_t n, int any_hit, t
 
 tr_status tr_stats_get(tr_ctx* x, tr_stats* out) {
     if (!x || !out) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
-    if (x->profiling == 2) {            // the sums over every render since the previous read
+    if (x->profiling == 2 && (x->prof_dirty || !x->prof_marks.empty())) {
+        // the sums over every render since the previous read (unchanged if none ran since)
         cudaSetDevice(x->device);
         const cudaError_t e = prof_readout(x);
         if (e != cudaSuccess) return fail(TR_ERR_CUDA, cudaGetErrorString(e));
@@ -1498,6 +1501,7 @@ tr_status tr_set_profiling(tr_ctx* x, int on) {
     x->prof_marks.clear();          // launches timed under another setting are dropped
     x->prof_next = 0;
     for (double& v : x->prof_sum) v = 0.0;
+    x->prof_dirty = false;
     return TR_OK;
 }
 

@@ -189,6 +189,7 @@ struct tr_ctx {
     // read-out kernel times not yet handed to tr_stats_get: raygen, extend, shade, shadow,
     // splat, guide, then the union of the traversal intervals (milliseconds)
     double prof_sum[7] = {0, 0, 0, 0, 0, 0, 0};
+    bool prof_dirty = false;              // prof_sum holds read-outs not yet published
     cudaStream_t s() const { return user_stream ? user_stream : stream; }
 
     template <class T>
