@@ -337,6 +337,12 @@ tr_status tr_guide_forward(tr_guide* g, const uint16_t* d_features, uint32_t n, 
 tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features, const float* d_dirs, const float* d_weights,
                               uint32_t n, float lr, float* loss, void* stream);
 tr_status tr_guide_get_grads(tr_guide* g, float* grads);
+/* Wait limit of the guide's tensor-core kernels: how many times a kernel polls the mbarrier of
+ * its own MMAs before the wait counts as timed out (default 2^24; 0 = every wait times out at
+ * once).  A timed-out kernel records the error, waits (with the full bound) for the MMAs it
+ * issued, frees its tensor memory and returns; the call that launched it then returns
+ * TR_ERR_TIMEOUT and the guide stays usable.  For tests and diagnostics of that path. */
+tr_status tr_guide_set_wait_limit(tr_guide* g, uint32_t polls);
 tr_status tr_guide_destroy(tr_guide* g);
 
 /* Renders the context with the learned proposal: surface directions are drawn from the

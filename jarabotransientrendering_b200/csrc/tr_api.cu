@@ -1375,18 +1375,18 @@ void train_enqueue(tr_guide* g, const uint4* x, const float* d_dirs, const float
     g->ensure(n);
     TR_CUDA(trg::mlp_forward(g->dev(), x, n, g->out, g->act, g->err, s));
     TR_CUDA(cudaMemsetAsync(g->scalars, 0, 4 * sizeof(float), s));
-    TR_CUDA(trg::mix_grad(g->out, d_dirs, d_weights, n, g->scalars, g->dy_bf, g->dy_f, g->scalars + 1, s));
+    TR_CUDA(trg::mix_grad(g->out, d_dirs, d_weights, n, g->scalars, g->dy_bf, g->scalars + 1, s));
     TR_CUDA(trg::mlp_backward(g->dev(), g->dy_bf, g->act, n, g->dh, g->err, s));
     TR_CUDA(cudaMemsetAsync(g->grads, 0, sizeof(float) * TR_GUIDE_PARAMS, s));
     float* gb = g->grads + 4 * 4096;
     const size_t mrow = (size_t)n * 8;
     trg::DwLayers dw{};
-    dw.prev[0] = x;                  dw.grad[0] = g->dh;
-    dw.prev[1] = g->act;             dw.grad[1] = g->dh + (size_t)n * 64;
-    dw.prev[2] = g->act + mrow;      dw.grad[2] = g->dh + (size_t)2 * n * 64;
-    dw.prev[3] = g->act + 2 * mrow;  dw.grad[3] = g->dy_f;                    // output layer
+    dw.prev[0] = x;                  dw.grad_bf[0] = g->dh;
+    dw.prev[1] = g->act;             dw.grad_bf[1] = g->dh + mrow;
+    dw.prev[2] = g->act + mrow;      dw.grad_bf[2] = g->dh + 2 * mrow;
+    dw.prev[3] = g->act + 2 * mrow;  dw.grad_bf[3] = g->dy_bf;                // output layer
     for (int l = 0; l < 4; ++l) { dw.gw[l] = g->grads + 4096 * l; dw.gb[l] = gb + 64 * l; }
-    TR_CUDA(trg::weight_grad(dw, n, s));
+    TR_CUDA(trg::weight_grad(dw, n, g->spin, g->err, s));
     if (lr > 0.0f) {
         g->step += 1;
         TR_CUDA(trg::adam(g->params, g->grads, g->m1, g->m2, TR_GUIDE_PARAMS, lr, g->step, s));
@@ -1408,6 +1408,12 @@ extern "C" tr_status tr_guide_train_step(tr_guide* g, const uint16_t* d_features
     } catch (const CudaError& e) {
         return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
     }
+}
+
+extern "C" tr_status tr_guide_set_wait_limit(tr_guide* g, uint32_t polls) {
+    if (!g) return fail(TR_ERR_INVALID_ARGUMENT, "null guide");
+    g->spin = polls;
+    return TR_OK;
 }
 
 extern "C" tr_status tr_guide_destroy(tr_guide* g) {

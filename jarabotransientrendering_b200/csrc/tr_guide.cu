@@ -8,8 +8,9 @@
 // accumulator in tensor memory; tcgen05.commit arrives on an mbarrier; every thread then reads
 // its row back with tcgen05.ld, adds the bias, applies ReLU and writes the BF16 row as the next
 // layer's A operand.  The weight gradients (a reduction over the batch, 2 GFLOP per 65,536-row
-// step) run on the CUDA cores.  Every wait on the mbarrier is bounded; on expiry the kernel
-// records an error, waits (bounded) for its MMAs, frees its tensor memory and returns.
+// step) run on the tensor cores too (k_dw_tc).  Every wait on an mbarrier is bounded (the
+// guide's wait limit); on expiry the kernel records an error, waits (bounded) for its MMAs,
+// frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(128, 4) k_mlp_fwd(GuideDev g, const uint4* __r
         for (int c = 0; c < 8; ++c) v[c] = row < m ? __ldg(&x[(size_t)row * 8 + c]) : make_uint4(0, 0, 0, 0);
         store_row_a(sA, tid, v);
         for (uint32_t l = 0; l < 4 && ok; ++l) {
-            ok = layer_mma(taddr, smem_u32(sA), smem_u32(smem + kSmemW + l * 8192u), bar, phase, s_ok);
+            ok = layer_mma(taddr, smem_u32(sA), smem_u32(smem + kSmemW + l * 8192u), bar, phase, s_ok, g.spin);
             if (!ok) break;
             float acc[64];
 #pragma unroll
@@ -84,11 +85,12 @@ __global__ void __launch_bounds__(128, 4) k_mlp_fwd(GuideDev g, const uint4* __r
 
 // ---------------------------------------------------------------------------------------------
 // backward through the hidden layers: given dY = dL/d(out) (bf16, cols >= 40 zero) and the
-// stored activations, dh[2] = dH3 = (dY W4^T) * 1[H3>0], dh[1] = dH2, dh[0] = dH1 (FP32).
+// stored activations, dh[2] = dH3 = (dY W4^T) * 1[H3>0], dh[1] = dH2, dh[0] = dH1 (BF16, the
+// weight-gradient kernel's B operands).
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 4) k_mlp_bwd(GuideDev g, const uint4* __restrict__ dy,
                                                     const uint4* __restrict__ act, uint32_t m,
-                                                    float* __restrict__ dh, int* err) {
+                                                    uint4* __restrict__ dh, int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sA = smem + kSmemA;
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kSmemBar);
@@ -113,7 +115,7 @@ __global__ void __launch_bounds__(128, 4) k_mlp_bwd(GuideDev g, const uint4* __r
         store_row_a(sA, tid, v);
         // layer index of the weights used: 3 (W4), 2 (W3), 1 (W2); activation masks H3, H2, H1
         for (int l = 3; l >= 1 && ok; --l) {
-            ok = layer_mma(taddr, smem_u32(sA), smem_u32(smem + kSmemW + (uint32_t)l * 8192u), bar, phase, s_ok);
+            ok = layer_mma(taddr, smem_u32(sA), smem_u32(smem + kSmemW + (uint32_t)l * 8192u), bar, phase, s_ok, g.spin);
             if (!ok) break;
             float acc[64];
 #pragma unroll
@@ -130,12 +132,8 @@ __global__ void __launch_bounds__(128, 4) k_mlp_bwd(GuideDev g, const uint4* __r
                     t[2 * e] = bf_lo(aw[e]) > 0.0f ? acc[8 * c + 2 * e] : 0.0f;
                     t[2 * e + 1] = bf_hi(aw[e]) > 0.0f ? acc[8 * c + 2 * e + 1] : 0.0f;
                 }
-                if (row < m) {
-                    float4* d = reinterpret_cast<float4*>(dh + ((size_t)(l - 1) * m + row) * 64 + 8 * c);
-                    d[0] = make_float4(t[0], t[1], t[2], t[3]);
-                    d[1] = make_float4(t[4], t[5], t[6], t[7]);
-                }
                 h[c] = make_uint4(pack2(t[0], t[1]), pack2(t[2], t[3]), pack2(t[4], t[5]), pack2(t[6], t[7]));
+                if (row < m) dh[((size_t)(l - 1) * m + row) * 8 + c] = h[c];
             }
             store_row_a(sA, tid, h);
         }
@@ -189,7 +187,7 @@ cudaError_t mlp_forward(const GuideDev& g, const uint4* x, uint32_t m, float* ou
     return cudaGetLastError();
 }
 
-cudaError_t mlp_backward(const GuideDev& g, const uint4* dy, const uint4* act, uint32_t m, float* dh, int* err,
+cudaError_t mlp_backward(const GuideDev& g, const uint4* dy, const uint4* act, uint32_t m, uint4* dh, int* err,
                          cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
@@ -218,11 +216,11 @@ __global__ void k_pack_weights(const float* __restrict__ params, uint8_t* __rest
     *reinterpret_cast<__nv_bfloat16*>(w_bwd + l * 8192u + canon_off(in, o)) = v;
 }
 
-// training loss -(w/W) log q(dir) and its gradient w.r.t. the 40 raw outputs; dy bf16 (and
-// FP32 copy) [m][64], columns >= 40 zero.  wsum = sum of weights over the batch.
+// training loss -(w/W) log q(dir) and its gradient w.r.t. the 40 raw outputs; dy bf16
+// [m][64], columns >= 40 zero.  wsum = sum of weights over the batch.
 __global__ void k_mix_grad(const float* __restrict__ out, const float* __restrict__ dirs, const float* __restrict__ w,
                            uint32_t m, const float* __restrict__ wsum, uint4* __restrict__ dy_bf,
-                           float* __restrict__ dy_f, float* __restrict__ loss) {
+                           float* __restrict__ loss) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float l_i = 0.0f;
     if (i < m) {
@@ -264,9 +262,6 @@ __global__ void k_mix_grad(const float* __restrict__ out, const float* __restric
         for (int c = 0; c < 8; ++c) {
             dy_bf[(size_t)i * 8 + c] = make_uint4(pack2(g[8 * c], g[8 * c + 1]), pack2(g[8 * c + 2], g[8 * c + 3]),
                                                   pack2(g[8 * c + 4], g[8 * c + 5]), pack2(g[8 * c + 6], g[8 * c + 7]));
-            float4* d = reinterpret_cast<float4*>(dy_f + (size_t)i * 64 + 8 * c);
-            d[0] = make_float4(g[8 * c], g[8 * c + 1], g[8 * c + 2], g[8 * c + 3]);
-            d[1] = make_float4(g[8 * c + 4], g[8 * c + 5], g[8 * c + 6], g[8 * c + 7]);
         }
     }
     // block-reduce the loss
@@ -281,56 +276,146 @@ __global__ void k_sum(const float* __restrict__ w, uint32_t m, float* __restrict
     if ((threadIdx.x & 31u) == 0) atomicAdd(out, s);
 }
 
-// weight gradients of all four layers in one launch (blockIdx.y = layer):
-// gw[in][out] = sum_rows prev[row][in] * grad[row][out], gb[out] = sum_rows grad[row][out];
-// prev is bf16 (x or a stored activation), grad FP32.  256 threads per block; each thread
-// owns a 4x4 patch of the 64x64 gradient and keeps it in registers while the block walks its
-// 64-row chunks (grid-stride), so each block adds its partial sums to global memory once.
-constexpr uint32_t kDwRows = 64;
-__global__ void __launch_bounds__(256) k_dw(DwLayers L, uint32_t m) {
-    __shared__ float sp[kDwRows][65];
-    __shared__ float sg[kDwRows][65];
-    const uint32_t l = blockIdx.y;
-    const uint4* __restrict__ prev = L.prev[l];
-    const float* __restrict__ grad = L.grad[l];
-    const uint32_t ti = (threadIdx.x >> 4) * 4u, to = (threadIdx.x & 15u) * 4u;
-    float acc[4][4] = {};
-    float sb = 0.0f;
-    for (uint32_t r0 = blockIdx.x * kDwRows; r0 < m; r0 += gridDim.x * kDwRows) {
+// Weight gradients of all four layers on the tensor cores (blockIdx.y = layer):
+//   gw[l][in][out] = sum_rows prev[row][in] * grad[row][out],  gb[l][out] = sum_rows grad[row][out]
+// with BF16 operands and FP32 accumulation in tensor memory.  One MMA chain per CTA computes
+// D (128 x 64) += A (128 x K) * B (64 x K)^T over the CTA's rows, in K-tiles of 64 rows:
+//   A rows 0..63 = prev^T (m = input unit, k = batch row); row 64 = 1 for every valid row, so
+//   D row 64 is the bias gradient; rows 65..127 = 0;
+//   B rows = grad^T (n = output unit, k = batch row).
+// Both operands are staged transposed into the canonical K-major layout (the same layout as
+// the forward's A tile), double-buffered: tile i + 1 is staged while the MMAs of tile i run
+// (one mbarrier per stage, each wait bounded).  The CTA then reads D rows 0..64 back from
+// tensor memory and adds them to gw / gb with coalesced atomics.
+constexpr uint32_t kDwK = 64;                                  // batch rows per K-tile
+constexpr uint32_t kDwA = 16384, kDwB = 8192;                  // bytes per stage
+constexpr uint32_t kDwSmemA0 = 0, kDwSmemB0 = 2 * kDwA, kDwSmemBar = 2 * kDwA + 2 * kDwB,
+                   kDwSmemSlot = kDwSmemBar + 16, kDwSmemOk = kDwSmemSlot + 4, kDwSmemBytes = kDwSmemOk + 12;
+constexpr uint32_t kIdescM128N64 = kIdesc;                     // BF16 x BF16 -> FP32, M = 128, N = 64
+
+__global__ void __launch_bounds__(128) k_dw_tc(DwLayers L, uint32_t m, uint32_t tiles_per_cta, uint32_t spin,
+                                               int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kDwSmemBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kDwSmemSlot);
+    volatile int* s_ok = reinterpret_cast<volatile int*>(smem + kDwSmemOk);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, l = blockIdx.y;
+    // constant-index selects keep the parameter arrays out of local memory
+    auto pick = [l](auto a0, auto a1, auto a2, auto a3) { return l == 0 ? a0 : l == 1 ? a1 : l == 2 ? a2 : a3; };
+    const uint4* __restrict__ prev = pick(L.prev[0], L.prev[1], L.prev[2], L.prev[3]);
+    const uint4* __restrict__ grad = pick(L.grad_bf[0], L.grad_bf[1], L.grad_bf[2], L.grad_bf[3]);
+    const uint32_t ntiles = (m + kDwK - 1) / kDwK;
+    const uint32_t t0 = blockIdx.x * tiles_per_cta;
+    const uint32_t t1 = min(ntiles, t0 + tiles_per_cta);
+    if (t0 >= t1) return;
+    // zero both A stages (rows 65..127 stay zero; rows 0..64 are rewritten per tile)
+    for (uint32_t i = tid; i < 2 * kDwA / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(smem + kDwSmemA0)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); fence_mbar_init(); }
+    if (warp == 0) { tmem_alloc(tslot, 64); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = *tslot;
+    uint32_t phases = 0u;              // bit s = parity of the next completion of stage s
+    bool ok = true;
+    // thread -> (row r of the tile, half h of the 8 16-byte chunks of a 64-wide row)
+    const uint32_t r = tid & 63u, h = tid >> 6;
+    for (uint32_t t = t0; t < t1 && ok; ++t) {
+        const uint32_t st = (t - t0) & 1u;
+        uint8_t* sA = smem + kDwSmemA0 + st * kDwA;
+        uint8_t* sB = smem + kDwSmemB0 + st * kDwB;
+        // the MMAs that last read this stage (two tiles ago) must have completed
+        if (t - t0 >= 2u) {
+            if (tid == 0) {
+                bool done = false;
+                for (uint32_t it = 0; it < spin && !done; ++it) done = mbar_try_wait(&bar[st], (phases >> st) & 1u);
+                *s_ok = done ? 1 : 0;
+            }
+            __syncthreads();
+            ok = *s_ok != 0;
+            if (!ok) break;
+            phases ^= 1u << st;
+        }
+        const uint32_t row = t * kDwK + r;
+        const bool valid = row < m;
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t c = 4u * h + q;                  // chunk: units 8c .. 8c + 7
+            const uint4 a = valid ? __ldg(&prev[(size_t)row * 8 + c]) : make_uint4(0u, 0u, 0u, 0u);
+            const uint4 b = valid ? __ldg(&grad[(size_t)row * 8 + c]) : make_uint4(0u, 0u, 0u, 0u);
+            const uint32_t aw[4] = {a.x, a.y, a.z, a.w}, bw[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (uint32_t e = 0; e < 4; ++e) {
+                *reinterpret_cast<uint16_t*>(sA + canon_off(8u * c + 2u * e, r)) = (uint16_t)(aw[e] & 0xffffu);
+                *reinterpret_cast<uint16_t*>(sA + canon_off(8u * c + 2u * e + 1u, r)) = (uint16_t)(aw[e] >> 16);
+                *reinterpret_cast<uint16_t*>(sB + canon_off(8u * c + 2u * e, r)) = (uint16_t)(bw[e] & 0xffffu);
+                *reinterpret_cast<uint16_t*>(sB + canon_off(8u * c + 2u * e + 1u, r)) = (uint16_t)(bw[e] >> 16);
+            }
+        }
+        if (h == 0) *reinterpret_cast<uint16_t*>(sA + canon_off(64u, r)) = valid ? (uint16_t)0x3f80u : (uint16_t)0u;
+        fence_proxy_async();
+        tc_fence_before();
         __syncthreads();
-        for (uint32_t e = threadIdx.x; e < kDwRows * 8u; e += blockDim.x) {
-            const uint32_t r = e >> 3, c = e & 7u, row = r0 + r;
-            const uint4 v = row < m ? __ldg(&prev[(size_t)row * 8 + c]) : make_uint4(0, 0, 0, 0);
-            const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
+        if (tid == 0) {
+            tc_fence_after();
 #pragma unroll
-            for (int q = 0; q < 4; ++q) { sp[r][8 * c + 2 * q] = bf_lo(vw[q]); sp[r][8 * c + 2 * q + 1] = bf_hi(vw[q]); }
+            for (uint32_t k = 0; k < 4; ++k)
+                umma_bf16(taddr, smem_desc(smem_u32(sA) + k * 256u), smem_desc(smem_u32(sB) + k * 256u),
+                          kIdescM128N64, (t > t0 || k > 0) ? 1u : 0u);
+            umma_commit(&bar[st]);
         }
-        for (uint32_t e = threadIdx.x; e < kDwRows * 16u; e += blockDim.x) {
-            const uint32_t r = e >> 4, c = (e & 15u) * 4u, row = r0 + r;
-            const float4 v = row < m ? __ldg(reinterpret_cast<const float4*>(grad + (size_t)row * 64 + c))
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-            sg[r][c] = v.x; sg[r][c + 1] = v.y; sg[r][c + 2] = v.z; sg[r][c + 3] = v.w;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (uint32_t r = 0; r < kDwRows; ++r) {
-            float a[4], b[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) { a[q] = sp[r][ti + q]; b[q] = sg[r][to + q]; }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(a[u], b[v], acc[u][v]);
-        }
-        if (threadIdx.x < 64u)
-            for (uint32_t r = 0; r < kDwRows; ++r) sb += sg[r][threadIdx.x];
     }
-    float* gw = L.gw[l];
+    // the last one or two tiles' MMAs
+    if (ok) {
+        const uint32_t n = t1 - t0;
+        if (tid == 0) {
+            bool done = true;
+            for (uint32_t back = (n >= 2u ? 2u : 1u); back >= 1u && done; --back) {
+                const uint32_t st = (n - back) & 1u;
+                done = false;
+                for (uint32_t it = 0; it < spin && !done; ++it) done = mbar_try_wait(&bar[st], (phases >> st) & 1u);
+                if (done) phases ^= 1u << st;
+            }
+            *s_ok = done ? 1 : 0;
+        }
+        __syncthreads();
+        ok = *s_ok != 0;
+    }
+    tc_fence_after();
+    if (ok) {
+        // D rows 0..64 -> shared memory (stage-0 A buffer, free now) -> coalesced atomics
+        float* sD = reinterpret_cast<float*>(smem + kDwSmemA0);       // [65][64]
+        if (warp < 3) {
+            float v[64];
+            const uint32_t lane_addr = taddr + ((32u * warp) << 16);
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+            for (int j = 0; j < 4; ++j) tmem_ld16(lane_addr + 16u * j, v + 16 * j);
+            tmem_wait_ld();
+            const uint32_t drow = 32u * warp + (tid & 31u);
+            if (drow <= 64u) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) atomicAdd(&gw[(ti + u) * 64u + to + v], acc[u][v]);
-    if (threadIdx.x < 64u) atomicAdd(&L.gb[l][threadIdx.x], sb);
+                for (int j = 0; j < 64; ++j) sD[drow * 64u + j] = v[j];
+            }
+        }
+        __syncthreads();
+        float* gw = pick(L.gw[0], L.gw[1], L.gw[2], L.gw[3]);
+        float* gb = pick(L.gb[0], L.gb[1], L.gb[2], L.gb[3]);
+        for (uint32_t i = tid; i < 64u * 64u; i += blockDim.x) atomicAdd(&gw[i], sD[i]);
+        if (tid < 64u) atomicAdd(&gb[tid], sD[64u * 64u + tid]);
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    // every MMA this CTA issued must have landed before its tensor memory is freed
+    if (!ok && tid == 0) {
+        for (uint32_t st = 0; st < 2; ++st) {
+            uint32_t it = 0;
+            while (!mbar_try_wait(&bar[st], (phases >> st) & 1u) && ++it < kSpin) {}
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr, 64);
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master parameters
@@ -351,22 +436,29 @@ cudaError_t pack_weights(const float* params, uint8_t* w_fwd, uint8_t* w_bwd, cu
     return cudaGetLastError();
 }
 cudaError_t mix_grad(const float* out, const float* dirs, const float* w, uint32_t m, float* wsum, uint4* dy_bf,
-                     float* dy_f, float* loss, cudaStream_t s) {
+                     float* loss, cudaStream_t s) {
     if (m == 0) return cudaSuccess;
     k_sum<<<256, 256, 0, s>>>(w, m, wsum);
-    k_mix_grad<<<(m + 127) / 128, 128, 0, s>>>(out, dirs, w, m, wsum, dy_bf, dy_f, loss);
+    k_mix_grad<<<(m + 127) / 128, 128, 0, s>>>(out, dirs, w, m, wsum, dy_bf, loss);
     return cudaGetLastError();
 }
-cudaError_t weight_grad(const DwLayers& L, uint32_t m, cudaStream_t s) {
+cudaError_t weight_grad(const DwLayers& L, uint32_t m, uint32_t spin, int* err, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDwSmemBytes);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
     if (m == 0) return cudaSuccess;
     int dev = 0, sms = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // four blocks per SM over the four layers
-    uint32_t gx = (uint32_t)sms;
-    const uint32_t chunks = (m + kDwRows - 1) / kDwRows;
-    if (gx > chunks) gx = chunks;
-    k_dw<<<dim3(gx, 4), 256, 0, s>>>(L, m);
+    // two CTAs per SM over the four layers; each CTA walks a contiguous run of K-tiles
+    const uint32_t ntiles = (m + kDwK - 1) / kDwK;
+    const uint32_t per_layer = std::max<uint32_t>(1u, (uint32_t)sms / 2u);
+    const uint32_t tiles_per_cta = (ntiles + per_layer - 1) / per_layer;
+    const uint32_t gx = (ntiles + tiles_per_cta - 1) / tiles_per_cta;
+    k_dw_tc<<<dim3(gx, 4), 128, kDwSmemBytes, s>>>(L, m, tiles_per_cta, spin, err);
     return cudaGetLastError();
 }
 cudaError_t adam(float* params, const float* grads, float* m1, float* m2, uint32_t n, float lr, uint32_t step,

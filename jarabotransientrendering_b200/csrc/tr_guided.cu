@@ -199,7 +199,8 @@ __global__ void __launch_bounds__(128, 4) k_guide(const __grid_constant__ Params
         }
         float o[48];
         for (uint32_t l = 0; l < 4; ++l) {
-            ok = trg::layer_mma(taddr, trg::smem_u32(sA), trg::smem_u32(smem + trg::kSmemW + l * 8192u), bar, phase, s_ok);
+            ok = trg::layer_mma(taddr, trg::smem_u32(sA), trg::smem_u32(smem + trg::kSmemW + l * 8192u), bar, phase, s_ok,
+                                G.net.spin);
             if (!ok) break;
             if (l < 3) {
                 float a[64];

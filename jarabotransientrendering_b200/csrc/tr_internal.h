@@ -80,9 +80,9 @@ struct tr_guide {
     uint4* act = nullptr;
     float* out = nullptr;
     uint4* dy_bf = nullptr;
-    float* dy_f = nullptr;
-    float* dh = nullptr;
+    uint4* dh = nullptr;       // BF16 hidden-layer gradients [3][n][64]
     uint32_t step = 0;
+    uint32_t spin = trg::kWaitPolls;   // mbarrier polls before a tensor-core wait times out
     template <class T>
     T* alloc(size_t n) {
         T* p = tri::dalloc<T>(n, bytes);
@@ -96,16 +96,15 @@ struct tr_guide {
     }
     trg::GuideDev dev() const {
         return trg::GuideDev{reinterpret_cast<const uint4*>(w_fwd), reinterpret_cast<const uint4*>(w_bwd),
-                             params + 4 * 4096};
+                             params + 4 * 4096, spin};
     }
     void ensure(uint32_t n) {
         if (cap >= n) return;
-        drop(act); drop(out); drop(dy_bf); drop(dy_f); drop(dh);
+        drop(act); drop(out); drop(dy_bf); drop(dh);
         act = alloc<uint4>((size_t)3 * n * 8);
         out = alloc<float>((size_t)n * trg::kOut);
         dy_bf = alloc<uint4>((size_t)n * 8);
-        dy_f = alloc<float>((size_t)n * 64);
-        dh = alloc<float>((size_t)3 * n * 64);
+        dh = alloc<uint4>((size_t)3 * n * 8);
         cap = n;
     }
 };

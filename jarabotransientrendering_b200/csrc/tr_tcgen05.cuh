@@ -8,6 +8,8 @@
 #include <cstdint>
 #include <cuda_bf16.h>
 
+#include "tr_guide.cuh"
+
 namespace trg {
 
 // ---------------------------------------------------------------------------------------------
@@ -87,7 +89,10 @@ __host__ __device__ __forceinline__ uint32_t canon_off(uint32_t row, uint32_t k)
     return (row >> 3) * 1024u + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
 }
 
-constexpr uint32_t kSpin = 1u << 24;    // bounded mbarrier wait
+// mbarrier polls before a wait for the CTA's own MMAs counts as timed out: the default wait
+// limit of the kernels' completion waits (host-settable per guide) and the fixed bound of the
+// drain wait that always lets in-flight MMAs land before tensor memory is freed
+constexpr uint32_t kSpin = kWaitPolls;
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -96,10 +101,11 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 __device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
 
-// Issues the four K=16 MMAs of one layer and waits (bounded) for them; returns false on timeout.
-// Called by all threads; thread 0 issues and waits, the others meet it at the barrier.
+// Issues the four K=16 MMAs of one layer and waits for them, polling the mbarrier at most `spin`
+// times (0: no wait at all - the wait times out at once); returns false on timeout.  Called by
+// all threads; thread 0 issues and waits, the others meet it at the barrier.
 __device__ __forceinline__ bool layer_mma(uint32_t taddr, uint32_t a_addr, uint32_t b_addr, uint64_t* bar,
-                                          uint32_t& phase, volatile int* s_ok) {
+                                          uint32_t& phase, volatile int* s_ok, uint32_t spin) {
     fence_proxy_async();
     tc_fence_before();
     __syncthreads();
@@ -109,9 +115,8 @@ __device__ __forceinline__ bool layer_mma(uint32_t taddr, uint32_t a_addr, uint3
         for (uint32_t k = 0; k < 4; ++k)
             umma_bf16(taddr, smem_desc(a_addr + k * 256u), smem_desc(b_addr + k * 256u), kIdesc, k > 0 ? 1u : 0u);
         umma_commit(bar);
-        uint32_t it = 0;
         bool done = false;
-        while (!(done = mbar_try_wait(bar, phase)) && ++it < kSpin) {}
+        for (uint32_t it = 0; it < spin && !done; ++it) done = mbar_try_wait(bar, phase);
         *s_ok = done ? 1 : 0;
     }
     __syncthreads();

@@ -2,8 +2,9 @@
 
 numpy restatement of the proposal network and its training step, rounding to BF16 at the same
 points as the CUDA kernels: features, weights and hidden activations are BF16, products are
-accumulated in FP32 (here: float64, then compared with a tolerance), the output-layer gradient
-feeds the hidden-layer backward as BF16 and the weight gradients as FP32.
+accumulated in FP32 (here: float64, then compared with a tolerance), and the gradients w.r.t.
+each layer's outputs are BF16 both where they feed the next backward layer and where they are
+the weight-gradient GEMM's operand (the tensor-core kernel k_dw_tc: BF16 x BF16 -> FP32).
 
 Mixture of 8 von Mises-Fisher lobes (per lobe: weight logit, unnormalised mean, concentration
 kappa = 0.05 + 2000 sigmoid(k - 8), log-like below a few hundred and smoothly saturating at
@@ -114,19 +115,18 @@ def gradients(params, x, dirs, w):
     loss, dout = loss_and_dout(out, dirs, w)
     dy = np.zeros((len(x), 64))
     dy[:, :40] = dout
-    dy_f = dy.astype(np.float32).astype(np.float64)
     dy_b = bf16(dy.astype(np.float32)).astype(np.float64)
     H = [x.astype(np.float64)] + [a.astype(np.float64) for a in acts]
     gW = np.zeros((4, 64, 64))
     gb = np.zeros((4, 64))
-    gW[3] = H[3].T @ dy_f
-    gb[3] = dy_f.sum(axis=0)
+    gW[3] = H[3].T @ dy_b
+    gb[3] = dy_b.sum(axis=0)
     g_in = dy_b
     for l in (3, 2, 1):
         dh = (g_in @ Wb[l].T) * (H[l] > 0)
-        gW[l - 1] = H[l - 1].T @ dh
-        gb[l - 1] = dh.sum(axis=0)
         g_in = bf16(dh.astype(np.float32)).astype(np.float64)
+        gW[l - 1] = H[l - 1].T @ g_in
+        gb[l - 1] = g_in.sum(axis=0)
     return loss, np.concatenate([gW.reshape(-1), gb.reshape(-1)]).astype(np.float32)
 
 

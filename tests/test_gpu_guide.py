@@ -143,3 +143,58 @@ def test_guide_errors(gpu):
         assert rc == 1
     finally:
         _abi.lib().tr_guide_destroy(g)
+
+
+def test_wait_timeout_is_reported_and_the_guide_recovers(gpu):
+    """With a wait limit of 0 every tensor-core completion wait gives up at once: the forward
+    pass, a training step and a guided render each return TR_ERR_TIMEOUT (the kernels first let
+    their in-flight MMAs land and free their tensor memory); with the limit restored, the same
+    guide and context compute correct results again."""
+    import torch
+    import jarabotransientrendering_b200 as T
+    from jarabotransientrendering_b200 import renderer as R, scenes as S
+    L = _abi.lib()
+    rng = np.random.default_rng(5)
+    n = 1000
+    params = rng.normal(0, 0.15, G.NP).astype(np.float32)
+    x = _features(rng, n)
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    w = (rng.random(n) + 0.05).astype(np.float32)
+    g = _guide()
+    try:
+        _abi.check(L.tr_guide_set_params(g, params.ctypes.data))
+        xd = _bits(x)
+        dd = _dev(dirs.astype(np.float32), torch.float32)
+        wd = _dev(w, torch.float32)
+        out = torch.zeros((n, 40), dtype=torch.float32, device="cuda")
+        _ready()
+        _abi.check(L.tr_guide_set_wait_limit(g, 0))
+        assert L.tr_guide_forward(g, C.c_void_p(xd.data_ptr()), n, C.c_void_p(out.data_ptr()), None) == 5
+        assert L.tr_guide_train_step(g, C.c_void_p(xd.data_ptr()), C.c_void_p(dd.data_ptr()),
+                                     C.c_void_p(wd.data_ptr()), n, 0.0, None, None) == 5
+        _abi.check(L.tr_guide_set_wait_limit(g, 1 << 24))
+        _abi.check(L.tr_guide_forward(g, C.c_void_p(xd.data_ptr()), n, C.c_void_p(out.data_ptr()), None))
+        got = out.cpu().numpy()
+    finally:
+        L.tr_guide_destroy(g)
+    ref, _ = G.forward(params, x)
+    scale = np.abs(ref).max() + 1e-6
+    assert np.abs(got - ref).max() <= 2e-2 * scale
+
+    sc = S.guided(width=32, height=32, time_bins=128, exposure=0.04, sqrt_spp=2, max_bounces=4)
+    sc.flags = S.FLAG_ORTHONORMAL_FRAME
+    gd = R.Guide(device=0, seed=1)
+    try:
+        with R.Context(sc, 0) as ctx:
+            ctx.set_guide(gd, mix_prob=0.5, learning_rate=1e-3, train_pool=4096)
+            _abi.check(L.tr_guide_set_wait_limit(gd.h, 0))
+            with pytest.raises(T.TransientError, match="timed out"):
+                ctx.render(0, sc.spp)
+            _abi.check(L.tr_guide_set_wait_limit(gd.h, 1 << 24))
+            ctx.clear()
+            ctx.render(sc.spp, sc.spp)
+            f = ctx.film()
+            assert np.isfinite(f["streak"]).all() and f["streak"].sum() > 0
+    finally:
+        gd.close()
