@@ -194,12 +194,22 @@ public:
     void render(const char* name, World<D, Radiance>& world, Integrator<D, Radiance, RadianceAttenuation>* integrator,
                 const Camera<D>& camera, Film<D, Radiance>* film, Sampler* sampler) const override {
         if (!integrator) throw std::runtime_error("Error: Need to define an integrator for rendering\n");
+        if (!film || !sampler) throw std::runtime_error("GPU renderer: film and sampler are required");
         tr_film f{};
         f.width = (uint32_t)film->get_width();
         f.height = (uint32_t)film->get_height();
         f.time_bins = film->get_time_resolution();
         f.exposure = film->get_exposure_time();
         f.offset = film->get_time_offset();
+        // the GPU renders the captured configuration: the reference's film and sampler must
+        // describe the same frame (StratifiedSampler::get_nb_samples = W x H x sqrt_spp^2)
+        const size_t spp = (size_t)m_integrator.sqrt_spp * m_integrator.sqrt_spp;
+        const size_t want = (size_t)f.width * f.height * spp;
+        if (sampler->get_nb_samples() != want)
+            throw std::runtime_error("GPU renderer: the sampler draws " + std::to_string(sampler->get_nb_samples()) +
+                                     " samples but the film (" + std::to_string(f.width) + "x" +
+                                     std::to_string(f.height) + ") at the captured " + std::to_string(spp) +
+                                     " samples per pixel needs " + std::to_string(want));
         tr_scene s = m_scene.view();
         tr_ctx* ctx = nullptr;
         check(tr_create(&s, &m_camera, &f, &m_integrator, m_device, &ctx));

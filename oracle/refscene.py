@@ -35,6 +35,9 @@ def build_ref(ref_src=REF_SRC):
     if os.path.isdir(ref_src):
         subprocess.check_call(["make", "-s", "-j", str(os.cpu_count() or 4), "-C", HERE, "ref",
                                f"REF_SRC={ref_src}"])
+        lib = os.path.join(os.path.dirname(HERE), "jarabotransientrendering_b200", "libtransient_b200.so")
+        if os.path.exists(lib):             # the adaptor program links the CUDA library
+            subprocess.check_call(["make", "-s", "-C", HERE, "adaptor", f"REF_SRC={ref_src}"])
     return ref_available()
 
 
