@@ -9,7 +9,8 @@ copy of the FP64 film and one reduction, which lie outside the timed render call
 
 The comparison of samplers (``time_to_error``) times each ``Context.render`` call with the host
 clock: that call returns after the pass is on the film and, with a learned proposal attached,
-after the network has been trained on the pass's samples, so training counts as render time.
+after the network has been trained on the previous pass's samples (that training runs beside
+the pass's rendering, within the call), so training counts as render time.
 """
 from __future__ import annotations
 

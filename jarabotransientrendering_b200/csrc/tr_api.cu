@@ -305,22 +305,34 @@ void ensure_lane_guided(tr_ctx* x, int k) {
 }
 
 void ensure_guided(tr_ctx* x, uint32_t capacity) {
-    if (x->gw_capacity >= capacity && x->gw.pool_cap == x->guide_pool && x->pool_state) return;
+    if (x->gw_capacity >= capacity && x->gw.pool_cap == x->guide_pool && x->pool_state && x->pool_alt.state) return;
     auto drop = [&](void* p) {
         if (!p) return;
         cudaFree(p);
         x->allocs.erase(std::remove(x->allocs.begin(), x->allocs.end(), p), x->allocs.end());
     };
     trk::GuideWave& g = x->gw;
+    tr_ctx::PoolBuf& a = x->pool_alt;
     drop(g.vrec); drop(g.pool_feat); drop(g.pool_dir); drop(g.pool_w); drop(g.pool_meta);
+    drop(a.feat); drop(a.dir); drop(a.w); drop(a.meta);
     g.vrec = x->alloc<uint4>((size_t)capacity * 5);
     const uint32_t pc = std::max<uint32_t>(1u, x->guide_pool);
     g.pool_feat = x->alloc<uint4>((size_t)pc * 8);
     g.pool_dir = x->alloc<float>((size_t)pc * 3);
     g.pool_w = x->alloc<float>(pc);
     g.pool_meta = x->alloc<uint4>(pc);
+    a.feat = x->alloc<uint4>((size_t)pc * 8);
+    a.dir = x->alloc<float>((size_t)pc * 3);
+    a.w = x->alloc<float>(pc);
+    a.meta = x->alloc<uint4>(pc);
     g.pool_cap = x->guide_pool;
     if (!x->pool_state) x->pool_state = x->alloc<uint32_t>(2);
+    if (!a.state) a.state = x->alloc<uint32_t>(2);
+    if (!x->w_snap) x->w_snap = x->alloc<uint4>(4 * 8192 / 16);
+    if (!x->bias_snap) x->bias_snap = x->alloc<float>(4 * 64);
+    if (!x->ev_snap) TR_CUDA(cudaEventCreateWithFlags(&x->ev_snap, cudaEventDisableTiming));
+    if (!x->ev_train) TR_CUDA(cudaEventCreateWithFlags(&x->ev_train, cudaEventDisableTiming));
+    x->pool_pending = 0;                 // a reallocated pool holds nothing to train on
     x->gw_capacity = capacity;
 }
 
@@ -350,6 +362,10 @@ trk::Params make_params(tr_ctx* x) {
     if (x->guide) {
         p.guide = x->gw;
         p.guide.net = guide_dev(x->guide);
+        if (x->w_snap) {                 // the render samples with the snapshot taken at its start
+            p.guide.net.w_fwd = x->w_snap;
+            p.guide.net.bias = x->bias_snap;
+        }
         p.guide.err = guide_err(x->guide);
     }
     return p;
@@ -359,7 +375,11 @@ trk::Params make_params(tr_ctx* x) {
 
 namespace {
 
-tr_status guide_after_render(tr_ctx* x, cudaStream_t s);
+// Guided renders: guide_begin_render snapshots the network for the render and starts training on
+// the previous render's samples beside it; guide_end_render waits for that training, reports
+// tensor-core timeouts and hands this render's pool to the next call.
+tr_status guide_begin_render(tr_ctx* x, cudaStream_t s);
+tr_status guide_end_render(tr_ctx* x, cudaStream_t s);
 
 // Host buffers the film is streamed into while rendering (tr_render_film): FP64 or FP32 sums
 // of the whole frame.
@@ -388,6 +408,8 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         x->gw.keep_prob = x->guide_pool ? std::min(1.0f, (float)x->guide_pool / (1.5f * (float)total_slots)) : 0.0f;
         x->gw.mix_prob = x->guide_mix;
         TR_CUDA(cudaMemsetAsync(x->pool_state, 0, 2 * sizeof(uint32_t), x->s()));
+        tr_status ts = guide_begin_render(x, x->s());
+        if (ts != TR_OK) return ts;
     }
     // samples per pixel per batch, and pixels per batch
     uint32_t ns_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(ns_total, cap / ninc));
@@ -523,10 +545,17 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             for (uint32_t d = 0; d < x->integ.max_bounces; ++d) {
                 tl(1, [&] { return trk::launch_extend(p, (int)d, x->trace_grid, ls); });
                 if (d > 0) TR_CUDA(order(lsh, ls));
-                tl(2, [&] { return trk::launch_shade(p, (int)d, ls); });
-                if (guided) {
+                if (guided && d < x->guide_depth) {
+                    tl(2, [&] { return trk::launch_shade(p, (int)d, ls); });
                     tl(5, [&] { return trk::launch_guide(p, (int)d, x->pool_state, ls); });
                     launches += 1;
+                } else if (guided) {
+                    // deeper vertices sample their BSDF in the shading kernel (unguided)
+                    trk::Params pu = p;
+                    pu.guide.vrec = nullptr;
+                    tl(2, [&] { return trk::launch_shade(pu, (int)d, ls); });
+                } else {
+                    tl(2, [&] { return trk::launch_shade(p, (int)d, ls); });
                 }
                 TR_CUDA(order(ls, lsh));
                 timed_on(3, lsh, [&] { return trk::launch_shadow(p, (int)d, x->trace_grid, lsh); });
@@ -627,7 +656,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     x->stats.paths += total_slots;
     x->stats.camera_samples += win_pix * ns_total;
     x->stats.render_ms = ms;
-    if (guided) return guide_after_render(x, strm);
+    if (guided) return guide_end_render(x, strm);
     return TR_OK;
 }
 
@@ -1279,7 +1308,11 @@ extern "C" tr_status tr_guide_create(int device, uint64_t seed, tr_guide** out) 
     try {
         g->device = device;
         TR_CUDA(cudaSetDevice(device));
-        TR_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        // highest priority: training steps that run beside a render get SMs as soon as the
+        // render's traversal blocks retire, instead of queueing behind its later launches
+        int lo = 0, hi = 0;
+        TR_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        TR_CUDA(cudaStreamCreateWithPriority(&g->stream, cudaStreamNonBlocking, hi));
         g->params = g->alloc<float>(TR_GUIDE_PARAMS);
         g->grads = g->alloc<float>(TR_GUIDE_PARAMS);
         g->m1 = g->alloc<float>(TR_GUIDE_PARAMS);
@@ -1462,15 +1495,64 @@ tr_status train_on_pool(tr_guide* g, const trk::GuideWave& gw, const uint32_t* p
 }  // namespace tri
 
 namespace {
-// After a guided render: surface an MMA timeout, then train on the collected pool.
-tr_status guide_after_render(tr_ctx* x, cudaStream_t s) {
-    return train_on_pool(x->guide, x->gw, x->pool_state, x->guide_pool, x->guide_lr, s, x->stats);
+tr_status guide_begin_render(tr_ctx* x, cudaStream_t s) {
+    tr_guide* g = x->guide;
+    x->stats.train_steps = 0;
+    try {
+        // the snapshot must not catch a training step of another render half-way
+        TR_CUDA(cudaEventRecord(x->ev_train, g->stream));
+        TR_CUDA(cudaStreamWaitEvent(s, x->ev_train, 0));
+        TR_CUDA(cudaMemcpyAsync(x->w_snap, g->w_fwd, 4 * 8192, cudaMemcpyDeviceToDevice, s));
+        TR_CUDA(cudaMemcpyAsync(x->bias_snap, g->params + 4 * 4096, 4 * 64 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        if (x->pool_pending == 0 || x->guide_lr <= 0.0f) return TR_OK;
+        // training on the previous render's pool runs on the guide's stream, after the snapshot
+        TR_CUDA(cudaEventRecord(x->ev_snap, s));
+        TR_CUDA(cudaStreamWaitEvent(g->stream, x->ev_snap, 0));
+        const uint32_t n = x->pool_pending, batch = 65536;
+        const tr_ctx::PoolBuf& a = x->pool_alt;
+        for (uint32_t off = 0; off + 1024 <= n; off += batch) {
+            const uint32_t m = std::min(batch, n - off);
+            train_enqueue(g, a.feat + (size_t)off * 8, a.dir + (size_t)off * 3, a.w + off, m, x->guide_lr, g->stream);
+            x->stats.train_steps += 1;
+        }
+        if (x->stats.train_steps)
+            TR_CUDA(cudaMemcpyAsync(&x->last_train_loss, g->scalars + 1, sizeof(float), cudaMemcpyDeviceToHost,
+                                    g->stream));
+        x->pool_pending = 0;
+    } catch (const CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
+    }
+    return TR_OK;
+}
+
+tr_status guide_end_render(tr_ctx* x, cudaStream_t s) {
+    tr_guide* g = x->guide;
+    uint32_t fill = 0;
+    try {
+        // the render has completed (render_region waited for it): its pool fill is final
+        TR_CUDA(cudaMemcpyAsync(&fill, x->pool_state, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TR_CUDA(cudaStreamSynchronize(s));
+        TR_CUDA(cudaStreamSynchronize(g->stream));     // the training that ran beside the render
+    } catch (const CudaError& e) {
+        return fail(TR_ERR_CUDA, e.what());
+    }
+    if (x->stats.train_steps) x->stats.train_loss = x->last_train_loss;
+    // this render's pool is trained during the next call; the other pool is filled next
+    trk::GuideWave& w = x->gw;
+    tr_ctx::PoolBuf& a = x->pool_alt;
+    std::swap(w.pool_feat, a.feat);
+    std::swap(w.pool_dir, a.dir);
+    std::swap(w.pool_w, a.w);
+    std::swap(w.pool_meta, a.meta);
+    std::swap(x->pool_state, a.state);
+    x->pool_pending = std::min(fill, x->guide_pool);
+    return guide_check_err(g, g->stream);             // tensor-core timeouts of render or training
 }
 }  // namespace
 
 extern "C" tr_status tr_set_guide(tr_ctx* x, tr_guide* g, float mix_prob, float lr, uint32_t train_pool) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
-    if (!g) { x->guide = nullptr; return TR_OK; }
+    if (!g) { x->guide = nullptr; x->pool_pending = 0; return TR_OK; }
     if (!(x->integ.flags & TR_FLAG_ORTHONORMAL_FRAME))
         return fail(TR_ERR_INVALID_ARGUMENT, "guided rendering needs TR_FLAG_ORTHONORMAL_FRAME (MIS needs the exact BSDF density)");
     if (x->integ.flags & TR_FLAG_BIDIRECTIONAL)
@@ -1483,6 +1565,13 @@ extern "C" tr_status tr_set_guide(tr_ctx* x, tr_guide* g, float mix_prob, float 
     x->guide_mix = mix_prob;
     x->guide_lr = lr;
     x->guide_pool = train_pool;     // ensure_guided reallocates the pool when its size changes
+    x->pool_pending = 0;            // samples collected for another guide are not trained on
+    return TR_OK;
+}
+
+extern "C" tr_status tr_set_guide_depth(tr_ctx* x, uint32_t depths) {
+    if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    x->guide_depth = depths;
     return TR_OK;
 }
 

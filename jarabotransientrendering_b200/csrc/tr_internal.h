@@ -177,6 +177,18 @@ struct tr_ctx {
     trk::GuideWave gw{};
     uint32_t gw_capacity = 0;
     uint32_t* pool_state = nullptr;       // [0] pool fill, [1] entries with targets
+    // Training pools are double-buffered: a render fills the pool in gw while the samples of the
+    // previous render (pool_alt, pool_pending entries) train the proposal beside it, on the
+    // guide's stream.  The render samples with a snapshot of the network (w_snap, bias_snap)
+    // taken when it starts, so the training it overlaps never changes the proposal mid-render.
+    struct PoolBuf { uint4* feat = nullptr; float* dir = nullptr; float* w = nullptr; uint4* meta = nullptr;
+                     uint32_t* state = nullptr; };
+    PoolBuf pool_alt{};
+    uint32_t pool_pending = 0;
+    uint4* w_snap = nullptr;              // packed forward tiles of the render's network (32 KB)
+    float* bias_snap = nullptr;           // and its biases [4][64]
+    cudaEvent_t ev_snap = nullptr, ev_train = nullptr;
+    uint32_t guide_depth = 0xffffffffu;   // path depths whose surface vertices use the proposal
     float last_train_loss = 0.0f;
     uint32_t train_steps = 0;
     cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null
@@ -198,6 +210,8 @@ struct tr_ctx {
         return p;
     }
     void release() {
+        if (ev_snap) { cudaEventDestroy(ev_snap); ev_snap = nullptr; }
+        if (ev_train) { cudaEventDestroy(ev_train); ev_train = nullptr; }
         for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
         prof_events.clear();
         for (cudaEvent_t e : dep_events) cudaEventDestroy(e);

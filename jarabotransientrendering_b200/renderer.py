@@ -173,6 +173,11 @@ class Context:
                                            learning_rate, train_pool))
         self._guide = guide
 
+    def set_guide_depth(self, depths):
+        """Only surface vertices at path depth < depths sample with the proposal
+        (tr_set_guide_depth); deeper ones sample their BSDF."""
+        _abi.check(_abi.lib().tr_set_guide_depth(self.h, depths))
+
     def stats(self):
         s = _abi.Stats()
         _abi.check(_abi.lib().tr_stats_get(self.h, C.byref(s)))

@@ -104,6 +104,8 @@ def test_guided_render_on_wave_lanes_is_unbiased_and_trains(gpu):
 
 
 def test_guided_training_updates_the_network(gpu):
+    """Each render call trains the proposal on the previous call's samples (beside its own
+    rendering), so the first call trains nothing and every later one at least one step."""
     sc = guided_scene(64, 64, 128, 0.04)
     g = gpu.Guide(seed=9)
     try:
@@ -114,6 +116,10 @@ def test_guided_training_updates_the_network(gpu):
             for k in range(6):
                 ctx.render(16 * k, 16)
                 st = ctx.stats()
+                if k == 0:
+                    assert st["train_steps"] == 0
+                    assert np.array_equal(g.params(), p0)
+                    continue
                 assert st["train_steps"] >= 1
                 losses.append(st["train_loss"])
             f = ctx.film()
