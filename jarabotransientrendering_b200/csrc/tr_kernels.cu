@@ -442,10 +442,13 @@ __device__ __noinline__ TaSample time_angular_sample(f3 l, float mod, float r, f
 
 // kTimeSampling: compiled with the time-sampling branches (a launch whose context, or some
 // context of whose batch, has TR_FLAG_TIME_SAMPLING; the flag is still read per slot).
-// The plain variant is held to 64 registers (4 CTAs per SM instead of 3; a few spilled
-// values stay in L1), which the latency-bound kernel turns into ~6 % less time.
+// Register budgets (the kernel is latency-bound, so resident warps matter more than a few
+// spilled values, which stay in L1): the plain variant 64 registers (4 CTAs per SM); the guided
+// and time-sampling variants 80 (3 CTAs per SM; unbounded they took 146-172 registers and ran
+// one CTA of 8 warps per SM); the multi-scene variants 128 (2 CTAs, no spills).
 template <bool kGuided, bool kMulti, bool kTimeSampling>
-__global__ void __launch_bounds__(256, (kGuided || kMulti || kTimeSampling) ? 1 : 4) k_shade(const __grid_constant__ Params p, int depth) {
+__global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) ? 3 : 4))
+    k_shade(const __grid_constant__ Params p, int depth) {
     uint32_t n0 = p.batch.n_slots;
     if constexpr (kMulti) n0 = cur_batch(p).n_slots;
     const uint32_t n = depth == 0 ? n0 : p.wave.counters[cnt_ext(depth)];
