@@ -454,6 +454,7 @@ def batched(args, device, frames=2):
             guided_films[i] = None
             torch.cuda.empty_cache()
         res["accuracy_vs_plain"] = acc
+        res["small_scenes"] = batched_small(device)
         res["speedup_batched_guided_vs_sequential_plain"] = res["guided"]["paths_per_s"] / res["plain_sequential"]["paths_per_s"]
         res["timed_sample_begin"] = begin_timed[:1]
     finally:
@@ -462,6 +463,59 @@ def batched(args, device, frames=2):
             c.close()
         torch.cuda.empty_cache()
     return res
+
+
+def batched_small(device, scenes=64, frames=3):
+    """Many small scenes (scenes.small_batch_scenes: 64 scenes of 64 x 64 pixels x 32 spp,
+    131,072 paths each): plain rendering in shared CUDA-graph batches (autotuned) beside the
+    same contexts rendered one after another, both by host wall clock around a frame."""
+    import torch
+    from jarabotransientrendering_b200 import renderer as R, scenes as S
+    scs = S.small_batch_scenes(n=scenes)
+    spp = [sc.spp for sc in scs]
+    paths_frame = sum(sc.paths_per_frame() for sc in scs)
+    ctxs = [R.Context(sc, device) for sc in scs]
+    out = {"workload": f"{scenes} scenes of 64x64 pixels, 256 bins, 32 spp (16 x 2), 1,314-327,714 triangles",
+           "paths_per_frame": paths_frame}
+    try:
+        # the batch renders at most 16 scenes: groups of 16 contexts, one batch object each
+        groups = [ctxs[i:i + 16] for i in range(0, len(ctxs), 16)]
+        batches = [R.Batch(g) for g in groups]
+        nxt = 0
+        for B, g in zip(batches, groups):
+            B.autotune(0, [1] * len(g))
+        def frame_batched():
+            nonlocal nxt
+            torch.cuda.synchronize(device)
+            t = time.perf_counter()
+            for B, g in zip(batches, groups):
+                B.render([nxt] * len(g), [c.scene.spp for c in g])
+            torch.cuda.synchronize(device)
+            nxt += max(spp)
+            return time.perf_counter() - t
+        def frame_sequential():
+            nonlocal nxt
+            torch.cuda.synchronize(device)
+            t = time.perf_counter()
+            for c, k in zip(ctxs, spp):
+                c.render(nxt, k)
+            torch.cuda.synchronize(device)
+            nxt += max(spp)
+            return time.perf_counter() - t
+        frame_batched()
+        frame_sequential()
+        tb = min(frame_batched() for _ in range(frames))
+        ts = min(frame_sequential() for _ in range(frames))
+        out["plain_batched"] = {"paths_per_s": paths_frame / tb, "ms_per_frame": tb * 1e3}
+        out["plain_sequential"] = {"paths_per_s": paths_frame / ts, "ms_per_frame": ts * 1e3}
+        out["speedup_batched_vs_sequential"] = ts / tb
+        for B in batches:
+            B.close()
+    finally:
+        for c in ctxs:
+            c.close()
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():

@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(128, 4) k_mlp_bwd(GuideDev g, const uint4* __r
     drain_and_free(taddr, bar, phase, ok);
 }
 
-int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem) {
+int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem, int tmem_cols) {
     int sms = 1, smem_sm = 0, regs_sm = 0, warps_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
@@ -154,7 +154,7 @@ int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem) 
     const int regs = fa.numRegs > 0 ? ((fa.numRegs + 7) / 8) * 8 : 1;
     int per_sm = std::min(smem_sm / per_cta_smem, regs_sm / (regs * threads));
     per_sm = std::min(per_sm, warps_sm / threads);
-    per_sm = std::min(per_sm, 512 / 64);                                          // 64 TMEM columns each
+    per_sm = std::min(per_sm, 512 / tmem_cols);                                   // TMEM columns each
     if (per_sm < 1) per_sm = 1;
     return (sms > 0 ? sms : 1) * per_sm;
 }

@@ -40,8 +40,8 @@ cudaError_t mlp_backward(const GuideDev& g, const uint4* dy, const uint4* act, u
                          cudaStream_t s);
 int mlp_grid(int device);
 // CTAs of `kernel` that fit on the device at once (SMs x CTAs per SM, from the kernel's
-// registers and shared memory), for persistent tile loops
-int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem);
+// registers, shared memory and `tmem_cols` tensor-memory columns per CTA), for persistent loops
+int resident_grid(int device, const void* kernel, int threads, size_t dyn_smem, int tmem_cols = 64);
 cudaError_t pack_weights(const float* params, uint8_t* w_fwd, uint8_t* w_bwd, cudaStream_t s);
 cudaError_t mix_grad(const float* out, const float* dirs, const float* w, uint32_t m, float* wsum, uint4* dy_bf,
                      float* loss, cudaStream_t s);

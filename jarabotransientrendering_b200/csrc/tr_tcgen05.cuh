@@ -139,6 +139,36 @@ __device__ __forceinline__ void drain_and_free(uint32_t taddr, uint64_t* bar, ui
 constexpr uint32_t kSmemW = 0, kSmemA = 32768, kSmemBias = 49152, kSmemBar = 50176, kSmemSlot = 50184,
                    kSmemOk = 50188, kSmemBytes = 50192;
 
+// Two-tile variant (the renderer's fused guided-sampling kernel): 4 weight tiles (32 KB) | A
+// tiles of two 128-row tiles (16 KB each) | bias (1 KB) | two mbarriers | tmem slot | flag.  The
+// two tiles' MMA chains are interleaved: both layers' MMAs are issued back to back, so one
+// tile's MMAs run while the CTA turns the other tile's accumulators into the next A operand.
+constexpr uint32_t kG2W = 0, kG2A0 = 32768, kG2A1 = 49152, kG2Bias = 65536, kG2Bar = 66560, kG2Slot = 66576,
+                   kG2Ok = 66580, kG2Bytes = 66592;
+
+// Thread 0 polls `bar` for completion of `phase` at most `spin` times; the result is made
+// CTA-uniform through shared memory and a barrier (every thread must call this).
+__device__ __forceinline__ bool wait_uniform(uint64_t* bar, uint32_t phase, volatile int* s_ok, uint32_t spin) {
+    if (threadIdx.x == 0) {
+        bool done = false;
+        for (uint32_t it = 0; it < spin && !done; ++it) done = mbar_try_wait(bar, phase);
+        *s_ok = done ? 1 : 0;
+    }
+    __syncthreads();
+    const bool ok = *s_ok != 0;
+    tc_fence_after();
+    return ok;
+}
+
+// Issues one layer's four K=16 MMAs (A tile x weight tile -> 128 x 64 FP32 accumulator in tensor
+// memory) and commits them to `bar`.  Thread 0 only; the caller fences and synchronises first.
+__device__ __forceinline__ void issue_layer(uint32_t taddr, uint32_t a_addr, uint32_t b_addr, uint64_t* bar) {
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k)
+        umma_bf16(taddr, smem_desc(a_addr + k * 256u), smem_desc(b_addr + k * 256u), kIdesc, k > 0 ? 1u : 0u);
+    umma_commit(bar);
+}
+
 __device__ __forceinline__ void stage_weights(uint8_t* smem, const uint4* w, const float* bias) {
     uint4* sw = reinterpret_cast<uint4*>(smem + kSmemW);
     for (uint32_t i = threadIdx.x; i < 2048u; i += blockDim.x) sw[i] = __ldg(&w[i]);

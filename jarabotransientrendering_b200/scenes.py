@@ -458,6 +458,22 @@ def batch_scenes(seed=1, n=16):
     return [batch_scene(i, seed) for i in range(n)]
 
 
+def small_batch_scenes(seed=1, n=64):
+    """Many small scenes: the batch workload's scenes (see ``batch_scene``) at 64 x 64 pixels,
+    256 time bins and 32 samples per pixel (4 x 4 camera samples x 2 incoming paths), i.e.
+    131,072 paths each -- scenes too small to fill the GPU one at a time."""
+    out = []
+    for i in range(n):
+        sc = batch_scene(i % 16, seed + i // 16)
+        sc.width = sc.height = 64
+        sc.time_bins = 256
+        sc.exposure = 5.12 / 256
+        sc.sqrt_spp, sc.incoming_samples = 4, 2
+        sc.name = f"small{i:02d}"
+        out.append(sc)
+    return out
+
+
 WORKLOADS = {"cornell": cornell, "icosphere": icosphere, "medium": medium, "guided": guided}
 
 
