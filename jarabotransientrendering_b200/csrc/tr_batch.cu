@@ -10,7 +10,8 @@
 // (*cur), so the launch sequence of a batch does not depend on the batch and is captured once:
 //   memset(counters) -> raygen -> depth x (extend, shade, [guide], shadow) -> [train gather]
 //   -> splat -> advance(*cur)
-// and replayed with cudaGraphLaunch for every batch.
+// for each of four wave lanes (own wave buffers, cursor and stream pair; lane k renders batches
+// k, k + 4, ...) as parallel branches of one graph, replayed once per group of four batches.
 #include "tr_internal.h"
 
 #include <chrono>
@@ -20,10 +21,11 @@ using namespace tri;
 
 struct tr_batch {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;          // lane 0's stream (every call forks from and joins it)
     cudaStream_t shadow_stream = nullptr;   // shadow launches beside the next depth's extend
-    // the second lane: every other batch, on its own wave and stream pair
-    cudaStream_t stream1 = nullptr, shadow_stream1 = nullptr;
+    // lanes 1..kLanes-1: batch k runs on lane k mod kLanes, each with its own wave and streams
+    static constexpr int kLanes = 4;
+    cudaStream_t lane_stream[kLanes - 1] = {}, lane_shadow[kLanes - 1] = {};
     cudaEvent_t dep[8] = {};                // ordering events between the streams, used in turn
     uint32_t next_dep = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -36,7 +38,7 @@ struct tr_batch {
     uint32_t batches_cap = 0;
     uint32_t* d_cur = nullptr;              // [lane]: index of the batch the lane is on
     trk::Wave wave{};
-    trk::Wave wave1{};                      // the second lane's (shares wave.stats)
+    trk::Wave lane_wave[kLanes - 1]{};      // the other lanes' (share wave.stats)
     uint32_t max_bounces = 1, bvh_depth = 0;
     int trace_grid = 0;
     tr_batch_config cfg{1u << 21, 256, 1, 1};
@@ -46,7 +48,7 @@ struct tr_batch {
     float mix = 0.5f, lr = 1e-3f;
     uint32_t pool = 0;
     trk::GuideWave gw{};
-    uint4* vrec1 = nullptr;                 // the second lane's guided-vertex records
+    uint4* lane_vrec[kLanes - 1] = {};      // the other lanes' guided-vertex records
     uint32_t gw_capacity = 0;
     uint32_t* pool_state = nullptr;
 
@@ -159,10 +161,12 @@ Plan make_plan(const tr_batch* b, const uint64_t* s_begin, const uint32_t* s_cou
 void ensure_lane(tr_batch* b, trk::Wave& w, uint32_t capacity, unsigned long long* stats);
 
 void ensure_batch_wave(tr_batch* b, uint32_t capacity) {
-    if (b->wave.capacity == capacity && b->wave1.capacity == capacity) return;
+    bool same = b->wave.capacity == capacity;
+    for (const trk::Wave& w : b->lane_wave) same = same && w.capacity == capacity;
+    if (same) return;
     b->drop_graph();
     ensure_lane(b, b->wave, capacity, nullptr);
-    ensure_lane(b, b->wave1, capacity, b->wave.stats);
+    for (trk::Wave& w : b->lane_wave) ensure_lane(b, w, capacity, b->wave.stats);
 }
 
 // one lane's wave buffers; `stats` null: allocate the statistics counters, else share them
@@ -203,8 +207,10 @@ void ensure_batch_guided(tr_batch* b, uint32_t capacity) {
     trk::GuideWave& g = b->gw;
     b->drop(g.vrec); b->drop(g.pool_feat); b->drop(g.pool_dir); b->drop(g.pool_w); b->drop(g.pool_meta);
     g.vrec = b->alloc<uint4>((size_t)capacity * 5);
-    b->drop(b->vrec1);
-    b->vrec1 = b->alloc<uint4>((size_t)capacity * 5);
+    for (uint4*& v : b->lane_vrec) {
+        b->drop(v);
+        v = b->alloc<uint4>((size_t)capacity * 5);
+    }
     const uint32_t pc = std::max<uint32_t>(1u, b->pool);
     g.pool_feat = b->alloc<uint4>((size_t)pc * 8);
     g.pool_dir = b->alloc<float>((size_t)pc * 3);
@@ -217,7 +223,7 @@ void ensure_batch_guided(tr_batch* b, uint32_t capacity) {
 
 trk::Params batch_params(const tr_batch* b, const Plan& pl, int lane) {
     trk::Params p{};
-    p.wave = lane ? b->wave1 : b->wave;
+    p.wave = lane ? b->lane_wave[lane - 1] : b->wave;
     p.bvh_depth = b->bvh_depth;
     p.max_bounces = b->max_bounces;
     p.multi.scenes = b->d_scenes;
@@ -230,7 +236,7 @@ trk::Params batch_params(const tr_batch* b, const Plan& pl, int lane) {
         p.guide = b->gw;
         p.guide.net = guide_dev(b->guide);
         p.guide.err = guide_err(b->guide);
-        if (lane) p.guide.vrec = b->vrec1;
+        if (lane) p.guide.vrec = b->lane_vrec[lane - 1];
         p.guide.tag = 1u;       // the lanes fill the pool at once: entries tagged by batch index
     }
     return p;
@@ -262,17 +268,17 @@ void enqueue_batch(tr_batch* b, const trk::Params& p, cudaStream_t s, cudaStream
     if (b->max_bounces) order(b, sh, s);
     if (guided && b->pool) { TR_CUDA(trk::launch_train_gather(p, b->pool_state, s)); count += 2; }
     TR_CUDA(trk::launch_splat(p, s));
-    TR_CUDA(trk::launch_advance(p.multi.cur, 2u, s));   // this lane's next batch
+    TR_CUDA(trk::launch_advance(p.multi.cur, (uint32_t)tr_batch::kLanes, s));   // this lane's next batch
     count += 3;
 }
 
-// Two batches, one per lane: lane 1 forks from the main stream and joins it again, so a
-// capture of the pair holds both as parallel branches.
-void enqueue_pair(tr_batch* b, const trk::Params& p0, const trk::Params& p1, uint64_t& count) {
-    order(b, b->stream, b->stream1);
-    enqueue_batch(b, p0, b->stream, b->shadow_stream, count);
-    enqueue_batch(b, p1, b->stream1, b->shadow_stream1, count);
-    order(b, b->stream1, b->stream);
+// kLanes batches, one per lane: the other lanes fork from lane 0's stream and join it again, so
+// a capture of the group holds all of them as parallel branches.
+void enqueue_group(tr_batch* b, const trk::Params* p, uint64_t& count) {
+    for (int k = 0; k + 1 < tr_batch::kLanes; ++k) order(b, b->stream, b->lane_stream[k]);
+    enqueue_batch(b, p[0], b->stream, b->shadow_stream, count);
+    for (int k = 0; k + 1 < tr_batch::kLanes; ++k) enqueue_batch(b, p[k + 1], b->lane_stream[k], b->lane_shadow[k], count);
+    for (int k = 0; k + 1 < tr_batch::kLanes; ++k) order(b, b->lane_stream[k], b->stream);
 }
 
 tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_count) {
@@ -286,9 +292,9 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
     b->stats.train_steps = 0;
     b->stats.render_ms = 0.0;
     if (pl.batches.empty()) return TR_OK;
-    // batches run in pairs, one per lane; an odd count ends with an empty batch (no slots, no
-    // splat blocks: its kernels find no work)
-    if (pl.batches.size() % 2u) pl.batches.push_back(trk::BatchDesc{});
+    // batches run in groups of kLanes, one per lane; a count that is not a multiple ends with
+    // empty batches (no slots, no splat blocks: their kernels find no work)
+    while (pl.batches.size() % (size_t)tr_batch::kLanes) pl.batches.push_back(trk::BatchDesc{});
     ensure_batch_wave(b, b->cfg.capacity);
     const bool guided = b->guide != nullptr;
     if (guided) {
@@ -307,10 +313,12 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
     }
     TR_CUDA(cudaMemcpyAsync(b->d_batches, pl.batches.data(), pl.batches.size() * sizeof(trk::BatchDesc),
                             cudaMemcpyHostToDevice, s));
-    // lane 0 starts at batch 0, lane 1 at batch 1
-    TR_CUDA(cudaMemsetAsync(b->d_cur, 0, 2 * sizeof(uint32_t), s));
-    TR_CUDA(trk::launch_advance(b->d_cur + 1, 1u, s));
-    const trk::Params p0 = batch_params(b, pl, 0), p1 = batch_params(b, pl, 1);
+    // lane k starts at batch k
+    TR_CUDA(cudaMemsetAsync(b->d_cur, 0, tr_batch::kLanes * sizeof(uint32_t), s));
+    for (int k = 1; k < tr_batch::kLanes; ++k) TR_CUDA(trk::launch_advance(b->d_cur + k, (uint32_t)k, s));
+    trk::Params pv[tr_batch::kLanes];
+    for (int k = 0; k < tr_batch::kLanes; ++k) pv[k] = batch_params(b, pl, k);
+    const trk::Params& p0 = pv[0];
 
     tr_batch::Shape shape;
     shape.capacity = b->cfg.capacity;
@@ -323,21 +331,21 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
 
     uint64_t launches = 0;
     TR_CUDA(cudaEventRecord(b->ev0, s));
-    const size_t pairs = pl.batches.size() / 2;
+    const size_t groups = pl.batches.size() / (size_t)tr_batch::kLanes;    // groups of kLanes batches
     size_t done = 0;
     if (b->cfg.use_graph) {
         if (!(b->exec && shape == b->shape)) {
-            // new launch shape: the first pair runs directly (which also performs the kernels'
-            // one-time attribute calls outside any capture), then one pair is captured for the
-            // remaining pairs and later calls with the same shape
-            enqueue_pair(b, p0, p1, launches);
+            // new launch shape: the first group runs directly (which also performs the kernels'
+            // one-time attribute calls outside any capture), then one group is captured for the
+            // remaining groups and later calls with the same shape
+            enqueue_group(b, pv, launches);
             done = 1;
             b->drop_graph();
-            if (done < pairs) {
+            if (done < groups) {
                 uint64_t n_capt = 0;
                 TR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 try {
-                    enqueue_pair(b, p0, p1, n_capt);
+                    enqueue_group(b, pv, n_capt);
                 } catch (...) {
                     cudaGraph_t g = nullptr;
                     cudaStreamEndCapture(s, &g);
@@ -349,14 +357,15 @@ tr_status batch_render(tr_batch* b, const uint64_t* s_begin, const uint32_t* s_c
                 b->shape = shape;
             }
         }
-        // kernels per replay (two batches of enqueue_batch)
-        const uint64_t per = 2 * (3 + 3ull * b->max_bounces + (guided ? b->max_bounces + (b->pool ? 2 : 0) : 0));
-        for (; done < pairs; ++done) {
+        // kernels per replay (kLanes batches of enqueue_batch)
+        const uint64_t per = (uint64_t)tr_batch::kLanes *
+                             (3 + 3ull * b->max_bounces + (guided ? b->max_bounces + (b->pool ? 2 : 0) : 0));
+        for (; done < groups; ++done) {
             TR_CUDA(cudaGraphLaunch(b->exec, s));
             launches += per;
         }
     } else {
-        for (; done < pairs; ++done) enqueue_pair(b, p0, p1, launches);
+        for (; done < groups; ++done) enqueue_group(b, pv, launches);
     }
     TR_CUDA(cudaEventRecord(b->ev1, s));
     TR_CUDA(cudaEventSynchronize(b->ev1));
@@ -407,8 +416,10 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         TR_CUDA(cudaSetDevice(b->device));
         TR_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         TR_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream, cudaStreamNonBlocking));
-        TR_CUDA(cudaStreamCreateWithFlags(&b->stream1, cudaStreamNonBlocking));
-        TR_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream1, cudaStreamNonBlocking));
+        for (int k = 0; k + 1 < tr_batch::kLanes; ++k) {
+            TR_CUDA(cudaStreamCreateWithFlags(&b->lane_stream[k], cudaStreamNonBlocking));
+            TR_CUDA(cudaStreamCreateWithFlags(&b->lane_shadow[k], cudaStreamNonBlocking));
+        }
         for (cudaEvent_t& e : b->dep) TR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         TR_CUDA(cudaEventCreate(&b->ev0));
         TR_CUDA(cudaEventCreate(&b->ev1));
@@ -433,7 +444,7 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         // before the data lands, on a stream that does not order with this one)
         TR_CUDA(cudaMemcpyAsync(b->d_scenes, slots.data(), n * sizeof(trk::SceneSlot), cudaMemcpyHostToDevice, b->stream));
         TR_CUDA(cudaStreamSynchronize(b->stream));
-        b->d_cur = b->alloc<uint32_t>(2);
+        b->d_cur = b->alloc<uint32_t>(tr_batch::kLanes);
         b->trace_grid = trk::trace_grid_size(b->device, b->bvh_depth, true);
         b->stats.device_bytes = b->bytes;
     } catch (const CudaError& e) {
@@ -441,8 +452,10 @@ tr_status tr_batch_create(tr_ctx* const* contexts, uint32_t n, tr_batch** out) {
         for (cudaEvent_t e : b->dep)
             if (e) cudaEventDestroy(e);
         if (b->shadow_stream) cudaStreamDestroy(b->shadow_stream);
-        if (b->stream1) cudaStreamDestroy(b->stream1);
-        if (b->shadow_stream1) cudaStreamDestroy(b->shadow_stream1);
+        for (int k = 0; k + 1 < tr_batch::kLanes; ++k) {
+            if (b->lane_stream[k]) cudaStreamDestroy(b->lane_stream[k]);
+            if (b->lane_shadow[k]) cudaStreamDestroy(b->lane_shadow[k]);
+        }
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return fail(e.code == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA, e.what());
@@ -580,8 +593,10 @@ tr_status tr_batch_destroy(tr_batch* b) {
     for (cudaEvent_t e : b->dep)
         if (e) cudaEventDestroy(e);
     if (b->shadow_stream) cudaStreamDestroy(b->shadow_stream);
-    if (b->stream1) cudaStreamDestroy(b->stream1);
-    if (b->shadow_stream1) cudaStreamDestroy(b->shadow_stream1);
+    for (int k = 0; k + 1 < tr_batch::kLanes; ++k) {
+        if (b->lane_stream[k]) cudaStreamDestroy(b->lane_stream[k]);
+        if (b->lane_shadow[k]) cudaStreamDestroy(b->lane_shadow[k]);
+    }
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return TR_OK;
