@@ -65,8 +65,9 @@ __global__ void __launch_bounds__(128, 4) k_mlp_fwd(GuideDev g, const uint4* __r
                 for (int c = 0; c < 8; ++c) {
                     float t[8];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) t[e] = fmaxf(acc[8 * c + e] + sB[l * 64 + 8 * c + e], 0.0f);
-                    h[c] = make_uint4(pack2(t[0], t[1]), pack2(t[2], t[3]), pack2(t[4], t[5]), pack2(t[6], t[7]));
+                    for (int e = 0; e < 8; ++e) t[e] = acc[8 * c + e] + sB[l * 64 + 8 * c + e];
+                    h[c] = make_uint4(pack2_relu(t[0], t[1]), pack2_relu(t[2], t[3]), pack2_relu(t[4], t[5]),
+                                      pack2_relu(t[6], t[7]));
                 }
                 store_row_a(sA, tid, h);
                 if (act && row < m) {

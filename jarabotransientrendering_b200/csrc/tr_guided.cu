@@ -212,9 +212,9 @@ __global__ void __launch_bounds__(128, 3) k_guide(const __grid_constant__ Params
         for (int q = 0; q < 8; ++q) {
             float t[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) t[e] = fmaxf(a[8 * q + e] + sB[l * 64 + 8 * q + e], 0.0f);
-            h[q] = make_uint4(trg::pack2(t[0], t[1]), trg::pack2(t[2], t[3]), trg::pack2(t[4], t[5]),
-                              trg::pack2(t[6], t[7]));
+            for (int e = 0; e < 8; ++e) t[e] = a[8 * q + e] + sB[l * 64 + 8 * q + e];
+            h[q] = make_uint4(trg::pack2_relu(t[0], t[1]), trg::pack2_relu(t[2], t[3]), trg::pack2_relu(t[4], t[5]),
+                              trg::pack2_relu(t[6], t[7]));
         }
         trg::store_row_a(sA, tid, h);
     };

@@ -456,11 +456,11 @@ __global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) 
     uint32_t* qout = p.wave.q[(depth + 1) & 1];
     const unsigned lane = threadIdx.x & 31u;
     // block-uniform iterations (the next-ray queue is filled per block, below)
-    __shared__ uint32_t oc[8], ob[8];
+    __shared__ uint32_t oc[8], ob[8], sc8[8], sb8[8];
     for (uint32_t bbase = blockIdx.x * blockDim.x; bbase < n; bbase += gridDim.x * blockDim.x) {
         const uint32_t base = bbase + (threadIdx.x & ~31u);
         const uint32_t idx = base + lane;
-        uint32_t oct = 0;
+        uint32_t oct = 0, soct = 0;
         bool want_shadow = false, want_next = false, want_guide = false;
         uint4 gv[5];                     // guided-vertex record (kGuided only)
         uint32_t slot = 0;
@@ -630,6 +630,7 @@ __global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) 
                             // TransientRenderer.h:165-169); otherwise only useful ones are traced
                             if ((inside && fin && (Lr != 0.0f || Lg != 0.0f || Lb != 0.0f)) || film.nbounce) {
                                 want_shadow = true;
+                                soct = (ld.x < 0.0f ? 1u : 0u) | (ld.y < 0.0f ? 2u : 0u) | (ld.z < 0.0f ? 4u : 0u);
                                 const uint32_t bin = inside ? (uint32_t)floorf(ps) : kBinOutside;
                                 sh_o = make_float4(lp.x, lp.y, lp.z, dl - kSigmaVis);
                                 sh_d = make_float4(ld.x, ld.y, ld.z, __uint_as_float(bin | ((uint32_t)depth << 24)));
@@ -777,32 +778,30 @@ __global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) 
             }
         }
         // ---- shadow queue: warp-aggregated appends (order preserved within the warp) ----
-        const unsigned ms = __ballot_sync(kFull, want_shadow);
-        uint32_t bs = 0;
-        if (lane == 0 && ms) bs = atomicAdd(&p.wave.counters[cnt_sh(depth)], (uint32_t)__popc(ms));
-        bs = __shfl_sync(kFull, bs, 0);
         const unsigned lt = lanemask_lt();
+        // ---- shadow and next-ray queues: the block's rays grouped by direction octant (one
+        // atomic per queue and block), so a warp of k_shadow / k_extend takes rays heading the
+        // same way; the shadow rays of a light also share their origin ----
+        if (threadIdx.x < 8) { oc[threadIdx.x] = 0; sc8[threadIdx.x] = 0; }
+        __syncthreads();
+        uint32_t rk = 0, rs = 0;
+        if (want_next) rk = atomicAdd(&oc[oct], 1u);
+        if (want_shadow) rs = atomicAdd(&sc8[soct], 1u);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t tot = 0, tsh = 0;
+            for (int o = 0; o < 8; ++o) { ob[o] = tot; tot += oc[o]; sb8[o] = tsh; tsh += sc8[o]; }
+            const uint32_t g0 = tot ? atomicAdd(&p.wave.counters[cnt_ext(depth + 1)], tot) : 0u;
+            const uint32_t s0 = tsh ? atomicAdd(&p.wave.counters[cnt_sh(depth)], tsh) : 0u;
+            for (int o = 0; o < 8; ++o) { ob[o] += g0; sb8[o] += s0; }
+        }
+        __syncthreads();
         if (want_shadow) {
-            const uint32_t k = bs + (uint32_t)__popc(ms & lt);
+            const uint32_t k = sb8[soct] + rs;
             p.wave.sh_o[k] = sh_o;
             p.wave.sh_d[k] = sh_d;
             p.wave.sh_L[k] = sh_L;
         }
-        // ---- next-ray queue: the block's rays grouped by direction octant (one atomic per
-        // block), so a warp of k_extend takes rays heading the same way (2.4 % less frame time
-        // on the icosphere workload) ----
-        if (threadIdx.x < 8) oc[threadIdx.x] = 0;
-        __syncthreads();
-        uint32_t rk = 0;
-        if (want_next) rk = atomicAdd(&oc[oct], 1u);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t tot = 0;
-            for (int o = 0; o < 8; ++o) { ob[o] = tot; tot += oc[o]; }
-            const uint32_t g0 = tot ? atomicAdd(&p.wave.counters[cnt_ext(depth + 1)], tot) : 0u;
-            for (int o = 0; o < 8; ++o) ob[o] += g0;
-        }
-        __syncthreads();
         if (want_next) qout[ob[oct] + rk] = slot;
         if (kGuided) {
             const unsigned mg = __ballot_sync(kFull, want_guide);

@@ -98,6 +98,13 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<uint32_t*>(&h);
 }
+// bf16x2 {relu(a) low, relu(b) high} rounded to nearest in one conversion (cvt.rn.relu.bf16x2.f32):
+// the same bits as pack2(fmaxf(a, 0), fmaxf(b, 0)) for every non-NaN input
+__device__ __forceinline__ uint32_t pack2_relu(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
 __device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
 
