@@ -280,9 +280,9 @@ def convergence(args, device):
     guided workload (GGX floor, 0.05 x 0.05 area light hidden behind an occluder slab, 512 x 512,
     2048 bins).  Reference: the plain tracer, two independent halves of ``convergence_ref_spp``
     samples per pixel (its own noise is subtracted from the error).  Both samplers render passes of
-    64 samples per pixel from a fresh context and network; the guided run trains online (batches
-    of 65,536 samples, Adam lr 3e-3, mixture probability 0.7) and drops its first 1,024 samples
-    per pixel after training on them.  Time = host wall clock of the render calls (training
+    64 samples per pixel from a fresh context and network; the guided run trains online (a pool of
+    131,072 samples per pass in batches of 65,536, Adam lr 5e-3, mixture probability 0.7) and
+    drops its first 1,024 samples per pixel after training on them.  Time = host wall clock of the render calls (training
     included); the error evaluation between passes is not timed."""
     import torch
     from jarabotransientrendering_b200 import convergence as CV, renderer as R, scenes as S
@@ -295,7 +295,7 @@ def convergence(args, device):
     g = R.Guide(device=device, seed=1)
     try:
         guided = CV.time_to_error(sc, ref, target=0.05, pass_spp=64, max_spp=262144, guide=g, mix_prob=0.7,
-                                  learning_rate=3e-3, train_pool=262144, device=device, warmup_spp=1024)
+                                  learning_rate=5e-3, train_pool=131072, device=device, warmup_spp=1024)
     finally:
         g.close()
     ref_noise = ref.rel_noise
@@ -312,7 +312,7 @@ def convergence(args, device):
            "reference": {"tracer": "plain", "spp": 2 * args.convergence_ref_spp, "rel_noise": ref_noise,
                          "seconds": ref_s},
            "plain": leg(plain),
-           "guided": dict(leg(guided), mix_prob=0.7, learning_rate=3e-3, train_batch=65536),
+           "guided": dict(leg(guided), mix_prob=0.7, learning_rate=5e-3, train_pool=131072, train_batch=65536),
            "passes_spp": 64}
     if plain["seconds"] and guided["seconds"]:
         res["speedup_guided_vs_plain"] = plain["seconds"] / guided["seconds"]
@@ -387,7 +387,9 @@ def batched(args, device, frames=2):
     try:
         B = R.Batch(ctxs)
         B.set_guide(g, mix_prob=0.7, learning_rate=3e-3, train_pool=262144)
-        trial = [max(1, k // 16) for k in spp]
+        # trials of half a frame: a trial much smaller than the frame favours small queues (its
+        # few batches overlap better across the lanes than a full frame's many)
+        trial = [max(1, k // 2) for k in spp]
         best, trials = B.autotune(0, trial)
         res["autotune"] = {"best": best, "trials": trials, "trial_spp": trial}
         nxt = [trials * t for t in trial]
