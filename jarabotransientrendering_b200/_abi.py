@@ -108,7 +108,7 @@ PROTOTYPES = {
     "tr_guide_destroy": (C.c_int, [C.c_void_p]),
     "tr_guide_set_wait_limit": (C.c_int, [C.c_void_p, C.c_uint32]),
     "tr_set_guide": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_uint32]),
-    "tr_set_guide_depth": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "tr_set_guide_scope": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float]),
     "tr_stats_get": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "tr_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)]),
     "tr_batch_set_config": (C.c_int, [C.c_void_p, C.POINTER(BatchConfig)]),

@@ -367,6 +367,7 @@ trk::Params make_params(tr_ctx* x) {
             p.guide.net.bias = x->bias_snap;
         }
         p.guide.err = guide_err(x->guide);
+        p.guide.min_alpha = x->guide_min_alpha;
     }
     return p;
 }
@@ -1569,9 +1570,11 @@ extern "C" tr_status tr_set_guide(tr_ctx* x, tr_guide* g, float mix_prob, float 
     return TR_OK;
 }
 
-extern "C" tr_status tr_set_guide_depth(tr_ctx* x, uint32_t depths) {
+extern "C" tr_status tr_set_guide_scope(tr_ctx* x, uint32_t depths, float min_roughness) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
+    if (!(min_roughness >= 0.0f)) return fail(TR_ERR_INVALID_ARGUMENT, "min_roughness must be >= 0");
     x->guide_depth = depths;
+    x->guide_min_alpha = min_roughness;
     return TR_OK;
 }
 

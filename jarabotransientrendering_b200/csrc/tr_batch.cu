@@ -238,6 +238,7 @@ trk::Params batch_params(const tr_batch* b, const Plan& pl, int lane) {
         p.guide.err = guide_err(b->guide);
         if (lane) p.guide.vrec = b->lane_vrec[lane - 1];
         p.guide.tag = 1u;       // the lanes fill the pool at once: entries tagged by batch index
+        p.guide.min_alpha = kGuideMinAlpha;
     }
     return p;
 }

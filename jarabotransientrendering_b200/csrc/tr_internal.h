@@ -58,6 +58,8 @@ constexpr uint32_t kDefaultCapacity = 1u << 21; // path slots per wavefront batc
 #define TR_WAVE_LANES 4
 #endif
 constexpr int kWaveLanes = TR_WAVE_LANES;        // wave buffer sets batches alternate between
+// default roughness below which GGX vertices sample their BSDF instead of the learned proposal
+constexpr float kGuideMinAlpha = 0.5f;
 
 }  // namespace tri
 
@@ -189,6 +191,7 @@ struct tr_ctx {
     float* bias_snap = nullptr;           // and its biases [4][64]
     cudaEvent_t ev_snap = nullptr, ev_train = nullptr;
     uint32_t guide_depth = 0xffffffffu;   // path depths whose surface vertices use the proposal
+    float guide_min_alpha = tri::kGuideMinAlpha;   // GGX vertices smoother than this sample their BSDF
     float last_train_loss = 0.0f;
     uint32_t train_steps = 0;
     cudaStream_t user_stream = nullptr;   // caller's stream (tr_set_stream) or null

@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) 
                         const bool tsm = kTimeSampling && (flags & kFlagTimeSampling) != 0;
                         const bool survive = tsm || !(pcg_float(rng) > albedo);
                         const float prr = tsm ? 1.0f : albedo;
-                        if (kGuided && surface && survive) {
+                        if (kGuided && surface && survive && !(ggx && alpha < p.guide.min_alpha)) {
                             // ---- direction deferred to the learned proposal (k_guide) ----
                             want_guide = true;
                             gv[0] = make_uint4(__float_as_uint(pos.x), __float_as_uint(pos.y), __float_as_uint(pos.z),
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) 
                             gv[2] = make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z),
                                                __float_as_uint(__ldg(&sc.tri_ng[id]).w));
                             gv[3] = make_uint4(__float_as_uint(nrm.x), __float_as_uint(nrm.y), __float_as_uint(nrm.z), slot);
-                        } else if ((!kGuided || !surface) && survive) {
+                        } else if (survive) {
                             // ---- outgoing direction ----
                             f3 fa, nd;
                             float pa;

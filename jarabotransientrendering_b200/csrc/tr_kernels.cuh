@@ -82,6 +82,9 @@ struct GuideWave {
     // batch tag written into pool_meta[k].w (0: untagged; the batch's entries are then the
     // pool range filled since the previous gather)
     uint32_t tag;
+    // GGX vertices smoother than this roughness sample their BSDF in the shading kernel instead of
+    // the proposal (glossy lobes are already sampled close to the product by the BSDF sampler)
+    float min_alpha;
 };
 
 struct CameraDev {

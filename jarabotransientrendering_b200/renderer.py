@@ -173,10 +173,10 @@ class Context:
                                            learning_rate, train_pool))
         self._guide = guide
 
-    def set_guide_depth(self, depths):
-        """Only surface vertices at path depth < depths sample with the proposal
-        (tr_set_guide_depth); deeper ones sample their BSDF."""
-        _abi.check(_abi.lib().tr_set_guide_depth(self.h, depths))
+    def set_guide_scope(self, depths=0xFFFFFFFF, min_roughness=0.5):
+        """Surface vertices at path depth < depths on Lambertian or GGX (roughness >= min_roughness)
+        materials sample with the proposal (tr_set_guide_scope); the others sample their BSDF."""
+        _abi.check(_abi.lib().tr_set_guide_scope(self.h, depths, min_roughness))
 
     def stats(self):
         s = _abi.Stats()

@@ -30,7 +30,8 @@ from jarabotransientrendering_b200 import scenes as S  # noqa: E402
 from oracle import refscene, refstats  # noqa: E402
 
 # name -> (scene factory, scanline rows or None, reference runs)
-CONFIGS = {"cornell": (S.cornell, None, 512), "medium": (S.medium, (112, 144), 256)}
+CONFIGS = {"cornell": (S.cornell, None, 512), "medium": (S.medium, (112, 144), 256),
+           "icosphere": (S.icosphere, (252, 260), 1024)}
 
 
 def main(names=None):

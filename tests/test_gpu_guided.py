@@ -29,11 +29,13 @@ def test_orthonormal_frame_matches_oracle(gpu, oracle_lib):
         assert np.allclose(fg["streak"], fo["streak"], rtol=RTOL_TILE, atol=1e-12)
 
 
-def _films(gpu, sc, K, spp, guide=None, train_pool=0):
+def _films(gpu, sc, K, spp, guide=None, train_pool=0, min_roughness=None):
     out = []
     with gpu.Context(sc) as ctx:
         if guide is not None:
             ctx.set_guide(guide, mix_prob=0.5, learning_rate=1e-3, train_pool=train_pool)
+            if min_roughness is not None:
+                ctx.set_guide_scope(min_roughness=min_roughness)
         for k in range(K):
             ctx.clear()
             ctx.render(spp * k, spp)
@@ -69,14 +71,16 @@ def _compare(a, b, tile=8, window=8):
             "window_max_z": float(np.abs(zw).max()), "window_mean_z": float(zw.mean())}
 
 
-@pytest.mark.parametrize("train", [False, True])
-def test_guided_render_is_unbiased(gpu, train):
+@pytest.mark.parametrize("train,min_roughness", [(False, None), (True, None), (True, 0.0)])
+def test_guided_render_is_unbiased(gpu, train, min_roughness):
+    """Untrained and trained proposals; min_roughness 0 guides the GGX floor's vertices too (by
+    default only rougher GGX and Lambertian vertices are guided)."""
     sc = guided_scene()
     K = 40
     plain, _ = _films(gpu, sc, K, 64)
     g = gpu.Guide(seed=5)
     try:
-        guided, st = _films(gpu, sc, K, 64, guide=g, train_pool=32768 if train else 0)
+        guided, st = _films(gpu, sc, K, 64, guide=g, train_pool=32768 if train else 0, min_roughness=min_roughness)
     finally:
         g.close()
     r = _compare(guided, plain)
