@@ -48,8 +48,8 @@ __device__ __forceinline__ void order2(float& ka, int& ra, float& kb, int& rb) {
     }
 }
 
-// Traversal state of one ray between calls of trav_run: next node (or leaf ref), stack depth,
-// closest hit so far.
+// Traversal state of one ray between calls of trav_run: next node (or the triangles left in a
+// leaf), stack depth, closest hit so far.
 struct Trav {
     int node, sp;
     float best, bu, bv;
@@ -59,7 +59,7 @@ __device__ __forceinline__ void trav_init(Trav& st, float tfar) {
     st.node = 0; st.sp = 0; st.best = tfar; st.bu = 0.f; st.bv = 0.f; st.bid = kInvalid;
 }
 
-// Runs at most `budget` node or leaf visits of the ray's traversal; returns true once the
+// Runs at most `budget` node or triangle visits of the ray's traversal; returns true once the
 // traversal is complete (closest hit, or any hit with kAnyHit, in st).  The stack lives in
 // shared memory at stack[k * stride].
 template <bool kAnyHit>
@@ -115,10 +115,12 @@ __device__ __forceinline__ bool trav_run(const SceneDev& sc, const WRay& r, Trav
             }
             continue;
         }
+        // one triangle per visit: the leaf's remaining triangles stay in st.node, so a lane in
+        // a leaf and a lane at an inner node each advance by one step per loop iteration
         const uint32_t ref = (uint32_t)(~st.node);
         const uint32_t first = ref >> 3, cnt = ref & 7u;
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const float4* tp = sc.tris + 3 * (first + k);
+        {
+            const float4* tp = sc.tris + 3 * first;
             const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
             const uint32_t id = __float_as_uint(q0.w);
             float t, u, v;
@@ -128,6 +130,10 @@ __device__ __forceinline__ bool trav_run(const SceneDev& sc, const WRay& r, Trav
                     if (kAnyHit) return true;
                 }
             }
+        }
+        if (cnt > 1u) {
+            st.node = (int)~(((first + 1u) << 3) | (cnt - 1u));
+            continue;
         }
         if (st.sp == 0) return true;
         --st.sp;
@@ -238,7 +244,7 @@ __global__ void __launch_bounds__(256) k_raygen(const __grid_constant__ Params p
 // -----------------------------------------------------------------------------------------
 // extend / shadow: persistent warps fetch 32 queue entries at a time.
 // -----------------------------------------------------------------------------------------
-// Node and leaf visits a lane makes between two refills of the warp's finished lanes.
+// Node and triangle visits a lane makes between two refills of the warp's finished lanes.
 constexpr int kTravBudget = 8;
 
 // Warp-aggregated refill from a queue: every lane with busy == false takes the next entry
