@@ -804,6 +804,13 @@ tr_status tr_create(const tr_scene* s, const tr_camera* c, const tr_film* f, con
             delete x;
             return fail(TR_ERR_NOT_SUPPORTED, "BVH deeper than the traversal stack");
         }
+        if (reinterpret_cast<uintptr_t>(dnodes) & 31u) {
+            // the traversal fetches a node's bounds with 256-bit loads (32-byte aligned)
+            cudaStreamSynchronize(x->stream);
+            x->release();
+            delete x;
+            return fail(TR_ERR_CUDA, "BVH node buffer not 32-byte aligned");
+        }
         x->bvh_nodes = dbv.nodes;
         x->bvh_depth = dbv.stack - 1;               // sizes the shared-memory traversal stack
         x->bvh_levels = dbv.depth;

@@ -41,6 +41,14 @@ __device__ __forceinline__ void slab4(float lo_x, float hi_x, float lo_y, float 
     const bool use = ref >= 0 || ((~ref) & 7) != 0;
     key = (use && tmin <= tmax) ? tmin : __int_as_float(0x7f800000);
 }
+// 32 bytes in one load (sm_100: 256-bit global loads); p must be 32-byte aligned (the launchers
+// check the node buffer).  A node's bounds arrive in three such loads instead of six 128-bit
+// ones: the divergent lanes of a warp each cost their own L1 request per load instruction.
+__device__ __forceinline__ void ldg256(const float4* p, float4& a, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
 __device__ __forceinline__ void order2(float& ka, int& ra, float& kb, int& rb) {
     if (kb < ka) {
         const float tk = ka; ka = kb; kb = tk;
@@ -72,8 +80,10 @@ __device__ __forceinline__ bool trav_run(const SceneDev& sc, const WRay& r, Trav
         if (budget-- == 0) return false;
         if (st.node >= 0) {
             const float4* np = sc.nodes + 8 * st.node;
-            const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-            const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+            float4 lx, hx, ly, hy, lz, hz;
+            ldg256(np, lx, hx);
+            ldg256(np + 2, ly, hy);
+            ldg256(np + 4, lz, hz);
             const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
             float k0, k1, k2, k3;
             int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
@@ -1396,6 +1406,7 @@ cudaError_t launch_raygen(const Params& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_extend(const Params& p, int depth, int grid, cudaStream_t s) {
+    if (reinterpret_cast<uintptr_t>(p.scene.nodes) & 31u) return cudaErrorMisalignedAddress;
     if (p.multi.scenes) k_extend<true><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     else k_extend<false><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
@@ -1432,6 +1443,7 @@ cudaError_t launch_shade(const Params& p, int depth, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_shadow(const Params& p, int depth, int grid, cudaStream_t s) {
+    if (reinterpret_cast<uintptr_t>(p.scene.nodes) & 31u) return cudaErrorMisalignedAddress;
     if (p.multi.scenes) k_shadow<true><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     else k_shadow<false><<<grid, kTraceBlock, trace_smem_bytes(p.bvh_depth), s>>>(p, depth);
     return cudaGetLastError();
@@ -1525,6 +1537,7 @@ cudaError_t launch_advance(uint32_t* cur, uint32_t step, cudaStream_t s) {
 }
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit, void* out,
                               uint32_t* cursor, int grid, cudaStream_t s) {
+    if (reinterpret_cast<uintptr_t>(sc.nodes) & 31u) return cudaErrorMisalignedAddress;
     k_trace_user<<<grid, kTraceBlock, trace_smem_bytes(sc.bvh_depth), s>>>(sc, rays, n, any_hit,
                                                                           reinterpret_cast<HitOut*>(out), cursor);
     return cudaGetLastError();
