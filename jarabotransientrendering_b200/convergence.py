@@ -86,14 +86,16 @@ class Reference:
 def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp: int = 4,
                   max_spp: int = 4096, guide: Optional[R.Guide] = None, mix_prob: float = 0.5,
                   learning_rate: float = 1e-3, train_pool: int = 262144, device: int = 0,
-                  sample_offset: int = 1 << 20, warmup_spp: int = 0):
+                  sample_offset: int = 1 << 20, warmup_spp: int = 0, train_spp: Optional[int] = None):
     """Renders ``scene`` progressively, ``pass_spp`` samples per pixel per pass, until the film's
     rel-L2 against ``ref`` is at most ``target`` (or ``max_spp`` is reached). Sample indices start
     at ``sample_offset``, so the passes are independent of the reference's samples.
 
     With a learned proposal, the first ``warmup_spp`` samples per pixel train the network and are
     then dropped from the film (the film is cleared once), as in the iterative schemes of path
-    guiding; their render and training time counts like every other pass.
+    guiding; their render and training time counts like every other pass.  ``train_spp`` (when
+    given) is the training budget: once the film holds that many samples per pixel the network is
+    frozen and the remaining passes render with it without training.
 
     Returns {"seconds": render wall time to the target (None if not reached), "spp": samples per
     pixel in the film then, "warmup_spp", "paths_per_s", "curve": [(spp in film, seconds, rel_l2),
@@ -121,7 +123,11 @@ def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp
         if warmup_spp:
             ctx.clear()
         spp = 0
+        frozen = guide is None or train_spp is None
         while spp < max_spp:
+            if not frozen and spp >= train_spp:
+                ctx.set_guide(guide, mix_prob=mix_prob, learning_rate=learning_rate, train_pool=0)
+                frozen = True
             n = min(pass_spp, max_spp - spp)
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
@@ -140,5 +146,5 @@ def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp
         train_loss = ctx.stats()["train_loss"]
     paths = rendered * scene.width * scene.height * scene.incoming_samples
     return {"seconds": reached[0] if reached else None, "spp": reached[1] if reached else None,
-            "warmup_spp": warmup_spp, "paths_per_s": paths / spent if spent > 0 else 0.0, "curve": curve,
+            "warmup_spp": warmup_spp, "train_spp": train_spp, "paths_per_s": paths / spent if spent > 0 else 0.0, "curve": curve,
             "train_steps": train_steps, "train_loss": train_loss}
