@@ -635,7 +635,8 @@ def main():
 
     if not args.no_e2e:
         # end to end through the C ABI with host buffers: scene upload + BVH build (tr_create),
-        # render, film read-back into pinned host memory (tr_get_film), tr_destroy
+        # render with the film streamed into pinned host memory as rows complete (tr_render_film:
+        # RGBE images as the reference writes them; FP32 and FP64 sums beside), tr_destroy
         ctx.close()
         del flush
         torch.cuda.empty_cache()
@@ -649,6 +650,10 @@ def main():
             return (torch.empty((H, W, Tb, 3), dtype=dt, pin_memory=True).numpy(),
                     torch.empty((H, W, 3), dtype=dt, pin_memory=True).numpy(),
                     torch.empty((H, W), dtype=dt, pin_memory=True).numpy())
+
+        def host_rgbe():
+            return (torch.empty((H, W, Tb, 4), dtype=torch.uint8, pin_memory=True).numpy(),
+                    torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True).numpy())
 
         def e2e_run(arrays, steps):
             """tr_create + tr_render_film (film rows streamed into the pinned arrays while the
@@ -669,24 +674,33 @@ def main():
             return sum(times[1:]) / steps, phases[1:]
 
         e2e_steps = max(1, min(args.steps, 3))
+        rg = host_rgbe()
+        et, ph = e2e_run(rg, e2e_steps)
+        d2h = sum(a.nbytes for a in rg)
+        del rg
         f32 = host_film(torch.float32)
-        et, ph = e2e_run(f32, e2e_steps)
-        d2h = sum(a.nbytes for a in f32)
+        et32, ph32 = e2e_run(f32, 1)
+        d2h32 = sum(a.nbytes for a in f32)
         del f32
         f64 = host_film(torch.float64)
         et64, ph64 = e2e_run(f64, 1)
         d2h64 = sum(a.nbytes for a in f64)
         del f64
         et = max_over_ranks(et, dist, "cuda")
+        et32 = max_over_ranks(et32, dist, "cuda")
         et64 = max_over_ranks(et64, dist, "cuda")
         out["e2e"] = {"value": whole_job_rate(paths_per_step, world, et), "unit": "paths/s",
                       "h2d_bytes_per_step": int(pv.nbytes + pt.nbytes + pm.nbytes),
                       "d2h_bytes_per_step": int(d2h),
                       "ms_per_step": et * 1e3,
-                      "film": "FP32 sums (the reference's film precision)",
+                      "film": "the reference's output images: every averaged film cell RGBE-encoded on the device "
+                              "as its .hdr writer encodes it (the pixel data of the 512 per-scanline streak files "
+                              "and of the steady image, byte for byte)",
                       "phases_per_step": ph,
+                      "fp32_film": {"value": whole_job_rate(paths_per_step, world, et32), "d2h_bytes_per_step": int(d2h32),
+                                    "ms_per_step": et32 * 1e3, "film": "FP32 sums and weights", "phases": ph32},
                       "fp64_film": {"value": whole_job_rate(paths_per_step, world, et64), "d2h_bytes_per_step": int(d2h64),
-                                    "ms_per_step": et64 * 1e3, "phases": ph64},
+                                    "ms_per_step": et64 * 1e3, "film": "FP64 sums and weights", "phases": ph64},
                       "includes": "tr_create (scene H2D from pinned memory + device BVH build + film alloc), "
                                   "tr_render_film (render with the film streamed into pinned host memory as "
                                   "pixel rows complete), tr_destroy"}

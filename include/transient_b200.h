@@ -256,8 +256,15 @@ tr_status tr_get_film(tr_ctx* ctx, double* streak, double* steady, double* weigh
  * reference's film itself accumulates in float), half the bytes.  streak/steady/weight point
  * to arrays of that type (any may be NULL).  The copies overlap the rendering only when the
  * host arrays are page-locked (cudaHostAlloc / cudaHostRegister); with pageable memory the call
- * is still correct but serialises them.  Returns when the film is in host memory.            */
-enum { TR_FILM_F64 = 0, TR_FILM_F32 = 1 };
+ * is still correct but serialises them.  Returns when the film is in host memory.
+ * type TR_FILM_RGBE delivers what tr_write_film writes instead of sums: each film cell averaged
+ * (sum / weight, in double, rounded to float, NaN -> 0) and RGBE-encoded on the device exactly
+ * as the .hdr writer encodes it (ImageIO.h:146-193), 4 bytes per cell.  streak is
+ * [height][width][time_bins][4] bytes -- for each scanline y, the pixel data of its streak
+ * file "<name>_%04d.hdr" when time_bins >= 8 (that file stores rows x, columns t; with fewer
+ * bins the file holds the transpose) -- and steady is [height][width][4], the pixel data of
+ * "<name>.hdr"; weight must be NULL.  A third of the FP32 bytes (a twelfth of FP64).          */
+enum { TR_FILM_F64 = 0, TR_FILM_F32 = 1, TR_FILM_RGBE = 2 };
 tr_status tr_render_film(tr_ctx* ctx, uint64_t sample_begin, uint32_t sample_count, int type, void* streak,
                          void* steady, void* weight);
 

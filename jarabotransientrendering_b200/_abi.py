@@ -67,7 +67,7 @@ class Stats(C.Structure):
                 ("trace_ms", C.c_double)]
 
 
-FILM_F64, FILM_F32 = 0, 1     # tr_render_film delivery types
+FILM_F64, FILM_F32, FILM_RGBE = 0, 1, 2     # tr_render_film delivery types
 
 
 class BatchConfig(C.Structure):

@@ -461,6 +461,7 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     // device first, into a staging buffer the copy stream reuses in order)
     const uint32_t T = x->film.time_bins;
     const bool f32 = sink && sink->type == TR_FILM_F32;
+    const bool rgbe = sink && sink->type == TR_FILM_RGBE;
     if (sink) {
         if (!x->copy_stream) {
             // highest priority: its FP32 conversions get SMs as soon as a traversal launch's
@@ -469,10 +470,12 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             TR_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
             TR_CUDA(cudaStreamCreateWithPriority(&x->copy_stream, cudaStreamNonBlocking, hi));
         }
-        const uint32_t per_pix_max = std::min<uint32_t>(ns_total, std::max<uint32_t>(1u, cap / ninc)) * ninc;
-        const size_t ppb_max = std::max<uint32_t>(1u, cap / per_pix_max);
-        const size_t stage = ppb_max * ((size_t)T * 3u + 4u);
-        if (f32 && x->stage_floats < stage) {
+        // only the last sample chunk's batches deliver rows; a shorter last chunk packs more
+        // pixels into a batch, so the staging buffer is sized by that chunk
+        const uint32_t ns_last = ns_total - ((ns_total - 1u) / ns_chunk) * ns_chunk;
+        const size_t ppb_last = std::min<uint64_t>(win_pix, std::max<uint32_t>(1u, cap / (ns_last * ninc)));
+        const size_t stage = ppb_last * ((size_t)T * 3u + 4u);
+        if ((f32 || rgbe) && x->stage_floats < stage) {
             x->d_stage = x->alloc<float>(stage);
             x->stage_floats = stage;
         }
@@ -604,7 +607,21 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 const size_t p0 = pb, np = npix;
                 const size_t es = f32 ? sizeof(float) : sizeof(double);
                 const size_t n_st = np * T * 3u, n_sd = np * 3u;
-                if (f32) {
+                if (rgbe) {
+                    // RGBE cells (4 bytes each) in the staging buffer, which holds 3 T + 4 floats per pixel
+                    uchar4* st = reinterpret_cast<uchar4*>(x->d_stage);
+                    uchar4* sd = st + np * T;
+                    TR_CUDA(trk::launch_to_rgbe(x->d_streak + p0 * T * 3u, x->d_steady + p0 * 3u, x->d_weight + p0,
+                                                (uint32_t)np, T, sink->streak ? st : nullptr,
+                                                sink->steady ? sd : nullptr, x->copy_stream));
+                    launches += 1;
+                    if (sink->streak)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->streak) + p0 * T * 4u, st, np * T * 4u,
+                                                cudaMemcpyDeviceToHost, x->copy_stream));
+                    if (sink->steady)
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->steady) + p0 * 4u, sd, np * 4u,
+                                                cudaMemcpyDeviceToHost, x->copy_stream));
+                } else if (f32) {
                     float* st = x->d_stage;
                     float* sd = st + n_st;
                     float* wt = sd + n_sd;
@@ -934,11 +951,13 @@ static tr_status copy_film(tr_ctx* x, double* streak, double* steady, double* we
 tr_status tr_render_film(tr_ctx* x, uint64_t sample_begin, uint32_t sample_count, int type, void* streak,
                          void* steady, void* weight) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
-    if (type != TR_FILM_F64 && type != TR_FILM_F32) return fail(TR_ERR_INVALID_ARGUMENT, "unknown film type");
+    if (type != TR_FILM_F64 && type != TR_FILM_F32 && type != TR_FILM_RGBE)
+        return fail(TR_ERR_INVALID_ARGUMENT, "unknown film type");
+    if (type == TR_FILM_RGBE && weight) return fail(TR_ERR_INVALID_ARGUMENT, "RGBE delivery has no weight array");
     if (sample_count == 0) {
         // nothing to render: deliver the current sums
         if (type == TR_FILM_F64) return copy_film(x, (double*)streak, (double*)steady, (double*)weight, cudaMemcpyDeviceToHost);
-        return fail(TR_ERR_INVALID_ARGUMENT, "sample_count must be >= 1 for FP32 delivery");
+        return fail(TR_ERR_INVALID_ARGUMENT, "sample_count must be >= 1 for FP32 and RGBE delivery");
     }
     try {
         TR_CUDA(cudaSetDevice(x->device));

@@ -1529,6 +1529,55 @@ cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t 
     return cudaGetLastError();
 }
 
+// Averaged film cells in the reference's .hdr encoding (the host writer's rgbe_encode of
+// avg_nan0(sum, weight), tr_film_io.cpp; ImageIO.h:146-193): the average in double rounded to
+// float (NaN -> 0), then the largest channel v = m 2^e (frexp, m in [0.5, 1)), scale m 256 / v,
+// each channel truncated to [0, 255], exponent e + 128; 0 for v < 1e-32.
+__device__ __forceinline__ float film_avg(double v, double w) {
+    const double t = v / w;
+    return isnan(t) ? 0.0f : (float)t;
+}
+__device__ __forceinline__ unsigned char rgbe_q(float c, float scale) {
+    const float s = c * scale;
+    return (unsigned char)(s > 0.f ? (s < 255.f ? s : 255.f) : 0.f);
+}
+__device__ __forceinline__ uchar4 rgbe_cell(const double* __restrict__ c, double w) {
+    const float r = film_avg(__ldcs(c), w), g = film_avg(__ldcs(c + 1), w), b = film_avg(__ldcs(c + 2), w);
+    float v = r > g ? r : g;
+    v = v > b ? v : b;
+    if (!(v >= 1e-32f)) return make_uchar4(0, 0, 0, 0);
+    int e = 0;
+    const float m = frexpf(v, &e);
+    const float scale = m * 256.0f / v;
+    return make_uchar4(rgbe_q(r, scale), rgbe_q(g, scale), rgbe_q(b, scale), (unsigned char)(e + 128));
+}
+// one thread per cell: the npix x T streak cells, then the npix steady cells; 24 B read, 4 B
+// written per cell (HBM-bound)
+__global__ void __launch_bounds__(256) k_to_rgbe(const double* __restrict__ streak, const double* __restrict__ steady,
+                                                 const double* __restrict__ weight, uint32_t npix, uint32_t T,
+                                                 uchar4* __restrict__ os, uchar4* __restrict__ od) {
+    const size_t ns = (size_t)npix * T, n = ns + npix;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (i < ns) {
+            if (os) os[i] = rgbe_cell(streak + i * 3, weight[i / T]);
+        } else if (od) {
+            const size_t px = i - ns;
+            od[px] = rgbe_cell(steady + px * 3, weight[px]);
+        }
+    }
+}
+cudaError_t launch_to_rgbe(const double* streak, const double* steady, const double* weight, uint32_t npix,
+                           uint32_t T, uchar4* out_streak, uchar4* out_steady, cudaStream_t s) {
+    if (npix == 0 || T == 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t need = ((size_t)npix * (T + 1u) + 255) / 256;
+    const int grid = (int)std::min<size_t>(need, (size_t)sms * 8);
+    k_to_rgbe<<<std::max(1, grid), 256, 0, s>>>(streak, steady, weight, npix, T, out_streak, out_steady);
+    return cudaGetLastError();
+}
+
 // last node of a multi-scene batch: the next replay renders the next batch descriptor
 __global__ void k_advance(uint32_t* cur, uint32_t step) { *cur += step; }
 cudaError_t launch_advance(uint32_t* cur, uint32_t step, cudaStream_t s) {

@@ -249,6 +249,10 @@ cudaError_t launch_build_tris(const float* vertices, const uint32_t* triangles, 
                               const uint32_t* order, uint32_t nt, float4* tris, float4* tri_ng, cudaStream_t s);
 // FP64 film sums -> FP32 (film streaming)
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
+// film cells averaged by their pixel's weight and RGBE-encoded as the .hdr writer does:
+// streak [npix][T] and steady [npix] RGBE quadruples from npix pixels' FP64 sums
+cudaError_t launch_to_rgbe(const double* streak, const double* steady, const double* weight, uint32_t npix,
+                           uint32_t T, uchar4* out_streak, uchar4* out_steady, cudaStream_t s);
 cudaError_t launch_advance(uint32_t* cur, uint32_t step, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);

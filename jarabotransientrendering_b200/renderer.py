@@ -134,19 +134,25 @@ class Context:
                                           weight.ctypes.data if weight is not None else None))
 
     def render_film(self, sample_begin, sample_count, streak=None, steady=None, weight=None):
-        """tr_render_film: render and stream the film's sums into caller-provided host arrays
-        (float64 or float32, all of one type; pinned arrays let the copies overlap the
-        rendering).  Returns nothing; the arrays hold the film when it returns."""
+        """tr_render_film: render and stream the film into caller-provided host arrays (pinned
+        arrays let the copies overlap the rendering).  float64 or float32 arrays receive the
+        sums (streak [H][W][T][3], steady [H][W][3], weight [H][W]); uint8 arrays receive the
+        averaged cells RGBE-encoded as the .hdr files hold them (streak [H][W][T][4], steady
+        [H][W][4], no weight).  Returns nothing; the arrays hold the film when it returns."""
         arrs = [a for a in (streak, steady, weight) if a is not None]
         dt = arrs[0].dtype if arrs else np.dtype(np.float64)
-        if any(a.dtype != dt for a in arrs) or dt not in (np.float64, np.float32):
-            raise ValueError("film arrays must all be float64 or all float32")
+        if any(a.dtype != dt for a in arrs) or dt not in (np.float64, np.float32, np.uint8):
+            raise ValueError("film arrays must all be float64, all float32 or all uint8")
         sc = self.scene
         H, W, T = sc.height, sc.width, sc.time_bins
-        for a, shape in ((streak, (H, W, T, 3)), (steady, (H, W, 3)), (weight, (H, W))):
+        ch = 4 if dt == np.uint8 else 3
+        if dt == np.uint8 and weight is not None:
+            raise ValueError("RGBE delivery has no weight array")
+        for a, shape in ((streak, (H, W, T, ch)), (steady, (H, W, ch)), (weight, (H, W))):
             if a is not None and (a.shape != shape or not a.flags["C_CONTIGUOUS"]):
                 raise ValueError(f"film array must be C-contiguous with shape {shape}")
-        kind = _abi.FILM_F32 if dt == np.float32 else _abi.FILM_F64
+        kind = {np.dtype(np.float32): _abi.FILM_F32, np.dtype(np.uint8): _abi.FILM_RGBE}.get(np.dtype(dt),
+                                                                                           _abi.FILM_F64)
         _abi.check(_abi.lib().tr_render_film(self.h, int(sample_begin), int(sample_count), kind,
                                              streak.ctypes.data if streak is not None else None,
                                              steady.ctypes.data if steady is not None else None,

@@ -144,3 +144,83 @@ def test_device_bvh_build_matches_the_host_builder(gpu, tmp_path, workload):
     with gpu.Context(small) as c:
         st = c.stats()
     assert st["bvh_nodes"] == host["nodes"] and st["bvh_depth"] == host["depth"], (st, host)
+
+
+def _rgbe_np(sums, weight):
+    """The .hdr writer's encoding restated in numpy: average in double rounded to float (NaN ->
+    0), v = max channel = m 2^e, channels * (m 256 / v) truncated to [0, 255], e + 128."""
+    with np.errstate(invalid="ignore", divide="ignore"):
+        avg = (sums / weight[..., None]).astype(np.float32)
+    avg[np.isnan(avg)] = 0.0
+    v = avg.max(axis=-1)
+    m, e = np.frexp(v)
+    ok = v >= np.float32(1e-32)
+    with np.errstate(invalid="ignore", divide="ignore", over="ignore"):
+        scale = (m * np.float32(256.0)).astype(np.float32) / v
+        s = avg * scale[..., None]
+    q = np.where(s > 0, np.where(s < 255, s, 255), 0).astype(np.uint8)
+    out = np.zeros(avg.shape[:-1] + (4,), np.uint8)
+    out[..., :3] = np.where(ok[..., None], q, 0)
+    out[..., 3] = np.where(ok, e + 128, 0).astype(np.uint8)
+    return out
+
+
+def _hdr_pixels(path):
+    data = open(path, "rb").read()
+    head, _, rest = data.partition(b"\n\n")
+    dims, _, pix = rest.partition(b"\n")
+    _, h, _, w = dims.split()
+    return int(h), int(w), np.frombuffer(pix, np.uint8).reshape(int(h), int(w), 4)
+
+
+@pytest.mark.parametrize("time_bins", [64, 4])
+def test_render_film_rgbe_is_the_written_files_pixel_data(gpu, tmp_path, time_bins):
+    """RGBE delivery: the averaged film encoded on the device equals, byte for byte, the pixel
+    data tr_write_film writes (per-scanline streak files, steady image) and the encoding
+    restated in numpy from the FP64 sums."""
+    sc = S.cornell(width=40, height=24, time_bins=time_bins, exposure=5.12 / time_bins, sqrt_spp=4, max_bounces=4)
+    H, W, T = sc.height, sc.width, sc.time_bins
+    st = np.full((H, W, T, 4), 7, np.uint8)
+    sd = np.full((H, W, 4), 7, np.uint8)
+    name = str(tmp_path / "film")
+    with gpu.Context(sc) as c:
+        c.render_film(0, 16, st, sd)
+        f = c.film()
+        c.write(name)
+    assert (st == _rgbe_np(f["streak"], f["weight"][..., None])).all()
+    assert (sd == _rgbe_np(f["steady"], f["weight"])).all()
+    assert (st[..., 3] > 0).mean() > 0.05          # a populated film, not only zero cells
+    for y in range(H):
+        h, w, pix = _hdr_pixels(f"{name}_{y:04d}.hdr")
+        if T >= 8:
+            assert (h, w) == (W, T) and (pix == st[y]).all()
+        else:
+            assert (h, w) == (T, W) and (pix == st[y].transpose(1, 0, 2)).all()
+    h, w, pix = _hdr_pixels(name + ".hdr")
+    assert (h, w) == (H, W) and (pix == sd).all()
+    with gpu.Context(sc) as c:
+        with pytest.raises(ValueError):
+            c.render_film(0, 1, st, sd, np.empty((H, W), np.uint8))
+
+
+def test_render_film_with_a_short_last_sample_chunk(gpu):
+    """256 paths per camera sample and 9,000 samples per pixel: the 2^21-slot wave holds 8,192
+    samples of a pixel, so the samples come in two chunks and the short last one packs ten
+    pixels into each batch; every delivered row equals the device film (F32 and RGBE)."""
+    sc = S.cornell(width=4, height=4, time_bins=32, exposure=0.1, sqrt_spp=1, max_bounces=2,
+                   incoming_samples=256)
+    H, W, T = sc.height, sc.width, sc.time_bins
+    n = 9000
+    st, sd, wt = _arrays(sc, np.float32, False)
+    with gpu.Context(sc) as c:
+        c.render_film(0, n, st, sd, wt)
+        f = c.film()
+    assert (wt == n).all()
+    assert (st == f["streak"].astype(np.float32)).all() and (sd == f["steady"].astype(np.float32)).all()
+    s8 = np.zeros((H, W, T, 4), np.uint8)
+    d8 = np.zeros((H, W, 4), np.uint8)
+    with gpu.Context(sc) as c:
+        c.render_film(0, n, s8, d8)
+        f = c.film()
+    assert (s8 == _rgbe_np(f["streak"], f["weight"][..., None])).all()
+    assert (d8 == _rgbe_np(f["steady"], f["weight"])).all()
