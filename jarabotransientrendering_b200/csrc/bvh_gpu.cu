@@ -115,28 +115,63 @@ __device__ __forceinline__ int32_t block_node(const int32_t* pn, uint32_t p0, ui
     return (a >= 0 && a == b) ? a : -1;
 }
 
-// triangle and centroid bounds of every active node (shared-memory partials when a block's
-// positions all belong to one node)
+// triangle and centroid bounds of every active node.  Each thread takes kChunk / 256 contiguous
+// positions and keeps their bounds in registers while the node stays the same (a node of the
+// level holds more than kSmall positions, so a thread meets at most two), then adds them with
+// one set of atomics per node; a block whose positions all belong to one node first reduces
+// over each warp and collects in shared memory.  min / max are exact, so the result does not
+// depend on the order.
 __global__ void __launch_bounds__(256) k_bounds(Dev d, int cur, uint32_t nt) {
+    constexpr uint32_t kPer = kChunk / 256;
     __shared__ float s[12];
     const uint32_t p0 = blockIdx.x * kChunk, p1 = min(nt, p0 + kChunk);
     const int32_t* pn = d.pn[cur];
     const int32_t one = block_node(pn, p0, p1);
     if (threadIdx.x < 12) s[threadIdx.x] = (threadIdx.x % 6u) < 3 ? kBig : -kBig;
     __syncthreads();
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+    float b[12];
+    int32_t bn = -1;
+    auto reset = [&]() {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) b[k] = (k % 6) < 3 ? kBig : -kBig;
+    };
+    auto flush = [&](float* nb, float* cb) {
+        amin(nb + 0, b[0]); amin(nb + 1, b[1]); amin(nb + 2, b[2]);
+        amax(nb + 3, b[3]); amax(nb + 4, b[4]); amax(nb + 5, b[5]);
+        amin(cb + 0, b[6]); amin(cb + 1, b[7]); amin(cb + 2, b[8]);
+        amax(cb + 3, b[9]); amax(cb + 4, b[10]); amax(cb + 5, b[11]);
+    };
+    reset();
+    const uint32_t q0 = p0 + threadIdx.x * kPer, q1 = min(p1, q0 + kPer);
+    for (uint32_t i = q0; i < q1; ++i) {
         const int32_t n = pn[i];
         if (n < 0) continue;
+        if (n != bn) {
+            if (bn >= 0 && one < 0) flush(d.nb + 6 * bn, d.cb + 6 * bn);
+            if (one < 0) reset();
+            bn = n;
+        }
         const uint32_t id = d.ids[cur][i];
         const float4 lo = d.plo[id], hi = d.phi[id], c = d.pc[id];
-        float* nb = one >= 0 ? s : d.nb + 6 * n;
-        float* cb = one >= 0 ? s + 6 : d.cb + 6 * n;
-        amin(nb + 0, lo.x); amin(nb + 1, lo.y); amin(nb + 2, lo.z);
-        amax(nb + 3, hi.x); amax(nb + 4, hi.y); amax(nb + 5, hi.z);
-        amin(cb + 0, c.x); amin(cb + 1, c.y); amin(cb + 2, c.z);
-        amax(cb + 3, c.x); amax(cb + 4, c.y); amax(cb + 5, c.z);
+        b[0] = fminf(b[0], lo.x); b[1] = fminf(b[1], lo.y); b[2] = fminf(b[2], lo.z);
+        b[3] = fmaxf(b[3], hi.x); b[4] = fmaxf(b[4], hi.y); b[5] = fmaxf(b[5], hi.z);
+        b[6] = fminf(b[6], c.x); b[7] = fminf(b[7], c.y); b[8] = fminf(b[8], c.z);
+        b[9] = fmaxf(b[9], c.x); b[10] = fmaxf(b[10], c.y); b[11] = fmaxf(b[11], c.z);
     }
-    if (one < 0) return;
+    if (one < 0) {
+        if (bn >= 0) flush(d.nb + 6 * bn, d.cb + 6 * bn);
+        return;
+    }
+    // one node: warp reduction (lanes without positions hold the empty box), lane 0 to shared
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const float o = __shfl_xor_sync(0xffffffffu, b[k], off);
+            b[k] = (k % 6) < 3 ? fminf(b[k], o) : fmaxf(b[k], o);
+        }
+    }
+    if ((threadIdx.x & 31u) == 0) flush(s, s + 6);
     __syncthreads();
     if (threadIdx.x < 3) {
         amin(d.nb + 6 * one + threadIdx.x, s[threadIdx.x]);
@@ -262,31 +297,47 @@ __global__ void k_split(Dev d, int cur, uint32_t na) {
 }
 
 // triangles into their child's range (order within a child is arbitrary: min/max and counts do
-// not depend on it); finished positions are carried over unchanged
+// not depend on it); finished positions are carried over unchanged.  The lanes of a warp going
+// to the same child take their slots with one atomic (iterations are warp-uniform).
 __global__ void k_partition(Dev d, int cur, uint32_t nt) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
-        const int32_t n = d.pn[cur][i];
-        const uint32_t id = d.ids[cur][i];
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < nt; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        int32_t n = -1, key = -1, side = 0;
+        uint32_t id = 0, pos = i, first = 0, nl = 0;
+        if (i < nt) {
+            n = d.pn[cur][i];
+            id = d.ids[cur][i];
+            if (n >= 0) {
+                first = d.act[cur][n].x;
+                nl = d.d_nl[n];
+                const int32_t ax = d.d_ax[n];
+                if (ax < 0) {
+                    side = i - first >= nl ? 1 : 0;
+                } else {
+                    const float* cb = d.cb + 6 * n;
+                    const float4 c = d.pc[id];
+                    const float cc = ax == 0 ? c.x : (ax == 1 ? c.y : c.z);
+                    side = bin_of(cc, cb[ax], d.d_scale[n]) > d.d_split[n] ? 1 : 0;
+                    key = 2 * n + side;
+                }
+            }
+        }
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        uint32_t base = 0;
+        if (key >= 0 && (int)lane == leader)
+            base = atomicAdd(side ? &d.rcur[n] : &d.lcur[n], (uint32_t)__popc(grp));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (i >= nt) continue;
         if (n < 0) {
             d.ids[cur ^ 1][i] = id;
             d.pn[cur ^ 1][i] = -1;
             continue;
         }
-        const uint32_t first = d.act[cur][n].x;
-        const uint32_t nl = d.d_nl[n];
-        const int32_t ax = d.d_ax[n];
-        uint32_t pos;
-        int side;
-        if (ax < 0) {
-            side = i - first >= nl ? 1 : 0;
-            pos = i;
-        } else {
-            const float* cb = d.cb + 6 * n;
-            const float4 c = d.pc[id];
-            const float cc = ax == 0 ? c.x : (ax == 1 ? c.y : c.z);
-            side = bin_of(cc, cb[ax], d.d_scale[n]) > d.d_split[n] ? 1 : 0;
-            pos = side ? first + nl + atomicAdd(&d.rcur[n], 1u) : first + atomicAdd(&d.lcur[n], 1u);
-        }
+        if (key >= 0) pos = (side ? first + nl : first) + base + (uint32_t)__popc(grp & lt);
         d.ids[cur ^ 1][pos] = id;
         d.pn[cur ^ 1][pos] = d.d_child[2 * n + side];
     }
