@@ -475,9 +475,16 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
         const uint32_t ns_last = ns_total - ((ns_total - 1u) / ns_chunk) * ns_chunk;
         const size_t ppb_last = std::min<uint64_t>(win_pix, std::max<uint32_t>(1u, cap / (ns_last * ninc)));
         const size_t stage = ppb_last * ((size_t)T * 3u + 4u);
-        if ((f32 || rgbe) && x->stage_floats < stage) {
+        if (f32 && x->stage_floats < stage) {
             x->d_stage = x->alloc<float>(stage);
             x->stage_floats = stage;
+        }
+        // RGBE: the images of the whole film in device memory (a third of the FP32 bytes), so each
+        // batch is encoded on its own lane right after its splat and the copy stream only copies
+        const size_t cells = (size_t)x->film.width * x->film.height * ((size_t)T + 1u);
+        if (rgbe && x->rgbe_cells < cells) {
+            x->d_rgbe = x->alloc<uchar4>(cells);
+            x->rgbe_cells = cells;
         }
     }
     // Wave lanes: with more than one pixel batch and each pixel in one batch only (a single
@@ -601,25 +608,27 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
             sh_l += x->integ.max_bounces;
             if (sink && sb + ns >= ns_total) {
                 // window = whole frame: the batch's pixels are contiguous film rows
+                const size_t p0 = pb, np = npix;
+                const size_t npix_all = (size_t)x->film.width * x->film.height;
+                uchar4* rst = rgbe ? x->d_rgbe + p0 * T : nullptr;
+                uchar4* rsd = rgbe ? x->d_rgbe + npix_all * T + p0 : nullptr;
+                if (rgbe) {
+                    TR_CUDA(trk::launch_to_rgbe(x->d_streak + p0 * T * 3u, x->d_steady + p0 * 3u, x->d_weight + p0,
+                                                (uint32_t)np, T, sink->streak ? rst : nullptr,
+                                                sink->steady ? rsd : nullptr, ls));
+                    launches += 1;
+                }
                 cudaEvent_t done = ev_get();
                 TR_CUDA(cudaEventRecord(done, ls));
                 TR_CUDA(cudaStreamWaitEvent(x->copy_stream, done, 0));
-                const size_t p0 = pb, np = npix;
                 const size_t es = f32 ? sizeof(float) : sizeof(double);
                 const size_t n_st = np * T * 3u, n_sd = np * 3u;
                 if (rgbe) {
-                    // RGBE cells (4 bytes each) in the staging buffer, which holds 3 T + 4 floats per pixel
-                    uchar4* st = reinterpret_cast<uchar4*>(x->d_stage);
-                    uchar4* sd = st + np * T;
-                    TR_CUDA(trk::launch_to_rgbe(x->d_streak + p0 * T * 3u, x->d_steady + p0 * 3u, x->d_weight + p0,
-                                                (uint32_t)np, T, sink->streak ? st : nullptr,
-                                                sink->steady ? sd : nullptr, x->copy_stream));
-                    launches += 1;
                     if (sink->streak)
-                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->streak) + p0 * T * 4u, st, np * T * 4u,
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->streak) + p0 * T * 4u, rst, np * T * 4u,
                                                 cudaMemcpyDeviceToHost, x->copy_stream));
                     if (sink->steady)
-                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->steady) + p0 * 4u, sd, np * 4u,
+                        TR_CUDA(cudaMemcpyAsync(static_cast<char*>(sink->steady) + p0 * 4u, rsd, np * 4u,
                                                 cudaMemcpyDeviceToHost, x->copy_stream));
                 } else if (f32) {
                     float* st = x->d_stage;

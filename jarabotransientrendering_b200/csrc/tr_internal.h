@@ -163,6 +163,8 @@ struct tr_ctx {
     size_t next_dep = 0;
     float* d_stage = nullptr;               // FP32 staging of one pixel batch's rows
     size_t stage_floats = 0;
+    uchar4* d_rgbe = nullptr;               // RGBE film images: [H][W][T] streak cells, then [H][W] steady
+    size_t rgbe_cells = 0;
     int trace_grid = 0;
 
     // ray-batch scratch
