@@ -234,51 +234,87 @@ __device__ __forceinline__ int32_t schedule(Dev& d, int nxt, uint32_t first, uin
     return (int32_t)k;
 }
 
-// one thread per active node: the host builder's SAH sweep (more than kSmall triangles: no
-// leaf test) and the children's scheduling
-__global__ void k_split(Dev d, int cur, uint32_t na) {
-    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= na) return;
+// one warp per active node, lane b holding bin b: the host builder's SAH sweep (more than kSmall
+// triangles: no leaf test) and the children's scheduling.  The right-hand and left-hand boxes and
+// counts are suffix and prefix scans over the lanes (min / max and integer sums: exact, so equal
+// to the host's sequential sweep), each split's cost is the host's expression, and the cheapest
+// split is the first in (axis, bin) order, as the host's strict comparison picks it.
+__global__ void __launch_bounds__(128) k_split(Dev d, int cur, uint32_t na) {
+    const uint32_t n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = (int)(threadIdx.x & 31u);
+    if (n >= na) return;                               // whole warps leave together
     const uint4 A = d.act[cur][n];
     const uint32_t first = A.x, count = A.y;
     const float* nb = d.nb + 6 * n;
     const float* cb = d.cb + 6 * n;
     float best = 3.4e38f;
-    int bax = -1, bsplit = -1;
+    int bidx = 0x7fffffff;                             // axis * kBins + bin of the best split
+    uint32_t lcnt_at[3];
     for (int ax = 0; ax < 3; ++ax) {
+        lcnt_at[ax] = 0;
         const float ext = cb[3 + ax] - cb[ax];
         if (!(ext > 0.f)) continue;
-        const float* bb = d.bb + (size_t)(n * 3 + ax) * kBins * 6;
-        const uint32_t* bc = d.bc + (size_t)(n * 3 + ax) * kBins;
-        float ra[kBins];
-        uint32_t rc[kBins];
-        float alo[3], ahi[3];
-        box_empty(alo, ahi);
-        uint32_t cnt = 0;
-        for (int b = kBins - 1; b > 0; --b) {
-            box_grow(alo, ahi, bb + b * 6, bb + b * 6 + 3);
-            cnt += bc[b];
-            ra[b] = area(alo, ahi);
-            rc[b] = cnt;
+        const float* bb = d.bb + ((size_t)(n * 3 + ax) * kBins + lane) * 6;
+        const uint32_t c0 = d.bc[(size_t)(n * 3 + ax) * kBins + lane];
+        float rlo[3] = {bb[0], bb[1], bb[2]}, rhi[3] = {bb[3], bb[4], bb[5]};
+        float llo[3] = {bb[0], bb[1], bb[2]}, lhi[3] = {bb[3], bb[4], bb[5]};
+        uint32_t rc = c0, lc = c0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            float t[6];
+            uint32_t tc;
+            // suffix: bins lane .. 31
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                t[k] = __shfl_down_sync(0xffffffffu, rlo[k], off);
+                t[3 + k] = __shfl_down_sync(0xffffffffu, rhi[k], off);
+            }
+            tc = __shfl_down_sync(0xffffffffu, rc, off);
+            if (lane + off < 32) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { rlo[k] = fminf(rlo[k], t[k]); rhi[k] = fmaxf(rhi[k], t[3 + k]); }
+                rc += tc;
+            }
+            // prefix: bins 0 .. lane
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                t[k] = __shfl_up_sync(0xffffffffu, llo[k], off);
+                t[3 + k] = __shfl_up_sync(0xffffffffu, lhi[k], off);
+            }
+            tc = __shfl_up_sync(0xffffffffu, lc, off);
+            if (lane >= off) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { llo[k] = fminf(llo[k], t[k]); lhi[k] = fmaxf(lhi[k], t[3 + k]); }
+                lc += tc;
+            }
         }
-        box_empty(alo, ahi);
-        cnt = 0;
-        for (int b = 0; b < kBins - 1; ++b) {
-            box_grow(alo, ahi, bb + b * 6, bb + b * 6 + 3);
-            cnt += bc[b];
-            if (cnt == 0 || rc[b + 1] == 0) continue;
-            const float cost = area(alo, ahi) * (float)cnt + ra[b + 1] * (float)rc[b + 1];
-            if (cost < best) { best = cost; bax = ax; bsplit = b; }
+        // split after bin `lane`: left = bins 0..lane, right = bins lane+1..31
+        const float ra = area(rlo, rhi);
+        const float ra_next = __shfl_down_sync(0xffffffffu, ra, 1);
+        const uint32_t rc_next = __shfl_down_sync(0xffffffffu, rc, 1);
+        lcnt_at[ax] = lc;
+        if (lane < kBins - 1 && lc != 0 && rc_next != 0) {
+            const float cost = area(llo, lhi) * (float)lc + ra_next * (float)rc_next;
+            if (cost < best) { best = cost; bidx = ax * kBins + lane; }
         }
     }
-    uint32_t nl;
-    if (bax < 0) {
-        nl = count / 2;                               // median split by position
-    } else {
-        const uint32_t* bc = d.bc + (size_t)(n * 3 + bax) * kBins;
-        nl = 0;
-        for (int b = 0; b <= bsplit; ++b) nl += bc[b];
+    // first minimum over the lanes in (axis, bin) order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+        if (ob < best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
     }
+    const int bax = bidx == 0x7fffffff ? -1 : bidx / kBins;
+    const int bsplit = bidx == 0x7fffffff ? -1 : bidx % kBins;
+    // left count = the prefix count at the split bin (lane bsplit of that axis's scan)
+    uint32_t nl_ax = 0;
+    for (int ax = 0; ax < 3; ++ax) {
+        const uint32_t v = __shfl_sync(0xffffffffu, lcnt_at[ax], bsplit < 0 ? 0 : bsplit);
+        if (ax == bax) nl_ax = v;
+    }
+    if (lane != 0) return;
+    const uint32_t nl = bax < 0 ? count / 2 : nl_ax;    // median split by position without a SAH split
     const uint32_t base = atomicAdd(&d.counters[0], 2u);
     BinNode& o = d.nodes[A.z];
     for (int k = 0; k < 3; ++k) { o.lo[k] = nb[k]; o.hi[k] = nb[3 + k]; }
@@ -617,7 +653,7 @@ bool build_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_t, uint32
         k_bounds<<<chunks, 256, 0, s>>>(d, cur, nt);
         k_bin<<<chunks, 256, 0, s>>>(d, cur, nt);
         TR_CUDA(cudaMemsetAsync(d.counters + 1, 0, sizeof(uint32_t), s));
-        k_split<<<(na + 127) / 128, 128, 0, s>>>(d, cur, na);
+        k_split<<<(na + 3) / 4, 128, 0, s>>>(d, cur, na);      // one warp per active node
         k_partition<<<grid_nt, 256, 0, s>>>(d, cur, nt);
         TR_CUDA(cudaGetLastError());
         cur ^= 1;
