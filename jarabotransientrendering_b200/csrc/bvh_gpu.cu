@@ -38,6 +38,14 @@ __device__ __forceinline__ void amax(float* a, float v) {
     if (v >= 0.0f) atomicMax(reinterpret_cast<int*>(a), __float_as_int(v));
     else atomicMin(reinterpret_cast<unsigned*>(a), __float_as_uint(v));
 }
+// the same in shared memory, skipped when v does not improve the stored value: a stored min
+// only decreases, so a value not below it now is not below the final one (exact)
+__device__ __forceinline__ void amin_s(float* a, float v) {
+    if (v < *reinterpret_cast<volatile float*>(a)) amin(a, v);
+}
+__device__ __forceinline__ void amax_s(float* a, float v) {
+    if (v > *reinterpret_cast<volatile float*>(a)) amax(a, v);
+}
 __device__ __forceinline__ int bin_of(float c, float lo, float scale) {
     const int b = (int)((c - lo) * scale);
     return b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
@@ -203,11 +211,17 @@ __global__ void __launch_bounds__(256) k_bin(Dev d, int cur, uint32_t nt) {
             if (!(ext > 0.f)) continue;
             const float scale = (float)kBins / ext;
             const int b = bin_of(cc[a], cb[a], scale);
-            float* bx = one >= 0 ? sb + (a * kBins + b) * 6 : d.bb + ((size_t)(n * 3 + a) * kBins + b) * 6;
-            uint32_t* bn = one >= 0 ? sc + a * kBins + b : d.bc + (size_t)(n * 3 + a) * kBins + b;
-            amin(bx + 0, lo.x); amin(bx + 1, lo.y); amin(bx + 2, lo.z);
-            amax(bx + 3, hi.x); amax(bx + 4, hi.y); amax(bx + 5, hi.z);
-            atomicAdd(bn, 1u);
+            if (one >= 0) {
+                float* bx = sb + (a * kBins + b) * 6;
+                amin_s(bx + 0, lo.x); amin_s(bx + 1, lo.y); amin_s(bx + 2, lo.z);
+                amax_s(bx + 3, hi.x); amax_s(bx + 4, hi.y); amax_s(bx + 5, hi.z);
+                atomicAdd(sc + a * kBins + b, 1u);
+            } else {
+                float* bx = d.bb + ((size_t)(n * 3 + a) * kBins + b) * 6;
+                amin(bx + 0, lo.x); amin(bx + 1, lo.y); amin(bx + 2, lo.z);
+                amax(bx + 3, hi.x); amax(bx + 4, hi.y); amax(bx + 5, hi.z);
+                atomicAdd(d.bc + (size_t)(n * 3 + a) * kBins + b, 1u);
+            }
         }
     }
     if (one < 0) return;
