@@ -382,8 +382,8 @@ namespace {
 tr_status guide_begin_render(tr_ctx* x, cudaStream_t s);
 tr_status guide_end_render(tr_ctx* x, cudaStream_t s);
 
-// Host buffers the film is streamed into while rendering (tr_render_film): FP64 or FP32 sums
-// of the whole frame.
+// Host buffers the film is streamed into while rendering (tr_render_film): FP64 or FP32 sums,
+// or RGBE images, of the whole frame.
 struct FilmSink { int type; void* streak; void* steady; void* weight; };
 
 tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
@@ -414,6 +414,8 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
     }
     // samples per pixel per batch, and pixels per batch
     uint32_t ns_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(ns_total, cap / ninc));
+    const bool film_was_clean = x->film_clean;
+    x->film_clean = false;
     cudaStream_t strm = x->s();
     // per-kernel timing: an event before and after each launch, kind-tagged.  Read out at the
     // end of the render (profiling 1) or at tr_stats_get (profiling 2; a long series of renders
@@ -596,7 +598,16 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 launches += 1 + 2ull * x->bd.nvert;
                 sh_l += x->bd.nvert;
             }
-            tl(4, [&] { return trk::launch_splat(p, ls); });
+            if (rgbe && sb + ns >= ns_total) {
+                // final pixels: the splat blocks encode their images as they finish them
+                trk::Params ps = p;
+                ps.film.rgbe_streak = x->d_rgbe;
+                ps.film.rgbe_steady = x->d_rgbe + (size_t)x->film.width * x->film.height * T;
+                ps.film.rgbe_fresh = (film_was_clean && ns_chunk >= ns_total) ? 1u : 0u;
+                tl(4, [&] { return trk::launch_splat(ps, ls); });
+            } else {
+                tl(4, [&] { return trk::launch_splat(p, ls); });
+            }
             for (uint32_t b = 0; b < x->film.bounce_films; ++b)
                 tl(4, [&] { return trk::launch_splat(p, ls, (int)b); });
             if (x->film.bounce_films) {
@@ -612,12 +623,6 @@ tr_status render_region(tr_ctx* x, uint32_t x0, uint32_t y0, uint32_t x1, uint32
                 const size_t npix_all = (size_t)x->film.width * x->film.height;
                 uchar4* rst = rgbe ? x->d_rgbe + p0 * T : nullptr;
                 uchar4* rsd = rgbe ? x->d_rgbe + npix_all * T + p0 : nullptr;
-                if (rgbe) {
-                    TR_CUDA(trk::launch_to_rgbe(x->d_streak + p0 * T * 3u, x->d_steady + p0 * 3u, x->d_weight + p0,
-                                                (uint32_t)np, T, sink->streak ? rst : nullptr,
-                                                sink->steady ? rsd : nullptr, ls));
-                    launches += 1;
-                }
                 cudaEvent_t done = ev_get();
                 TR_CUDA(cudaEventRecord(done, ls));
                 TR_CUDA(cudaStreamWaitEvent(x->copy_stream, done, 0));
@@ -981,6 +986,7 @@ tr_status tr_clear_film(tr_ctx* x) {
     if (!x) return fail(TR_ERR_INVALID_ARGUMENT, "null context");
     try {
         TR_CUDA(cudaSetDevice(x->device));
+        x->film_clean = true;
         const size_t npix = (size_t)x->film.width * x->film.height;
         TR_CUDA(cudaMemsetAsync(x->d_streak, 0, npix * x->film.time_bins * 3u * sizeof(double), x->s()));
         TR_CUDA(cudaMemsetAsync(x->d_steady, 0, npix * 3u * sizeof(double), x->s()));
@@ -1244,6 +1250,7 @@ extern "C" tr_status tr_render_region_noalloc(tr_ctx* x, uint32_t x0, uint32_t y
     if (s0 + ns > (1ull << 32)) return fail(TR_ERR_INVALID_ARGUMENT, "camera sample index must stay below 2^32");
     if (x->integ.flags & TR_FLAG_BIDIRECTIONAL)
         return fail(TR_ERR_NOT_SUPPORTED, "light subpaths need their vertex arrays: render with tr_render");
+    x->film_clean = false;
     if (x->integ.max_bounces > TR_NOALLOC_MAX_BOUNCES)
         return fail(TR_ERR_INVALID_ARGUMENT, "tr_render_region_noalloc supports max_bounces <= " +
                                                  std::to_string(TR_NOALLOC_MAX_BOUNCES) + " (scene has " +

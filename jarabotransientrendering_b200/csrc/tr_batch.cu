@@ -488,6 +488,7 @@ tr_status tr_batch_get_config(tr_batch* b, tr_batch_config* cfg) {
 
 tr_status tr_batch_render(tr_batch* b, const uint64_t* sample_begin, const uint32_t* sample_count) {
     if (!b || !sample_begin || !sample_count) return fail(TR_ERR_INVALID_ARGUMENT, "null argument");
+    for (tr_ctx* x : b->ctx) x->film_clean = false;
     try {
         return batch_render(b, sample_begin, sample_count);
     } catch (const CudaError& e) {

@@ -165,6 +165,7 @@ struct tr_ctx {
     size_t stage_floats = 0;
     uchar4* d_rgbe = nullptr;               // RGBE film images: [H][W][T] streak cells, then [H][W] steady
     size_t rgbe_cells = 0;
+    bool film_clean = true;                 // no samples added since the film was zeroed
     int trace_grid = 0;
 
     // ray-batch scratch

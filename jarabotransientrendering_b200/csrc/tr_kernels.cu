@@ -844,6 +844,30 @@ __global__ void __launch_bounds__(256, kMulti ? 2 : ((kGuided || kTimeSampling) 
 // lane and added the same way once per pass over the slots.
 // -----------------------------------------------------------------------------------------
 
+// Averaged film cells in the reference's .hdr encoding (the host writer's rgbe_encode of
+// avg_nan0(sum, weight), tr_film_io.cpp; ImageIO.h:146-193): the average in double rounded to
+// float (NaN -> 0), then the largest channel v = m 2^e (frexp, m in [0.5, 1)), scale m 256 / v,
+// each channel truncated to [0, 255], exponent e + 128; 0 for v < 1e-32.
+__device__ __forceinline__ float film_avg(double v, double w) {
+    const double t = v / w;
+    return isnan(t) ? 0.0f : (float)t;
+}
+__device__ __forceinline__ unsigned char rgbe_q(float c, float scale) {
+    const float s = c * scale;
+    return (unsigned char)(s > 0.f ? (s < 255.f ? s : 255.f) : 0.f);
+}
+// cell c (three FP64 sums, read through L2: just written by this block's atomics)
+__device__ __forceinline__ uchar4 rgbe_cell(const double* c, double w) {
+    const float r = film_avg(__ldcg(c), w), g = film_avg(__ldcg(c + 1), w), b = film_avg(__ldcg(c + 2), w);
+    float v = r > g ? r : g;
+    v = v > b ? v : b;
+    if (!(v >= 1e-32f)) return make_uchar4(0, 0, 0, 0);
+    int e = 0;
+    const float m = frexpf(v, &e);
+    const float scale = m * 256.0f / v;
+    return make_uchar4(rgbe_q(r, scale), rgbe_q(g, scale), rgbe_q(b, scale), (unsigned char)(e + 128));
+}
+
 // Sum (x, y, z) over the lanes of `peers` (the calling lane's group, all lanes active); the
 // group's lowest lane receives the total.  Tree over the group's ranks: at step s the member of
 // rank r (r a multiple of 2s) adds the partial sum of rank r + s.  Each lane keeps the lane
@@ -905,6 +929,14 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
     const uint32_t slot0 = B.slot_begin + pix0 * per_pix;
     const size_t rs = p.wave.capacity;           // records are [bounce][slot]
     const unsigned lane = threadIdx.x & 31u;
+    // RGBE images of a fresh film: one bit per (pixel, bin) cell this block adds to (dynamic
+    // shared memory, sized by the launcher)
+    extern __shared__ uint32_t touched[];
+    const bool mark = !kMulti && bsel < 0 && film.rgbe_streak != nullptr && film.rgbe_fresh != 0u;
+    if (mark) {
+        for (uint32_t i = threadIdx.x; i < (gp * T + 31u) / 32u; i += blockDim.x) touched[i] = 0u;
+        __syncthreads();
+    }
     for (uint32_t base = (threadIdx.x & ~31u); base < nslots; base += blockDim.x) {
         const uint32_t ls = base + lane;
         const bool act = ls < nslots;
@@ -935,6 +967,10 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
             if (inwin && (peers & lanemask_lt()) == 0u) {
                 double* cell = out_streak + film_pixel(pl) * TT + (size_t)bin * 3u;
                 atomicAdd(cell, (double)vx); atomicAdd(cell + 1, (double)vy); atomicAdd(cell + 2, (double)vz);
+                if (mark) {
+                    const uint32_t c = pl * T + bin;
+                    atomicOr(&touched[c >> 5], 1u << (c & 31u));
+                }
             }
             if (inwin || (steady_all && valid)) { ax += rc.x; ay += rc.y; az += rc.z; }
         }
@@ -952,6 +988,27 @@ __global__ void __launch_bounds__(kSplatBlock) k_splat(const __grid_constant__ P
     // sample chunks of the same pixels)
     if (bsel < 0)
         for (uint32_t pl = threadIdx.x; pl < gp; pl += blockDim.x) atomicAdd(&film.weight[film_pixel(pl)], (double)B.ns);
+    if constexpr (!kMulti) {
+        if (bsel < 0 && film.rgbe_streak) {
+            // the block's pixels are final: their images, cell by cell (the block's own atomics
+            // are visible to it after the barrier)
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < gp * (T + 1u); i += blockDim.x) {
+                if (i < gp * T) {
+                    const uint32_t pl = i / T, t = i - pl * T;
+                    const size_t fp = film_pixel(pl);
+                    // a cell of a fresh film that this block did not add to is zero: RGBE 0
+                    const bool any = !mark || ((touched[i >> 5] >> (i & 31u)) & 1u) != 0u;
+                    film.rgbe_streak[fp * T + t] =
+                        any ? rgbe_cell(out_streak + fp * TT + (size_t)t * 3u, __ldcg(&film.weight[fp]))
+                            : make_uchar4(0, 0, 0, 0);
+                } else {
+                    const size_t fp = film_pixel(i - gp * T);
+                    film.rgbe_steady[fp] = rgbe_cell(out_steady + fp * 3u, __ldcg(&film.weight[fp]));
+                }
+            }
+        }
+    }
 }
 
 // Per-bounce film weights (MultibounceStreakCameraFilm.h:151-171 with StreakCameraFilm.h:139-160):
@@ -1454,7 +1511,17 @@ cudaError_t launch_splat(const Params& p, cudaStream_t s, int bsel) {
     } else {
         const uint32_t G = splat_pixels_per_block(p.batch.ns * p.batch.ninc);
         const uint32_t blocks = (p.batch.npix + G - 1) / G;
-        k_splat<false><<<blocks, kSplatBlock, 0, s>>>(p, (int)G, bsel);
+        // a fresh film's RGBE images: the cells each block adds to, one bit each (up to 32 KB;
+        // beyond that every cell is read back)
+        const size_t bits = (size_t)G * p.film.T;
+        const bool mark = bsel < 0 && p.film.rgbe_streak && p.film.rgbe_fresh && bits <= 32u * 8192u;
+        if (p.film.rgbe_fresh && !mark) {
+            Params q = p;
+            q.film.rgbe_fresh = 0;
+            k_splat<false><<<blocks, kSplatBlock, 0, s>>>(q, (int)G, bsel);
+        } else {
+            k_splat<false><<<blocks, kSplatBlock, mark ? (bits + 31u) / 32u * 4u : 0u, s>>>(p, (int)G, bsel);
+        }
     }
     return cudaGetLastError();
 }
@@ -1526,55 +1593,6 @@ cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t 
     const size_t need = (n + 255) / 256;
     const int grid = (int)std::min<size_t>(need, (size_t)sms * 8);
     k_to_f32<<<std::max(1, grid), 256, 0, s>>>(src, dst, n);
-    return cudaGetLastError();
-}
-
-// Averaged film cells in the reference's .hdr encoding (the host writer's rgbe_encode of
-// avg_nan0(sum, weight), tr_film_io.cpp; ImageIO.h:146-193): the average in double rounded to
-// float (NaN -> 0), then the largest channel v = m 2^e (frexp, m in [0.5, 1)), scale m 256 / v,
-// each channel truncated to [0, 255], exponent e + 128; 0 for v < 1e-32.
-__device__ __forceinline__ float film_avg(double v, double w) {
-    const double t = v / w;
-    return isnan(t) ? 0.0f : (float)t;
-}
-__device__ __forceinline__ unsigned char rgbe_q(float c, float scale) {
-    const float s = c * scale;
-    return (unsigned char)(s > 0.f ? (s < 255.f ? s : 255.f) : 0.f);
-}
-__device__ __forceinline__ uchar4 rgbe_cell(const double* __restrict__ c, double w) {
-    const float r = film_avg(__ldcs(c), w), g = film_avg(__ldcs(c + 1), w), b = film_avg(__ldcs(c + 2), w);
-    float v = r > g ? r : g;
-    v = v > b ? v : b;
-    if (!(v >= 1e-32f)) return make_uchar4(0, 0, 0, 0);
-    int e = 0;
-    const float m = frexpf(v, &e);
-    const float scale = m * 256.0f / v;
-    return make_uchar4(rgbe_q(r, scale), rgbe_q(g, scale), rgbe_q(b, scale), (unsigned char)(e + 128));
-}
-// one thread per cell: the npix x T streak cells, then the npix steady cells; 24 B read, 4 B
-// written per cell (HBM-bound)
-__global__ void __launch_bounds__(256) k_to_rgbe(const double* __restrict__ streak, const double* __restrict__ steady,
-                                                 const double* __restrict__ weight, uint32_t npix, uint32_t T,
-                                                 uchar4* __restrict__ os, uchar4* __restrict__ od) {
-    const size_t ns = (size_t)npix * T, n = ns + npix;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (i < ns) {
-            if (os) os[i] = rgbe_cell(streak + i * 3, weight[i / T]);
-        } else if (od) {
-            const size_t px = i - ns;
-            od[px] = rgbe_cell(steady + px * 3, weight[px]);
-        }
-    }
-}
-cudaError_t launch_to_rgbe(const double* streak, const double* steady, const double* weight, uint32_t npix,
-                           uint32_t T, uchar4* out_streak, uchar4* out_steady, cudaStream_t s) {
-    if (npix == 0 || T == 0) return cudaSuccess;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t need = ((size_t)npix * (T + 1u) + 255) / 256;
-    const int grid = (int)std::min<size_t>(need, (size_t)sms * 8);
-    k_to_rgbe<<<std::max(1, grid), 256, 0, s>>>(streak, steady, weight, npix, T, out_streak, out_steady);
     return cudaGetLastError();
 }
 

@@ -149,6 +149,13 @@ struct FilmDev {
     double* cdepth;           // [H][W] camera-ray record sums
     double* cpos;             // [H][W][3]
     double* cnorm;            // [H][W][3]
+    // set on the splat launch of a batch whose pixels are final (last sample chunk) when the film
+    // is delivered as RGBE images: each splat block encodes its pixels once it has added them
+    uchar4* rgbe_streak = nullptr;   // [H][W][T]
+    uchar4* rgbe_steady = nullptr;   // [H][W]
+    // the film held no samples before this render, which has one sample chunk: a splat block's
+    // pixels hold only its own additions, so cells it did not add to are zero
+    uint32_t rgbe_fresh = 0;
 };
 
 // bin of a radiance sample outside the time window: kept (with bounce films only) because the
@@ -249,10 +256,7 @@ cudaError_t launch_build_tris(const float* vertices, const uint32_t* triangles, 
                               const uint32_t* order, uint32_t nt, float4* tris, float4* tri_ng, cudaStream_t s);
 // FP64 film sums -> FP32 (film streaming)
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
-// film cells averaged by their pixel's weight and RGBE-encoded as the .hdr writer does:
-// streak [npix][T] and steady [npix] RGBE quadruples from npix pixels' FP64 sums
-cudaError_t launch_to_rgbe(const double* streak, const double* steady, const double* weight, uint32_t npix,
-                           uint32_t T, uchar4* out_streak, uchar4* out_steady, cudaStream_t s);
+
 cudaError_t launch_advance(uint32_t* cur, uint32_t step, cudaStream_t s);
 cudaError_t launch_trace_user(const SceneDev& sc, const float* rays, uint32_t n, int any_hit,
                               void* out_hits, uint32_t* cursor, int grid, cudaStream_t s);

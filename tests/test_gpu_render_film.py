@@ -224,3 +224,23 @@ def test_render_film_with_a_short_last_sample_chunk(gpu):
         f = c.film()
     assert (s8 == _rgbe_np(f["streak"], f["weight"][..., None])).all()
     assert (d8 == _rgbe_np(f["steady"], f["weight"])).all()
+
+
+def test_render_film_rgbe_after_earlier_samples(gpu):
+    """RGBE delivery of a film that already held samples (an earlier tr_render) and of one whose
+    earlier samples were cleared: both equal the encoding of the final sums."""
+    sc = S.medium(width=32, height=24, time_bins=128, exposure=0.04, sqrt_spp=4, incoming_samples=2, max_bounces=8)
+    H, W, T = sc.height, sc.width, sc.time_bins
+    for clear in (False, True):
+        st = np.full((H, W, T, 4), 7, np.uint8)
+        sd = np.full((H, W, 4), 7, np.uint8)
+        with gpu.Context(sc) as c:
+            c.render(0, 4)
+            if clear:
+                c.clear()
+            c.render_film(4, 8, st, sd)
+            f = c.film()
+        assert (f["weight"] == (8 if clear else 12)).all()
+        assert (st == _rgbe_np(f["streak"], f["weight"][..., None])).all()
+        assert (sd == _rgbe_np(f["steady"], f["weight"])).all()
+        assert (st[..., 3] > 0).mean() > 0.02
