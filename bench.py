@@ -281,10 +281,10 @@ def convergence(args, device):
     2048 bins).  Reference: the plain tracer, two independent halves of ``convergence_ref_spp``
     samples per pixel (its own noise is subtracted from the error).  Both samplers render passes of
     64 samples per pixel from a fresh context and network; the guided run trains online (a pool of
-    131,072 samples per pass in batches of 65,536, Adam lr 5e-3, mixture probability 0.7), drops
-    its first 2,048 samples per pixel after training on them and stops training once the film holds
-    8,192 samples per pixel.  Time = host wall clock of the render calls (training included); the
-    error evaluation between passes is not timed."""
+    131,072 samples per pass in batches of 65,536, Adam lr 5e-3, mixture probability 0.7), first
+    trains on 32 warm-up passes of 16 samples per pixel that it then drops, and stops training once
+    the film holds 8,192 samples per pixel.  Time = host wall clock of the render calls (warm-up and
+    training included); the error evaluation between passes is not timed."""
     import torch
     from jarabotransientrendering_b200 import convergence as CV, renderer as R, scenes as S
     sc = S.guided()
@@ -296,8 +296,8 @@ def convergence(args, device):
     g = R.Guide(device=device, seed=1)
     try:
         guided = CV.time_to_error(sc, ref, target=0.05, pass_spp=64, max_spp=262144, guide=g, mix_prob=0.7,
-                                  learning_rate=5e-3, train_pool=131072, device=device, warmup_spp=2048,
-                                  train_spp=8192)
+                                  learning_rate=5e-3, train_pool=131072, device=device, warmup_spp=512,
+                                  warmup_pass_spp=16, train_spp=8192)
     finally:
         g.close()
     ref_noise = ref.rel_noise
@@ -306,7 +306,7 @@ def convergence(args, device):
 
     def leg(r):
         return {"seconds": r["seconds"], "spp": r["spp"], "warmup_spp": r["warmup_spp"],
-                "train_spp": r["train_spp"],
+                "warmup_pass_spp": r["warmup_pass_spp"], "train_spp": r["train_spp"],
                 "paths_per_s": r["paths_per_s"], "train_steps": r["train_steps"],
                 "rel_l2_at_stop": r["curve"][-1][2] if r["curve"] else None}
     res = {"metric": "seconds to 5% rel-L2 streak-film error (lower is better)", "unit": "s",
@@ -679,11 +679,11 @@ def main():
         d2h = sum(a.nbytes for a in rg)
         del rg
         f32 = host_film(torch.float32)
-        et32, ph32 = e2e_run(f32, 1)
+        et32, ph32 = e2e_run(f32, 2)
         d2h32 = sum(a.nbytes for a in f32)
         del f32
         f64 = host_film(torch.float64)
-        et64, ph64 = e2e_run(f64, 1)
+        et64, ph64 = e2e_run(f64, 2)
         d2h64 = sum(a.nbytes for a in f64)
         del f64
         et = max_over_ranks(et, dist, "cuda")

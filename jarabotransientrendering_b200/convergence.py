@@ -86,14 +86,17 @@ class Reference:
 def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp: int = 4,
                   max_spp: int = 4096, guide: Optional[R.Guide] = None, mix_prob: float = 0.5,
                   learning_rate: float = 1e-3, train_pool: int = 262144, device: int = 0,
-                  sample_offset: int = 1 << 20, warmup_spp: int = 0, train_spp: Optional[int] = None):
+                  sample_offset: int = 1 << 20, warmup_spp: int = 0, train_spp: Optional[int] = None,
+                  warmup_pass_spp: Optional[int] = None):
     """Renders ``scene`` progressively, ``pass_spp`` samples per pixel per pass, until the film's
     rel-L2 against ``ref`` is at most ``target`` (or ``max_spp`` is reached). Sample indices start
     at ``sample_offset``, so the passes are independent of the reference's samples.
 
     With a learned proposal, the first ``warmup_spp`` samples per pixel train the network and are
     then dropped from the film (the film is cleared once), as in the iterative schemes of path
-    guiding; their render and training time counts like every other pass.  ``train_spp`` (when
+    guiding; their render and training time counts like every other pass.  They are rendered in
+    passes of ``warmup_pass_spp`` (default ``pass_spp``): every pass fills the same training pool,
+    so smaller warm-up passes give the network as many training steps for fewer rendered paths.  ``train_spp`` (when
     given) is the training budget: once the film holds that many samples per pixel the network is
     frozen and the remaining passes render with it without training.
 
@@ -112,8 +115,9 @@ def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp
             ctx.set_guide(guide, mix_prob=mix_prob, learning_rate=learning_rate, train_pool=train_pool)
         else:
             warmup_spp = 0
+        wpass = warmup_pass_spp or pass_spp
         while rendered < warmup_spp:
-            n = min(pass_spp, warmup_spp - rendered)
+            n = min(wpass, warmup_spp - rendered)
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
             ctx.render(sample_offset + rendered, n)
@@ -146,5 +150,6 @@ def time_to_error(scene: S.Scene, ref: Reference, target: float = 0.05, pass_spp
         train_loss = ctx.stats()["train_loss"]
     paths = rendered * scene.width * scene.height * scene.incoming_samples
     return {"seconds": reached[0] if reached else None, "spp": reached[1] if reached else None,
-            "warmup_spp": warmup_spp, "train_spp": train_spp, "paths_per_s": paths / spent if spent > 0 else 0.0, "curve": curve,
+            "warmup_spp": warmup_spp, "warmup_pass_spp": (warmup_pass_spp or pass_spp) if warmup_spp else None,
+            "train_spp": train_spp, "paths_per_s": paths / spent if spent > 0 else 0.0, "curve": curve,
             "train_steps": train_steps, "train_loss": train_loss}
