@@ -244,3 +244,18 @@ def test_render_film_rgbe_after_earlier_samples(gpu):
         assert (st == _rgbe_np(f["streak"], f["weight"][..., None])).all()
         assert (sd == _rgbe_np(f["steady"], f["weight"])).all()
         assert (st[..., 3] > 0).mean() > 0.02
+
+
+def test_render_film_rgbe_when_the_touched_cells_do_not_fit_shared_memory(gpu):
+    """One sample per pixel puts 512 pixels in a splat block; with 1,024 bins their cell bitmap
+    (64 KB) exceeds the 32 KB the launcher allows, so the blocks read every cell back instead."""
+    sc = S.cornell(width=64, height=32, time_bins=1024, exposure=0.005, sqrt_spp=1, max_bounces=4)
+    H, W, T = sc.height, sc.width, sc.time_bins
+    st = np.full((H, W, T, 4), 7, np.uint8)
+    sd = np.full((H, W, 4), 7, np.uint8)
+    with gpu.Context(sc) as c:
+        c.render_film(0, 1, st, sd)
+        f = c.film()
+    assert (st == _rgbe_np(f["streak"], f["weight"][..., None])).all()
+    assert (sd == _rgbe_np(f["steady"], f["weight"])).all()
+    assert (st[..., 3] > 0).sum() > 100
