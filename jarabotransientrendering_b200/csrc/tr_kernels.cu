@@ -463,7 +463,7 @@ __device__ __noinline__ TaSample time_angular_sample(f3 l, float mod, float r, f
 // and time-sampling variants 80 (3 CTAs per SM; unbounded they took 146-172 registers and ran
 // one CTA of 8 warps per SM); the multi-scene variants 128 (2 CTAs, no spills).
 template <bool kGuided, bool kMulti, bool kTimeSampling>
-__global__ void __launch_bounds__(256, kMulti ? 2 : (kTimeSampling ? 3 : 4))
+__global__ void __launch_bounds__(256, kMulti ? 3 : (kTimeSampling ? 3 : 4))
     k_shade(const __grid_constant__ Params p, int depth) {
     uint32_t n0 = p.batch.n_slots;
     if constexpr (kMulti) n0 = cur_batch(p).n_slots;
