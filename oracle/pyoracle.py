@@ -106,6 +106,10 @@ def lib():
         L.orc_ggx_sample.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                      C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_ggx_eval_cos.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_hg_eval.argtypes = [C.c_float, C.c_float]
+        L.orc_hg_eval.restype = C.c_float
+        L.orc_hg_sample_cos.argtypes = [C.c_float, C.c_float]
+        L.orc_hg_sample_cos.restype = C.c_float
         L.orc_pcg32_first.restype = C.c_uint32
         L.orc_pcg32_first.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32]
         _lib = L

@@ -559,6 +559,25 @@ static inline float hg_eval(float g, float cs) {
     return ((1.0f - gg) * INV_4PI_F) / (b * sqrtf(b));
 }
 
+/* cosine to the propagation direction of an HG sample by the inverse CDF
+ * (HenyeyGreensteinPhaseFunction.h:218-240); uniform for |g| < 1e-4 */
+static inline float hg_sample_cos(float g, float x2) {
+    float ct;
+    if (fabsf(g) < 1e-4f) {
+        ct = 1.0f - 2.0f * x2;
+    } else {
+        float gg = g * g;
+        float a = (1.0f - gg) / ((1.0f - g) + (2.0f * g) * x2);
+        ct = ((1.0f + gg) - a * a) / (2.0f * g);
+        if (ct < -1.0f) ct = -1.0f;
+        if (ct > 1.0f) ct = 1.0f;
+    }
+    return ct;
+}
+
+float orc_hg_eval(float g, float cs) { return hg_eval(g, cs); }
+float orc_hg_sample_cos(float g, float x) { return hg_sample_cos(g, x); }
+
 static inline int is_finite3(const float* L) {
     return isfinite(L[0]) && isfinite(L[1]) && isfinite(L[2]);
 }
@@ -1145,16 +1164,7 @@ static int trace_path(const orc_ctx* x, v3 org, v3 dir, pcg* rng, pcg* rl, float
             fa = mk((kd.x * INV_PI_F) * ca, (kd.y * INV_PI_F) * ca, (kd.z * INV_PI_F) * ca);
             pa = ct * INV_PI_F;
         } else {
-            float ct;
-            if (fabsf(g) < 1e-4f) {
-                ct = 1.0f - 2.0f * x2;
-            } else {
-                float gg = g * g;
-                float a = (1.0f - gg) / ((1.0f - g) + (2.0f * g) * x2);
-                ct = ((1.0f + gg) - a * a) / (2.0f * g);
-                if (ct < -1.0f) ct = -1.0f;
-                if (ct > 1.0f) ct = 1.0f;
-            }
+            float ct = hg_sample_cos(g, x2);
             float stt = sqrtf(1.0f - ct * ct);
             /* orthonormal frame around the propagation direction (Duff et al., JCGT 6(1), 2017) */
             float sg = copysignf(1.0f, dir.z);

@@ -136,6 +136,11 @@ int  orc_ggx_sample(const float* kd, float alpha, const float* n, const float* w
 void orc_ggx_eval_cos(const float* kd, float alpha, const float* n, const float* wo, const float* wi, float* out);
 
 /* The math kernels shared by the oracle and the CUDA path, exposed for unit tests. */
+/* Henyey-Greenstein phase function (unit tests): density of a cosine, and the cosine the
+ * inverse-CDF sampler returns for a uniform number x. */
+float orc_hg_eval(float g, float cs);
+float orc_hg_sample_cos(float g, float x);
+
 float orc_log(float x);
 float orc_exp(float x);
 void  orc_sincos2pi(float xi, float* s, float* c);

@@ -63,3 +63,32 @@ def test_vmf_lobes_are_normalised_and_sample_their_mean_cosine():
         w = d @ mu
         mean = 1.0 / np.tanh(kappa) - 1.0 / kappa
         assert abs(w.mean() - mean) < 5.0 * w.std() / np.sqrt(n), (kappa, w.mean(), mean)
+
+
+def test_hg_phase_function_is_normalised_with_mean_cosine_g(oracle_lib):
+    """The oracle's Henyey-Greenstein density (HenyeyGreensteinPhaseFunction.h:254-276; the GPU's
+    is the same operation sequence, compared per path) integrates to one over the sphere with
+    mean cosine g, and its inverse-CDF sampler (:218-240) draws cosines with that density."""
+    L = oracle_lib.lib()
+    c = np.linspace(-1.0, 1.0, 200_001)
+    rng = np.random.default_rng(11)
+    xs = rng.random(200_000).astype(np.float32)
+    for g in (-0.9, -0.3, 0.0, 0.3, 0.9):
+        f = np.array([L.orc_hg_eval(g, float(v)) for v in c[::20]], np.float64)
+        cc = c[::20]
+        total = 2.0 * np.pi * np.trapezoid(f, cc)
+        mean = 2.0 * np.pi * np.trapezoid(f * cc, cc)
+        assert abs(total - 1.0) < 2e-3 and abs(mean - g) < 2e-3, (g, total, mean)
+        s = np.array([L.orc_hg_sample_cos(g, float(x)) for x in xs], np.float64)
+        assert (np.abs(s) <= 1.0).all()
+        assert abs(s.mean() - g) < 5.0 * s.std() / np.sqrt(len(s)) + 1e-4, (g, s.mean())
+        # the sampled cosines follow the density: counts per interval against its integral
+        edges = np.linspace(-1.0, 1.0, 21)
+        counts, _ = np.histogram(s, edges)
+        fine = np.linspace(-1.0, 1.0, 20 * 200 + 1)
+        fv = np.array([L.orc_hg_eval(g, float(v)) for v in fine], np.float64)
+        p = np.array([2.0 * np.pi * np.trapezoid(fv[i * 200:(i + 1) * 200 + 1], fine[i * 200:(i + 1) * 200 + 1])
+                      for i in range(20)])
+        expect = p / p.sum() * len(s)
+        z = (counts - expect) / np.sqrt(np.maximum(expect, 1.0))
+        assert np.abs(z).max() < 5.0, (g, z)
